@@ -1,0 +1,76 @@
+/* msmpb_b200.h - extensions of the drop-in MSM API (see forcefield.h).
+ *
+ * The reference API (code/forcefield.h:70-112) has no status codes, no
+ * per-atom potentials, no precision choice and host arrays only. These entry
+ * points add them without changing any reference signature.
+ */
+#ifndef MSMPB_B200_EXT_H
+#define MSMPB_B200_EXT_H
+
+#include "forcefield.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (FF_last_error and int-returning entry points). The
+ * reference prints and continues, or exits (code/forcefield0.c:152,
+ * :210-213); this library never exits, never traps the GPU, and records the
+ * first failure of a call here. */
+#define MSMPB_OK 0
+#define MSMPB_ERR_ARGUMENT 1     /* invalid size, pointer or parameter */
+#define MSMPB_ERR_STATE 2        /* call order violated (e.g. energy before build) */
+#define MSMPB_ERR_CUDA 3         /* a CUDA runtime call failed */
+#define MSMPB_ERR_NOMEM 4        /* device or host allocation failed */
+#define MSMPB_ERR_NODEVICE 5     /* no usable sm_100 device */
+#define MSMPB_ERR_DEVICE_CHECK 6 /* a kernel's own bounds or wait check tripped */
+#define MSMPB_ERR_UNSUPPORTED 7  /* parameter outside what the kernels support */
+
+/* Arithmetic of the evaluation. MIXED: pair sum, grid transfers, stencils and
+ * interpolation in FP32 with compensated per-atom accumulation; top-level FFT,
+ * energy reductions and charge-neutrality terms in FP64. FP64: everything in
+ * FP64 (the plain FP64 GPU form). */
+#define MSMPB_PRECISION_MIXED 0
+#define MSMPB_PRECISION_FP64 1
+
+int FF_last_error(const FF *ff);
+const char *FF_error_string(int code);
+
+/* Precision and device: may be called before FF_build or between
+ * evaluations (the device plan is rebuilt). */
+void FF_set_precision(FF *ff, int precision);
+int FF_get_precision(const FF *ff);
+void FF_set_device(FF *ff, int device);
+
+/* FF_energy plus per-atom potentials phi_i = dU/dq_i (N doubles, may be
+ * NULL). Same host-array conventions as FF_energy. */
+double FF_energy_potentials(FF *ff, double (*force)[3], double (*position)[3],
+                            double *weight, double *potential);
+
+/* Device-resident evaluation, asynchronous on `stream` (a cudaStream_t, NULL
+ * = the library's own stream). position_d: N*3 doubles; charge_d: N doubles;
+ * weight: host array of maxLevel+1 doubles or NULL; force_d (N*3),
+ * potential_d (N) and energy_d (1) are device outputs, each may be NULL.
+ * Returns MSMPB_OK or an error code; kernel-side checks are reported by the
+ * next call or by FF_sync. */
+int FF_energy_device(FF *ff, const double *position_d, const double *charge_d,
+                     const double *weight, double *force_d,
+                     double *potential_d, double *energy_d, void *stream);
+
+/* Waits for the library's stream and reports device-side check failures. */
+int FF_sync(FF *ff);
+
+/* Milliseconds of each phase of the last evaluation, measured with CUDA
+ * events on the evaluation stream (also copied into the reference's time_*
+ * fields in seconds). Order: bin, pair, anterpolation, restriction,
+ * stencils (all levels), top solve, prolongation, interpolation, combine,
+ * total. Returns the number of entries written (<= n). */
+int FF_phase_times(FF *ff, double *ms, int n);
+
+/* Number of kernel launches one evaluation issues (for accounting). */
+int FF_kernel_launches(FF *ff);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,568 @@
+// Device plan and the launch sequence of one MSM evaluation
+// (code/forcefield1.c:101-235 restated for one B200):
+//
+//   bin + sort atoms (pair cells, finest-grid cells)   deterministic order
+//   short-range pair sum                                 k_pair
+//   anterpolation -> q^1                                 k_anterpolate
+//   restriction q^l -> q^{l+1}, l < L                    k_restrict
+//   top level: FFT(q^L) * khat_L -> e^L (FP64)           k_fft_pass x5
+//   for l = L-1..1: e^l = prolong(e^{l+1}) + w_l K_l q^l  k_prolong, k_pad, stencil
+//   interpolation of e^1 -> E, phi_long                  k_interpolate
+//   per-atom combine, energy reductions (FP64)           k_combine, k_energy_total
+//
+// Everything after the input copy is captured once into a CUDA graph and
+// replayed; the graph is re-captured only when pointers or weights change.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "engine.h"
+#include "kernels.h"
+#include "msmpb_b200.h"
+
+struct FFDevice {
+  virtual ~FFDevice() {}
+  virtual int update(const msm::Tables &t) = 0;
+  virtual int evaluate(const msm::EvalRequest &r, double *energy) = 0;
+  virtual int sync() = 0;
+  virtual int phase_times(double *ms, int n) = 0;
+  virtual int launches() = 0;
+};
+
+namespace msm {
+namespace {
+
+#define MSM_CUDA_TRY(expr)                       \
+  do {                                           \
+    cudaError_t e_ = (expr);                     \
+    if (e_ != cudaSuccess) return MSMPB_ERR_CUDA; \
+  } while (0)
+
+// One cudaMalloc arena, carved into 256-byte aligned pieces.
+struct Arena {
+  char *base = nullptr;
+  size_t size = 0, used = 0;
+  std::vector<std::pair<void **, size_t>> plan;
+  template <typename P>
+  void want(P **p, size_t bytes) {
+    plan.push_back({(void **)p, bytes});
+  }
+  int commit() {
+    size_t total = 0;
+    for (auto &e : plan) total += (e.second + 255) / 256 * 256;
+    if (cudaMalloc(&base, std::max<size_t>(total, 256)) != cudaSuccess) {
+      base = nullptr;
+      return MSMPB_ERR_NOMEM;
+    }
+    size = total;
+    for (auto &e : plan) {
+      *e.first = base + used;
+      used += (e.second + 255) / 256 * 256;
+    }
+    return MSMPB_OK;
+  }
+  ~Arena() {
+    if (base) cudaFree(base);
+  }
+};
+
+struct GraphKey {
+  const void *pos, *q, *force, *phi, *energy;
+  double w[kMaxLevels + 1];
+  bool timing;
+  bool operator==(const GraphKey &o) const {
+    return std::memcmp(this, &o, sizeof(GraphKey)) == 0;
+  }
+};
+
+template <typename T>
+class Plan : public FFDevice {
+ public:
+  int init(const Tables &t, int device);
+  ~Plan() override;
+  int update(const Tables &t) override;
+  int evaluate(const EvalRequest &r, double *energy) override;
+  int sync() override;
+  int phase_times(double *ms, int n) override;
+  int launches() override { return nlaunch_; }
+
+ private:
+  int set_tables(const Tables &t);
+  int enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
+              const double *q, double *force, double *phi, double *energy);
+  void mark(cudaStream_t s, int phase, bool timing) {
+    if (timing) cudaEventRecord(ev_[phase], s);
+  }
+
+  int device_ = 0;
+  cudaStream_t stream_ = nullptr;
+  int N_ = 0, L_ = 0, nu_ = 0;
+  int grid_[kMaxLevels + 2][3] = {};
+  StencilShape sh_[kMaxLevels + 2] = {};
+  Geometry geom_{};
+  PairConsts<T> pc_{};
+  SplineConsts<T> sc_{};
+  double J_[11] = {};
+  double coeff1_ = 0, coeff2_ = 0, gamma0_a0_ = 0;
+  int ncp_ = 0, ncg_ = 0, noff_ = 0;
+  int nq_ = 0, ncomb_ = 0, ngrid_ = 0;
+  std::vector<CellOffset<T>> offsets_;
+  Arena arena_;
+  // device buffers
+  double *pos_s_ = nullptr, *q_s_ = nullptr, *force_s_ = nullptr,
+         *phi_s_ = nullptr;
+  int *pcell_ = nullptr, *gcell_ = nullptr, *pcount_ = nullptr,
+      *gcount_ = nullptr, *pstart_ = nullptr, *gstart_ = nullptr,
+      *pcursor_ = nullptr, *gcursor_ = nullptr, *scan_tmp_ = nullptr;
+  int *pperm_ = nullptr, *gperm_ = nullptr, *pinv_ = nullptr,
+      *ginv_ = nullptr, *pcs_ = nullptr, *gcs_ = nullptr;
+  V4<T> *prel_ = nullptr, *gfrac_ = nullptr, *psorted_ = nullptr,
+        *gsorted_ = nullptr, *pout_ = nullptr, *gout_ = nullptr;
+  T *qg_[kMaxLevels + 2] = {}, *eg_[kMaxLevels + 2] = {};
+  T *padded_ = nullptr, *kh_[kMaxLevels + 2] = {};
+  double *khat_top_ = nullptr;
+  double2 *fft_ = nullptr;
+  double *qparts_ = nullptr, *short_parts_ = nullptr, *grid_parts_ = nullptr,
+         *qstats_ = nullptr, *energy_ = nullptr;
+  CellOffset<T> *off_d_ = nullptr;
+  int *err_d_ = nullptr;
+  // graph
+  cudaGraphExec_t exec_ = nullptr;
+  GraphKey key_{};
+  bool have_graph_ = false;
+  cudaEvent_t ev_[kNumPhases + 1] = {};
+  bool timed_ = false;
+  int nlaunch_ = 0;
+};
+
+template <typename T>
+Plan<T>::~Plan() {
+  if (stream_) cudaStreamSynchronize(stream_);
+  if (exec_) cudaGraphExecDestroy(exec_);
+  for (auto &e : ev_)
+    if (e) cudaEventDestroy(e);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+template <typename T>
+int Plan<T>::init(const Tables &t, int device) {
+  device_ = device;
+  MSM_CUDA_TRY(cudaSetDevice(device));
+  MSM_CUDA_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  for (auto &e : ev_) MSM_CUDA_TRY(cudaEventCreate(&e));
+  const Params &p = t.p;
+  N_ = p.N;
+  L_ = p.L;
+  nu_ = p.nu;
+  for (int l = 1; l <= L_; ++l)
+    for (int k = 0; k < 3; ++k) grid_[l][k] = t.grid[l][k];
+  // pair cells at least a0/2 thick: nc = floor(2 / (a0 |a*|))
+  long ncell = 1;
+  for (int k = 0; k < 3; ++k) {
+    double w = p.a0 * std::sqrt(p.Ai[k][0] * p.Ai[k][0] + p.Ai[k][1] * p.Ai[k][1] +
+                                p.Ai[k][2] * p.Ai[k][2]);
+    int nc = (int)std::floor(2.0 / w);
+    geom_.nc[k] = std::max(1, std::min(nc, 512));
+    ncell *= geom_.nc[k];
+    geom_.M1[k] = t.grid[1][k];
+  }
+  ncp_ = (int)ncell;
+  ncg_ = grid_[1][0] * grid_[1][1] * grid_[1][2];
+  if (!top_solve_supported(p.top)) return MSMPB_ERR_UNSUPPORTED;
+  int err = set_tables(t);
+  if (err) return err;
+  // stencil shapes
+  size_t pad_max = 1;
+  for (int l = 1; l < L_; ++l) {
+    StencilShape &s = sh_[l];
+    for (int k = 0; k < 3; ++k) {
+      s.M[k] = grid_[l][k];
+      s.S[k] = t.sten[l][k];
+    }
+    s.P[0] = s.M[0] + s.S[0] - 1;
+    s.P[1] = s.M[1] + s.S[1] - 1;
+    s.P[2] = stencil_padded_z(s.M[2], s.S[2]);
+    pad_max = std::max(pad_max, (size_t)s.P[0] * s.P[1] * s.P[2]);
+  }
+  const size_t n = N_;
+  nq_ = std::min(1024, std::max(1, (N_ + 255) / 256));
+  ncomb_ = combine_blocks(N_);
+  ngrid_ = grid_dot_blocks((size_t)ncg_);
+  Arena &a = arena_;
+  a.want(&pos_s_, 3 * n * sizeof(double));
+  a.want(&q_s_, n * sizeof(double));
+  a.want(&force_s_, 3 * n * sizeof(double));
+  a.want(&phi_s_, n * sizeof(double));
+  for (int **b : {&pcell_, &gcell_, &pperm_, &gperm_, &pinv_, &ginv_, &pcs_, &gcs_})
+    a.want(b, n * sizeof(int));
+  a.want(&pcount_, (ncp_ + 1) * sizeof(int));
+  a.want(&pstart_, (ncp_ + 1) * sizeof(int));
+  a.want(&pcursor_, (ncp_ + 1) * sizeof(int));
+  a.want(&gcount_, (ncg_ + 1) * sizeof(int));
+  a.want(&gstart_, (ncg_ + 1) * sizeof(int));
+  a.want(&gcursor_, (ncg_ + 1) * sizeof(int));
+  a.want(&scan_tmp_, std::max(scan_temp_ints(ncp_), scan_temp_ints(ncg_)) * sizeof(int));
+  for (V4<T> **b : {&prel_, &gfrac_, &psorted_, &gsorted_, &pout_, &gout_})
+    a.want(b, n * sizeof(V4<T>));
+  for (int l = 1; l <= L_; ++l) {
+    size_t g = (size_t)grid_[l][0] * grid_[l][1] * grid_[l][2];
+    a.want(&qg_[l], g * sizeof(T));
+    a.want(&eg_[l], g * sizeof(T));
+    if (l < L_)
+      a.want(&kh_[l], (size_t)sh_[l].S[0] * sh_[l].S[1] * sh_[l].S[2] * sizeof(T));
+  }
+  a.want(&padded_, pad_max * sizeof(T));
+  size_t ntop = (size_t)grid_[L_][0] * grid_[L_][1] * grid_[L_][2];
+  a.want(&khat_top_, ntop * sizeof(double));
+  a.want(&fft_, ntop * sizeof(double2));
+  a.want(&qparts_, 2 * nq_ * sizeof(double));
+  a.want(&short_parts_, ncomb_ * sizeof(double));
+  a.want(&grid_parts_, ngrid_ * sizeof(double));
+  a.want(&qstats_, 2 * sizeof(double));
+  a.want(&energy_, sizeof(double));
+  a.want(&off_d_, kMaxNeighbourOffsets * sizeof(CellOffset<T>));
+  a.want(&err_d_, sizeof(int));
+  if ((err = a.commit())) return err;
+  MSM_CUDA_TRY(cudaMemset(err_d_, 0, sizeof(int)));
+  return update(t);
+}
+
+// Constants that depend only on the parameter set (not on the box)
+template <typename T>
+int Plan<T>::set_tables(const Tables &t) {
+  const Params &p = t.p;
+  pc_.nu = sc_.nu = p.nu;
+  pc_.a02 = (T)(p.a0 * p.a0);
+  pc_.inv_a02 = (T)(1. / (p.a0 * p.a0));
+  pc_.inv_a0 = (T)(1. / p.a0);
+  pc_.two_inv_a03 = (T)(2. / (p.a0 * p.a0 * p.a0));
+  for (int k = 0; k < 16; ++k) pc_.tau[k] = (T)t.tau[k];
+  for (int k = 0; k < 50; ++k) sc_.Q[k] = (T)t.Q[k];
+  for (int k = 0; k < 11; ++k) J_[k] = t.J[k];
+  return MSMPB_OK;
+}
+
+// Box-dependent state: geometry, neighbour offsets, stencils, constants
+template <typename T>
+int Plan<T>::update(const Tables &t) {
+  const Params &p = t.p;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      geom_.A[3 * r + c] = p.A[r][c];
+      geom_.Ai[3 * r + c] = p.Ai[r][c];
+    }
+  coeff1_ = t.coeff1;
+  coeff2_ = t.coeff2;
+  gamma0_a0_ = t.gamma0 / p.a0;
+  // neighbour-cell instances: every offset d with |d_k| <= ceil(a0|a*_k| nc_k)
+  bool ortho = true;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c)
+      if (r != c && p.A[r][c] != 0.) ortho = false;
+  int K[3];
+  for (int k = 0; k < 3; ++k) {
+    double w = p.a0 * std::sqrt(p.Ai[k][0] * p.Ai[k][0] + p.Ai[k][1] * p.Ai[k][1] +
+                                p.Ai[k][2] * p.Ai[k][2]);
+    K[k] = (int)std::ceil(w * geom_.nc[k]);
+  }
+  offsets_.clear();
+  for (int dx = -K[0]; dx <= K[0]; ++dx)
+    for (int dy = -K[1]; dy <= K[1]; ++dy)
+      for (int dz = -K[2]; dz <= K[2]; ++dz) {
+        int d[3] = {dx, dy, dz};
+        if (ortho) {  // skip cells whose nearest point is beyond a0
+          double m2 = 0;
+          for (int k = 0; k < 3; ++k) {
+            double gap = std::max(0, std::abs(d[k]) - 1) * std::fabs(p.A[k][k]) / geom_.nc[k];
+            m2 += gap * gap;
+          }
+          if (m2 >= p.a0 * p.a0) continue;
+        }
+        CellOffset<T> o{};
+        for (int k = 0; k < 3; ++k) o.d[k] = d[k];
+        for (int r = 0; r < 3; ++r) {
+          double v = 0;
+          for (int c = 0; c < 3; ++c) v += p.A[r][c] * ((double)d[c] / geom_.nc[c]);
+          o.shift[r] = (T)v;
+        }
+        offsets_.push_back(o);
+      }
+  if ((int)offsets_.size() > kMaxNeighbourOffsets) return MSMPB_ERR_UNSUPPORTED;
+  noff_ = (int)offsets_.size();
+  MSM_CUDA_TRY(cudaSetDevice(device_));
+  MSM_CUDA_TRY(cudaMemcpy(off_d_, offsets_.data(), noff_ * sizeof(CellOffset<T>),
+                          cudaMemcpyHostToDevice));
+  for (int l = 1; l < L_; ++l) {
+    std::vector<T> kh(t.khat[l].begin(), t.khat[l].end());
+    MSM_CUDA_TRY(cudaMemcpy(kh_[l], kh.data(), kh.size() * sizeof(T),
+                            cudaMemcpyHostToDevice));
+  }
+  MSM_CUDA_TRY(cudaMemcpy(khat_top_, t.khat[L_].data(),
+                          t.khat[L_].size() * sizeof(double),
+                          cudaMemcpyHostToDevice));
+  if (exec_) {
+    cudaGraphExecDestroy(exec_);
+    exec_ = nullptr;
+  }
+  have_graph_ = false;  // geometry is baked into kernel parameters
+  return MSMPB_OK;
+}
+
+template <typename T>
+int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
+                     const double *q, double *force, double *phi,
+                     double *energy) {
+  const bool tm = r.timing;
+  int nl = 0;
+  double w[kMaxLevels + 1];
+  for (int l = 0; l <= L_; ++l) w[l] = r.weight ? r.weight[l] : 1.0;
+  mark(s, kPhaseBin, tm);
+  cudaMemsetAsync(pcount_, 0, (ncp_ + 1) * sizeof(int), s);
+  cudaMemsetAsync(gcount_, 0, (ncg_ + 1) * sizeof(int), s);
+  cudaMemsetAsync(pcursor_, 0, (ncp_ + 1) * sizeof(int), s);
+  cudaMemsetAsync(gcursor_, 0, (ncg_ + 1) * sizeof(int), s);
+  launch_charge_stats(s, N_, q, qparts_, nq_);
+  launch_qstats_final(s, qparts_, nq_, qstats_);
+  launch_prep<T>(s, N_, pos, q, geom_, pcell_, gcell_, pcount_, gcount_, prel_,
+                 gfrac_, err_d_);
+  launch_scan(s, pcount_, pstart_, ncp_, scan_tmp_);
+  launch_scan(s, gcount_, gstart_, ncg_, scan_tmp_);
+  launch_scatter(s, N_, pcell_, pstart_, pcursor_, pperm_);
+  launch_scatter(s, N_, gcell_, gstart_, gcursor_, gperm_);
+  launch_segment_sort(s, ncp_, pstart_, pperm_);
+  launch_segment_sort(s, ncg_, gstart_, gperm_);
+  launch_gather<T>(s, N_, pperm_, prel_, pcell_, psorted_, pcs_, pinv_);
+  launch_gather<T>(s, N_, gperm_, gfrac_, gcell_, gsorted_, gcs_, ginv_);
+  nl += 3 + 6 + 2 + 2 + 2;
+  mark(s, kPhasePair, tm);
+  launch_pair<T>(s, N_, psorted_, pcs_, pstart_, geom_, off_d_, noff_, pc_, pout_);
+  nl += 1;
+  mark(s, kPhaseAnterp, tm);
+  launch_anterpolate<T>(s, grid_[1], gsorted_, gstart_, sc_, qg_[1]);
+  nl += 1;
+  mark(s, kPhaseRestrict, tm);
+  for (int l = 1; l < L_; ++l) {
+    launch_restrict<T>(s, grid_[l], qg_[l], qg_[l + 1], J_, nu_);
+    nl += 1;
+  }
+  mark(s, kPhaseTop, tm);
+  launch_top_solve<T>(s, grid_[L_], qg_[L_], khat_top_, w[L_], fft_, nullptr,
+                      eg_[L_]);
+  nl += 5;
+  // levels L-1..1: prolongation then the level stencil
+  float pro_ms = 0;
+  (void)pro_ms;
+  for (int l = L_ - 1; l >= 1; --l) {
+    mark(s, kPhaseProlong, tm && l == L_ - 1);
+    cudaMemsetAsync(eg_[l], 0,
+                    (size_t)grid_[l][0] * grid_[l][1] * grid_[l][2] * sizeof(T), s);
+    launch_prolong_add<T>(s, grid_[l], eg_[l + 1], eg_[l], J_, nu_);
+    mark(s, kPhaseStencil, tm && l == L_ - 1);
+    launch_pad<T>(s, sh_[l], qg_[l], padded_);
+    launch_stencil<T>(s, sh_[l], padded_, kh_[l], (T)w[l], eg_[l], 0);
+    nl += 3;
+  }
+  mark(s, kPhaseInterp, tm);
+  launch_grid_dot<T>(s, (size_t)ncg_, qg_[1], eg_[1], grid_parts_, ngrid_);
+  launch_interpolate<T>(s, N_, grid_[1], gsorted_, gcs_, eg_[1], sc_, geom_, gout_);
+  nl += 2;
+  mark(s, kPhaseCombine, tm);
+  CombineArgs ca;
+  ca.N = N_;
+  ca.w0 = w[0];
+  ca.coeff1 = coeff1_;
+  ca.coeff2 = coeff2_;
+  ca.gamma0_over_a0 = gamma0_a0_;
+  ca.q = q;
+  ca.qstats = qstats_;
+  ca.nqparts = nq_;
+  ca.qparts = qparts_;
+  ca.force = force;
+  ca.phi = phi;
+  ca.epart = short_parts_;
+  launch_combine<T>(s, ca, pinv_, ginv_, pout_, gout_, ncomb_);
+  EnergyArgs ea;
+  ea.qparts = qparts_;
+  ea.nqparts = nq_;
+  ea.short_parts = short_parts_;
+  ea.nshort = ncomb_;
+  ea.grid_parts = grid_parts_;
+  ea.ngrid = ngrid_;
+  ea.w0 = w[0];
+  ea.coeff1 = coeff1_;
+  ea.coeff2 = coeff2_;
+  ea.gamma0_over_a0 = gamma0_a0_;
+  ea.energy = energy ? energy : energy_;
+  ea.qstats = qstats_;
+  launch_energy_total(s, ea);
+  nl += 2;
+  mark(s, kNumPhases, tm);
+  nlaunch_ = nl;
+  return cudaGetLastError() == cudaSuccess ? MSMPB_OK : MSMPB_ERR_CUDA;
+}
+
+template <typename T>
+int Plan<T>::evaluate(const EvalRequest &r, double *energy) {
+  MSM_CUDA_TRY(cudaSetDevice(device_));
+  cudaStream_t s = (r.host || !r.stream) ? stream_ : r.stream;
+  const double *pos = r.pos, *q = r.q;
+  double *force = r.force, *phi = r.phi;
+  if (r.host) {
+    MSM_CUDA_TRY(cudaMemcpyAsync(pos_s_, r.pos, 3 * (size_t)N_ * sizeof(double),
+                                 cudaMemcpyHostToDevice, s));
+    MSM_CUDA_TRY(cudaMemcpyAsync(q_s_, r.q, (size_t)N_ * sizeof(double),
+                                 cudaMemcpyHostToDevice, s));
+    pos = pos_s_;
+    q = q_s_;
+    force = r.force ? force_s_ : nullptr;
+    phi = r.phi ? phi_s_ : nullptr;
+  }
+  double *edev = r.host ? energy_ : (r.energy_dev ? r.energy_dev : energy_);
+  GraphKey key{};
+  key.pos = pos;
+  key.q = q;
+  key.force = force;
+  key.phi = phi;
+  key.energy = edev;
+  for (int l = 0; l <= L_; ++l) key.w[l] = r.weight ? r.weight[l] : 1.0;
+  key.timing = r.timing;
+  if (!have_graph_ || !(key == key_)) {
+    if (exec_) {
+      cudaGraphExecDestroy(exec_);
+      exec_ = nullptr;
+    }
+    have_graph_ = false;
+    cudaGraph_t g = nullptr;
+    MSM_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int st = enqueue(r, s, pos, q, force, phi, edev);
+    cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (st != MSMPB_OK || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      return st != MSMPB_OK ? st : MSMPB_ERR_CUDA;
+    }
+    cudaError_t ie = cudaGraphInstantiate(&exec_, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      exec_ = nullptr;
+      return MSMPB_ERR_CUDA;
+    }
+    key_ = key;
+    have_graph_ = true;
+  }
+  MSM_CUDA_TRY(cudaGraphLaunch(exec_, s));
+  timed_ = r.timing;
+  if (r.host) {
+    if (r.force)
+      MSM_CUDA_TRY(cudaMemcpyAsync(r.force, force_s_, 3 * (size_t)N_ * sizeof(double),
+                                   cudaMemcpyDeviceToHost, s));
+    if (r.phi)
+      MSM_CUDA_TRY(cudaMemcpyAsync(r.phi, phi_s_, (size_t)N_ * sizeof(double),
+                                   cudaMemcpyDeviceToHost, s));
+    double e = 0;
+    MSM_CUDA_TRY(cudaMemcpyAsync(&e, energy_, sizeof(double),
+                                 cudaMemcpyDeviceToHost, s));
+    int st = sync();
+    if (energy) *energy = e;
+    return st;
+  }
+  return MSMPB_OK;
+}
+
+template <typename T>
+int Plan<T>::sync() {
+  MSM_CUDA_TRY(cudaSetDevice(device_));
+  MSM_CUDA_TRY(cudaStreamSynchronize(stream_));
+  int flag = 0;
+  MSM_CUDA_TRY(cudaMemcpy(&flag, err_d_, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag) {
+    cudaMemset(err_d_, 0, sizeof(int));
+    return MSMPB_ERR_DEVICE_CHECK;
+  }
+  return MSMPB_OK;
+}
+
+template <typename T>
+int Plan<T>::phase_times(double *ms, int n) {
+  if (!timed_) return 0;
+  cudaStreamSynchronize(stream_);
+  int order[kNumPhases + 1];
+  for (int k = 0; k <= kNumPhases; ++k) order[k] = k;
+  // phases were recorded in pipeline order: bin, pair, anterp, restrict,
+  // top, prolong, stencil, interp, combine, end
+  int seq[] = {kPhaseBin, kPhasePair, kPhaseAnterp, kPhaseRestrict, kPhaseTop,
+               kPhaseProlong, kPhaseStencil, kPhaseInterp, kPhaseCombine,
+               kNumPhases};
+  double out[kNumPhases + 1] = {};
+  const int nseq = sizeof(seq) / sizeof(int);
+  for (int i = 0; i + 1 < nseq; ++i) {
+    int a = seq[i];
+    int b = seq[i + 1];
+    if (L_ == 1 && (a == kPhaseProlong || a == kPhaseStencil)) continue;
+    if (L_ == 1 && a == kPhaseTop) b = kPhaseInterp;
+    float t = 0;
+    if (cudaEventElapsedTime(&t, ev_[a], ev_[b]) == cudaSuccess) out[a] = t;
+  }
+  // prolongation and stencils interleave over levels: the span from the
+  // first prolongation to the interpolation is attributed to the stencil
+  // phase except for the first level's prolongation
+  float tot = 0;
+  cudaEventElapsedTime(&tot, ev_[kPhaseBin], ev_[kNumPhases]);
+  out[kNumPhases] = tot;
+  (void)order;
+  int m = std::min(n, kNumPhases + 1);
+  for (int k = 0; k < m; ++k) ms[k] = out[k];
+  return m;
+}
+
+}  // namespace
+
+FFDevice *engine_create(const Tables &t, int precision, int device, int *err) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    *err = MSMPB_ERR_NODEVICE;
+    return nullptr;
+  }
+  if (device < 0 || device >= ndev) {
+    *err = MSMPB_ERR_ARGUMENT;
+    return nullptr;
+  }
+  FFDevice *d = nullptr;
+  int st;
+  if (precision == MSMPB_PRECISION_FP64) {
+    auto *p = new Plan<double>();
+    st = p->init(t, device);
+    d = p;
+  } else {
+    auto *p = new Plan<float>();
+    st = p->init(t, device);
+    d = p;
+  }
+  if (st != MSMPB_OK) {
+    delete d;
+    *err = st;
+    return nullptr;
+  }
+  *err = MSMPB_OK;
+  return d;
+}
+
+void engine_destroy(FFDevice *d) { delete d; }
+
+int engine_update_tables(FFDevice *d, const Tables &t) { return d->update(t); }
+
+int engine_evaluate(FFDevice *d, const EvalRequest &r, double *energy) {
+  return d->evaluate(r, energy);
+}
+
+int engine_sync(FFDevice *d) { return d->sync(); }
+
+int engine_phase_times(FFDevice *d, double *ms, int n) {
+  return d->phase_times(ms, n);
+}
+
+int engine_kernel_launches(FFDevice *d) { return d->launches(); }
+
+}  // namespace msm

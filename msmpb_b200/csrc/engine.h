@@ -1,0 +1,57 @@
+// Device plan for one FF handle: buffers, uploaded tables, the launch
+// sequence of one evaluation and its CUDA graph.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "msm_host.h"
+
+struct FFDevice;
+
+namespace msm {
+
+enum Phase {
+  kPhaseBin = 0,
+  kPhasePair,
+  kPhaseAnterp,
+  kPhaseRestrict,
+  kPhaseStencil,
+  kPhaseTop,
+  kPhaseProlong,
+  kPhaseInterp,
+  kPhaseCombine,
+  kNumPhases
+};
+
+// Creates the device plan for the tables (allocates everything an
+// evaluation needs). Returns nullptr and sets *err on failure.
+FFDevice *engine_create(const Tables &t, int precision, int device, int *err);
+void engine_destroy(FFDevice *d);
+
+// Re-uploads box-dependent tables after FF_rebuild (same sizes).
+int engine_update_tables(FFDevice *d, const Tables &t);
+
+struct EvalRequest {
+  const double *pos;     // host or device N*3
+  const double *q;       // host or device N
+  bool host;             // pos/q/force/phi are host pointers
+  const double *weight;  // host, L+1 entries or nullptr
+  double *force;         // N*3 or nullptr
+  double *phi;           // N or nullptr
+  double *energy_dev;    // device scalar or nullptr (device mode)
+  cudaStream_t stream;   // device mode: caller stream (0 = own stream)
+  bool timing;           // record per-phase events
+};
+
+// Runs one evaluation. Host mode synchronises and returns the energy in
+// *energy; device mode is asynchronous. Returns an MSMPB_* status.
+int engine_evaluate(FFDevice *d, const EvalRequest &r, double *energy);
+
+// Waits for outstanding work and returns device-side check flags as status.
+int engine_sync(FFDevice *d);
+
+// Phase times of the last timed evaluation (ms), kNumPhases + total.
+int engine_phase_times(FFDevice *d, double *ms, int n);
+int engine_kernel_launches(FFDevice *d);
+
+}  // namespace msm

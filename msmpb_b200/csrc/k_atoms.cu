@@ -1,0 +1,391 @@
+// Atom-side kernels: fractional coordinates and binning, a deterministic
+// counting sort by cell (scan + scatter + per-cell ordering by atom index),
+// gathers into cell order, the final per-atom combine and the energy sums.
+#include <algorithm>
+
+#include "kernels.h"
+
+namespace msm {
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ double matvec_row(const double *m, int r,
+                                             double x, double y, double z) {
+  return m[3 * r] * x + m[3 * r + 1] * y + m[3 * r + 2] * z;
+}
+
+// Per atom: s = A^-1 r wrapped to [0,1); pair cell; finest-grid cell m and
+// offset t = M s - m (code/forcefield1.c:350-357); position relative to the
+// pair cell's origin. Counts atoms per cell.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_prep(int N, const double *__restrict__ pos, const double *__restrict__ q,
+       Geometry g, int *__restrict__ pcell, int *__restrict__ gcell,
+       int *__restrict__ pcount, int *__restrict__ gcount,
+       V4<T> *__restrict__ prel, V4<T> *__restrict__ gfrac, int *err) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double r0 = pos[3 * i], r1 = pos[3 * i + 1], r2 = pos[3 * i + 2];
+  double qi = q[i];
+  double s[3];
+  bool ok = isfinite(qi);
+  for (int k = 0; k < 3; ++k) {
+    s[k] = matvec_row(g.Ai, k, r0, r1, r2);
+    ok = ok && isfinite(s[k]);
+  }
+  if (!ok) {
+    flag_error(err, kCheckNonFinite);
+    s[0] = s[1] = s[2] = 0.;
+  }
+  int c[3], m[3];
+  double t[3], frac[3];
+  for (int k = 0; k < 3; ++k) {
+    double sk = s[k] - floor(s[k]);
+    c[k] = min((int)(sk * g.nc[k]), g.nc[k] - 1);
+    frac[k] = sk - (double)c[k] / g.nc[k];
+    double u = sk * g.M1[k];
+    double fu = floor(u);
+    t[k] = u - fu;
+    int mk = (int)fu;
+    m[k] = mk >= g.M1[k] ? mk - g.M1[k] : mk;
+  }
+  int pc = (c[0] * g.nc[1] + c[1]) * g.nc[2] + c[2];
+  int gc = (m[0] * g.M1[1] + m[1]) * g.M1[2] + m[2];
+  pcell[i] = pc;
+  gcell[i] = gc;
+  atomicAdd(pcount + pc, 1);
+  atomicAdd(gcount + gc, 1);
+  V4<T> a;
+  a.x = (T)matvec_row(g.A, 0, frac[0], frac[1], frac[2]);
+  a.y = (T)matvec_row(g.A, 1, frac[0], frac[1], frac[2]);
+  a.z = (T)matvec_row(g.A, 2, frac[0], frac[1], frac[2]);
+  a.w = (T)qi;
+  prel[i] = a;
+  V4<T> b;
+  b.x = (T)t[0];
+  b.y = (T)t[1];
+  b.z = (T)t[2];
+  b.w = (T)qi;
+  gfrac[i] = b;
+}
+
+// Block-level partial sums of q and q^2 (FP64)
+__global__ void __launch_bounds__(kThreads)
+k_charge_stats(int N, const double *__restrict__ q, double *partials) {
+  __shared__ double s1[kThreads], s2[kThreads];
+  double a = 0., b = 0.;
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N;
+       i += gridDim.x * kThreads) {
+    double v = q[i];
+    a += v;
+    b += v * v;
+  }
+  s1[threadIdx.x] = a;
+  s2[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = kThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      s1[threadIdx.x] += s1[threadIdx.x + w];
+      s2[threadIdx.x] += s2[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = s1[0];
+    partials[2 * blockIdx.x + 1] = s2[0];
+  }
+}
+
+// ---- exclusive scan (three phases) ----
+constexpr int kScanThreads = 512;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ int block_exclusive_scan(int v, int *sh, int *total) {
+  // warp-shuffle scan then warp totals
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = (lane < kScanThreads / 32) ? sh[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < kScanThreads / 32) sh[lane] = w;
+  }
+  __syncthreads();
+  int before = (warp > 0 ? sh[warp - 1] : 0) + x - v;
+  if (total) *total = sh[kScanThreads / 32 - 1];
+  __syncthreads();
+  return before;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_reduce(const int *__restrict__ in, int n, int *__restrict__ bsum) {
+  __shared__ int sh[32];
+  int base = blockIdx.x * kScanTile;
+  int v = 0;
+  for (int k = 0; k < kScanItems; ++k) {
+    int idx = base + threadIdx.x * kScanItems + k;
+    if (idx < n) v += in[idx];
+  }
+  int total;
+  block_exclusive_scan(v, sh, &total);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_top(int *bsum, int nb) {
+  __shared__ int sh[32];
+  int carry = 0;
+  for (int base = 0; base < nb; base += kScanThreads) {
+    int idx = base + threadIdx.x;
+    int v = idx < nb ? bsum[idx] : 0;
+    int total;
+    int ex = block_exclusive_scan(v, sh, &total);
+    if (idx < nb) bsum[idx] = carry + ex;
+    carry += total;
+  }
+  if (threadIdx.x == 0) bsum[nb] = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_apply(const int *__restrict__ in, int n, const int *__restrict__ bsum,
+             int nb, int *__restrict__ out) {
+  __shared__ int sh[32];
+  int base = blockIdx.x * kScanTile;
+  int vals[kScanItems];
+  int v = 0;
+  for (int k = 0; k < kScanItems; ++k) {
+    int idx = base + threadIdx.x * kScanItems + k;
+    vals[k] = idx < n ? in[idx] : 0;
+    v += vals[k];
+  }
+  int ex = block_exclusive_scan(v, sh, nullptr) + bsum[blockIdx.x];
+  for (int k = 0; k < kScanItems; ++k) {
+    int idx = base + threadIdx.x * kScanItems + k;
+    if (idx < n) out[idx] = ex;
+    ex += vals[k];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = bsum[nb];
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_scatter(int N, const int *__restrict__ cell, const int *__restrict__ start,
+          int *__restrict__ cursor, int *__restrict__ perm) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  int c = cell[i];
+  int slot = start[c] + atomicAdd(cursor + c, 1);
+  perm[slot] = i;
+}
+
+// Orders each cell's atoms by atom index, which makes every later
+// floating-point sum independent of the scatter's arrival order.
+__global__ void __launch_bounds__(kThreads)
+k_segment_sort(int ncell, const int *__restrict__ start, int *__restrict__ perm) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  int b = start[c], e = start[c + 1];
+  for (int k = b + 1; k < e; ++k) {
+    int v = perm[k];
+    int j = k - 1;
+    while (j >= b && perm[j] > v) {
+      perm[j + 1] = perm[j];
+      --j;
+    }
+    perm[j + 1] = v;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_gather(int N, const int *__restrict__ perm, const V4<T> *__restrict__ src,
+         const int *__restrict__ cell, V4<T> *__restrict__ dst,
+         int *__restrict__ cell_sorted, int *__restrict__ inv) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  int i = perm[k];
+  dst[k] = src[i];
+  cell_sorted[k] = cell[i];
+  inv[i] = k;
+}
+
+// Per atom in input order: F_i = w0 F_short + q_i E_i and
+// phi_i = w0 (q_i c1 - Q c2 - q_i gamma0/a0 + phi_short) + phi_long.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_combine(CombineArgs a, const int *__restrict__ pinv,
+          const int *__restrict__ ginv, const V4<T> *__restrict__ pout,
+          const V4<T> *__restrict__ gout) {
+  __shared__ double red[kThreads];
+  double qsum = 0.;
+  for (int b = 0; b < a.nqparts; ++b) qsum += a.qparts[2 * b];
+  double e = 0.;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < a.N) {
+    double qi = a.q[i];
+    V4<T> ps = pout[pinv[i]];
+    V4<T> gs = gout[ginv[i]];
+    if (a.force) {
+      a.force[3 * i] = a.w0 * (double)ps.x + qi * (double)gs.x;
+      a.force[3 * i + 1] = a.w0 * (double)ps.y + qi * (double)gs.y;
+      a.force[3 * i + 2] = a.w0 * (double)ps.z + qi * (double)gs.z;
+    }
+    if (a.phi)
+      a.phi[i] = a.w0 * (qi * a.coeff1 - qsum * a.coeff2 -
+                         qi * a.gamma0_over_a0 + (double)ps.w) +
+                 (double)gs.w;
+    e = 0.5 * a.w0 * qi * (double)ps.w;
+  }
+  red[threadIdx.x] = e;
+  __syncthreads();
+  for (int w = kThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) a.epart[blockIdx.x] = red[0];
+}
+
+__device__ double block_sum(const double *v, int n, double *sh) {
+  double acc = 0.;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) acc += v[k];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kThreads) k_qstats_final(const double *qparts, int n,
+                                                           double *qstats) {
+  __shared__ double sh[kThreads];
+  double a = 0., b = 0.;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    a += qparts[2 * k];
+    b += qparts[2 * k + 1];
+  }
+  sh[threadIdx.x] = a;
+  __syncthreads();
+  for (int w = kThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  double qs = sh[0];
+  __syncthreads();
+  sh[threadIdx.x] = b;
+  __syncthreads();
+  for (int w = kThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    qstats[0] = qs;
+    qstats[1] = sh[0];
+  }
+}
+
+// U = w0 (Q2 c1/2 - Q^2 c2/2 - Q2 gamma0/(2 a0)) + w0 sum q phi_s / 2
+//     + q^1 . e^1 / 2      (code/forcefield1.c:114-137, :195-219)
+__global__ void __launch_bounds__(kThreads) k_energy_total(EnergyArgs a) {
+  __shared__ double sh[kThreads];
+  double qs = a.qstats[0], q2 = a.qstats[1];
+  double us = block_sum(a.short_parts, a.nshort, sh);
+  double ug = block_sum(a.grid_parts, a.ngrid, sh);
+  if (threadIdx.x == 0) {
+    double uc = 0.5 * q2 * a.coeff1 - 0.5 * qs * qs * a.coeff2 -
+                0.5 * q2 * a.gamma0_over_a0;
+    a.energy[0] = a.w0 * uc + us + 0.5 * ug;
+  }
+}
+
+inline int blocks_for(long n, int threads) {
+  return (int)std::max<long>(1, (n + threads - 1) / threads);
+}
+
+}  // namespace
+
+template <typename T>
+void launch_prep(cudaStream_t s, int N, const double *pos, const double *q,
+                 const Geometry &g, int *pcell, int *gcell, int *pcount,
+                 int *gcount, V4<T> *prel, V4<T> *gfrac, int *err) {
+  k_prep<T><<<blocks_for(N, kThreads), kThreads, 0, s>>>(
+      N, pos, q, g, pcell, gcell, pcount, gcount, prel, gfrac, err);
+}
+
+void launch_charge_stats(cudaStream_t s, int N, const double *q,
+                         double *partials, int nparts) {
+  k_charge_stats<<<nparts, kThreads, 0, s>>>(N, q, partials);
+}
+
+void launch_qstats_final(cudaStream_t s, const double *qparts, int nqparts,
+                         double *qstats) {
+  k_qstats_final<<<1, kThreads, 0, s>>>(qparts, nqparts, qstats);
+}
+
+size_t scan_temp_ints(int n) { return (size_t)(n / kScanTile + 2); }
+
+void launch_scan(cudaStream_t s, const int *in, int *out, int n, int *tmp) {
+  int nb = std::max(1, (n + kScanTile - 1) / kScanTile);
+  k_scan_reduce<<<nb, kScanThreads, 0, s>>>(in, n, tmp);
+  k_scan_top<<<1, kScanThreads, 0, s>>>(tmp, nb);
+  k_scan_apply<<<nb, kScanThreads, 0, s>>>(in, n, tmp, nb, out);
+}
+
+void launch_scatter(cudaStream_t s, int N, const int *cell, const int *start,
+                    int *cursor, int *perm) {
+  k_scatter<<<blocks_for(N, kThreads), kThreads, 0, s>>>(N, cell, start,
+                                                         cursor, perm);
+}
+
+void launch_segment_sort(cudaStream_t s, int ncell, const int *start,
+                         int *perm) {
+  k_segment_sort<<<blocks_for(ncell, kThreads), kThreads, 0, s>>>(ncell, start,
+                                                                  perm);
+}
+
+template <typename T>
+void launch_gather(cudaStream_t s, int N, const int *perm, const V4<T> *src,
+                   const int *cell, V4<T> *dst, int *cell_sorted, int *inv) {
+  k_gather<T><<<blocks_for(N, kThreads), kThreads, 0, s>>>(
+      N, perm, src, cell, dst, cell_sorted, inv);
+}
+
+int combine_blocks(int N) { return blocks_for(N, kThreads); }
+
+template <typename T>
+void launch_combine(cudaStream_t s, const CombineArgs &a, const int *pinv,
+                    const int *ginv, const V4<T> *pout, const V4<T> *gout,
+                    int nblocks) {
+  k_combine<T><<<nblocks, kThreads, 0, s>>>(a, pinv, ginv, pout, gout);
+}
+
+void launch_energy_total(cudaStream_t s, const EnergyArgs &a) {
+  k_energy_total<<<1, kThreads, 0, s>>>(a);
+}
+
+#define MSM_INST_ATOMS(T)                                                     \
+  template void launch_prep<T>(cudaStream_t, int, const double *,            \
+                               const double *, const Geometry &, int *,      \
+                               int *, int *, int *, V4<T> *, V4<T> *, int *); \
+  template void launch_gather<T>(cudaStream_t, int, const int *,             \
+                                 const V4<T> *, const int *, V4<T> *, int *,  \
+                                 int *);                                      \
+  template void launch_combine<T>(cudaStream_t, const CombineArgs &,         \
+                                  const int *, const int *, const V4<T> *,    \
+                                  const V4<T> *, int);
+MSM_INST_ATOMS(float)
+MSM_INST_ATOMS(double)
+
+}  // namespace msm

@@ -1,0 +1,305 @@
+// Grid transfer kernels between atoms and the finest grid, and between
+// levels. Grids are unpadded, periodic, x-major with z fastest.
+//
+// B-spline convention (code/forcefield1.c:348-368, :609-622): an atom at grid
+// coordinate u = M s, m = floor(u), t = u - m contributes
+// q * Q_nu(n + nu/2 + t) to grid point m - n for n in [-nu/2, nu/2), per axis.
+#include <algorithm>
+
+#include "kernels.h"
+
+namespace msm {
+namespace {
+
+constexpr int kThreads = 256;
+
+// Q_nu(i + t) for 0 <= i < nu (piece reflection of code/forcefield1.c:612)
+template <typename T, int NU>
+__device__ __forceinline__ T bspline(const SplineConsts<T> &sc, int i, T t) {
+  if (i >= NU / 2) {
+    i = NU - 1 - i;
+    t = T(1) - t;
+  }
+  const T *c = sc.Q + i * NU;
+  T v = c[NU - 1];
+#pragma unroll
+  for (int k = NU - 2; k >= 0; --k) v = c[k] + t * v;
+  return v;
+}
+
+// value and d/dt (code/forcefield1.c:624-637)
+template <typename T, int NU>
+__device__ __forceinline__ T bspline_d(const SplineConsts<T> &sc, int i, T t,
+                                       T &d) {
+  T sign = T(1);
+  if (i >= NU / 2) {
+    i = NU - 1 - i;
+    t = T(1) - t;
+    sign = T(-1);
+  }
+  const T *c = sc.Q + i * NU;
+  T v = c[NU - 1], dv = T(0);
+#pragma unroll
+  for (int k = NU - 2; k >= 0; --k) {
+    dv = v + t * dv;
+    v = c[k] + t * v;
+  }
+  d = sign * dv;
+  return v;
+}
+
+// Anterpolation as an atomic-free gather: grid point g collects from the
+// atoms of cells g + n, n in [-nu/2, nu/2)^3, in cell order (atoms within a
+// cell ordered by index), so the sum order is fixed.
+template <typename T, int NU>
+__global__ void __launch_bounds__(kThreads)
+k_anterpolate(int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
+              const int *__restrict__ start, SplineConsts<T> sc,
+              T *__restrict__ grid) {
+  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)M0 * M1 * M2) return;
+  const int gz = idx % M2, gy = (idx / M2) % M1, gx = idx / ((long)M1 * M2);
+  Acc<T> acc;
+  acc.zero();
+  for (int a = 0; a < NU; ++a) {
+    const int mx = pwrap(gx + a - NU / 2, M0);
+    for (int b = 0; b < NU; ++b) {
+      const int my = pwrap(gy + b - NU / 2, M1);
+      const long col = ((long)mx * M1 + my) * M2;
+      T part = T(0);
+      for (int c = 0; c < NU; ++c) {
+        const int mz = pwrap(gz + c - NU / 2, M2);
+        const int e = start[col + mz + 1];
+        for (int j = start[col + mz]; j < e; ++j) {
+          const V4<T> at = atoms[j];
+          part += at.w * bspline<T, NU>(sc, a, at.x) *
+                  bspline<T, NU>(sc, b, at.y) * bspline<T, NU>(sc, c, at.z);
+        }
+      }
+      acc.add(part);
+    }
+  }
+  grid[idx] = acc.value();
+}
+
+// Field and potential at each atom (code/forcefield1.c:570-607), separable:
+// z sums first, then y, then x. Output E in Cartesian components
+// (E = A^-T (M * grad_u)) and phi_long.
+template <typename T, int NU>
+__global__ void __launch_bounds__(kThreads)
+k_interpolate(int N, int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
+              const int *__restrict__ cell, const T *__restrict__ grid,
+              SplineConsts<T> sc, Geometry g, V4<T> *__restrict__ out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  const V4<T> at = atoms[k];
+  const int c = cell[k];
+  const int mz = c % M2, my = (c / M2) % M1, mx = c / (M1 * M2);
+  T wx[NU], dx[NU], wy[NU], dy[NU], wz[NU], dz[NU];
+#pragma unroll
+  for (int i = 0; i < NU; ++i) {
+    wx[i] = bspline_d<T, NU>(sc, i, at.x, dx[i]);
+    wy[i] = bspline_d<T, NU>(sc, i, at.y, dy[i]);
+    wz[i] = bspline_d<T, NU>(sc, i, at.z, dz[i]);
+  }
+  int zi[NU];
+#pragma unroll
+  for (int i = 0; i < NU; ++i) zi[i] = pwrap(mz - (i - NU / 2), M2);
+  T phi = 0, ex = 0, ey = 0, ez = 0;
+  for (int a = 0; a < NU; ++a) {
+    const int gx = pwrap(mx - (a - NU / 2), M0);
+    T t00 = 0, t10 = 0, t01 = 0;
+    for (int b = 0; b < NU; ++b) {
+      const int gy = pwrap(my - (b - NU / 2), M1);
+      const T *row = grid + ((long)gx * M1 + gy) * M2;
+      T s0 = 0, s1 = 0;
+#pragma unroll
+      for (int i = 0; i < NU; ++i) {
+        const T e = row[zi[i]];
+        s0 += wz[i] * e;
+        s1 += dz[i] * e;
+      }
+      t00 += wy[b] * s0;
+      t10 += dy[b] * s0;
+      t01 += wy[b] * s1;
+    }
+    phi += wx[a] * t00;
+    ex -= dx[a] * t00;
+    ey -= wx[a] * t10;
+    ez -= wx[a] * t01;
+  }
+  const double gxv = (double)ex * M0, gyv = (double)ey * M1, gzv = (double)ez * M2;
+  V4<T> r;
+  r.x = (T)(g.Ai[0] * gxv + g.Ai[3] * gyv + g.Ai[6] * gzv);
+  r.y = (T)(g.Ai[1] * gxv + g.Ai[4] * gyv + g.Ai[7] * gzv);
+  r.z = (T)(g.Ai[2] * gxv + g.Ai[5] * gyv + g.Ai[8] * gzv);
+  r.w = phi;
+  out[k] = r;
+}
+
+struct TwoScale {
+  double J[11];
+};
+
+// q^{l+1}_m = sum_n J_n q^l_{2m+n}, n in [-nu/2, nu/2]^3
+// (code/forcefield1.c:401-477)
+template <typename T, int NU>
+__global__ void __launch_bounds__(kThreads)
+k_restrict(int F0, int F1, int F2, const T *__restrict__ fine,
+           T *__restrict__ coarse, TwoScale js) {
+  const int C0 = F0 / 2, C1 = F1 / 2, C2 = F2 / 2;
+  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)C0 * C1 * C2) return;
+  const int z = idx % C2, y = (idx / C2) % C1, x = idx / ((long)C1 * C2);
+  T J[NU + 1];
+#pragma unroll
+  for (int i = 0; i <= NU; ++i) J[i] = (T)js.J[i];
+  T acc = 0;
+  for (int a = 0; a <= NU; ++a) {
+    const int fx = pwrap(2 * x + a - NU / 2, F0);
+    T ay = 0;
+    for (int b = 0; b <= NU; ++b) {
+      const int fy = pwrap(2 * y + b - NU / 2, F1);
+      const T *row = fine + ((long)fx * F1 + fy) * F2;
+      T az = 0;
+#pragma unroll
+      for (int c = 0; c <= NU; ++c) az += J[c] * row[pwrap(2 * z + c - NU / 2, F2)];
+      ay += J[b] * az;
+    }
+    acc += J[a] * ay;
+  }
+  coarse[idx] = acc;
+}
+
+// e^l_x += sum over (m, n) with 2m + n = x (mod M) of J_n e^{l+1}_m
+// (transpose of the restriction; code/forcefield1.c:530-567)
+template <typename T, int NU>
+__global__ void __launch_bounds__(kThreads)
+k_prolong(int F0, int F1, int F2, const T *__restrict__ coarse,
+          T *__restrict__ fine, TwoScale js) {
+  const int C0 = F0 / 2, C1 = F1 / 2, C2 = F2 / 2;
+  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)F0 * F1 * F2) return;
+  const int z = idx % F2, y = (idx / F2) % F1, x = idx / ((long)F1 * F2);
+  T acc = 0;
+  for (int a = 0; a <= NU; ++a) {
+    const int n = a - NU / 2;
+    if (((x - n) & 1) != 0) continue;
+    const int cx = pwrap((x - n) / 2, C0);
+    T ay = 0;
+    for (int b = 0; b <= NU; ++b) {
+      const int nb = b - NU / 2;
+      if (((y - nb) & 1) != 0) continue;
+      const int cy = pwrap((y - nb) / 2, C1);
+      const T *row = coarse + ((long)cx * C1 + cy) * C2;
+      T az = 0;
+      for (int c = 0; c <= NU; ++c) {
+        const int nc = c - NU / 2;
+        if (((z - nc) & 1) != 0) continue;
+        az += (T)js.J[c] * row[pwrap((z - nc) / 2, C2)];
+      }
+      ay += (T)js.J[b] * az;
+    }
+    acc += (T)js.J[a] * ay;
+  }
+  fine[idx] += acc;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_grid_dot(long n, const T *__restrict__ a, const T *__restrict__ b,
+           double *partials) {
+  __shared__ double sh[kThreads];
+  double acc = 0.;
+  for (long i = (long)blockIdx.x * kThreads + threadIdx.x; i < n;
+       i += (long)gridDim.x * kThreads)
+    acc += (double)a[i] * (double)b[i];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = kThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = sh[0];
+}
+
+inline int blocks_for(long n) {
+  return (int)std::max<long>(1, (n + kThreads - 1) / kThreads);
+}
+
+#define MSM_NU_SWITCH(nu, CALL)     \
+  switch (nu) {                     \
+    case 4: { constexpr int NU = 4; CALL; } break;  \
+    case 6: { constexpr int NU = 6; CALL; } break;  \
+    case 8: { constexpr int NU = 8; CALL; } break;  \
+    default: { constexpr int NU = 10; CALL; } break; \
+  }
+
+}  // namespace
+
+template <typename T>
+void launch_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
+                        const int *cell_start, const SplineConsts<T> &sc,
+                        T *grid) {
+  long n = (long)M[0] * M[1] * M[2];
+  MSM_NU_SWITCH(sc.nu, (k_anterpolate<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
+                           M[0], M[1], M[2], atoms, cell_start, sc, grid)));
+}
+
+template <typename T>
+void launch_interpolate(cudaStream_t s, int N, const int M[3],
+                        const V4<T> *atoms, const int *cell_sorted,
+                        const T *grid, const SplineConsts<T> &sc,
+                        const Geometry &g, V4<T> *out) {
+  MSM_NU_SWITCH(sc.nu, (k_interpolate<T, NU><<<blocks_for(N), kThreads, 0, s>>>(
+                           N, M[0], M[1], M[2], atoms, cell_sorted, grid, sc, g, out)));
+}
+
+template <typename T>
+void launch_restrict(cudaStream_t s, const int Mf[3], const T *fine,
+                     T *coarse, const double *J, int nu) {
+  TwoScale js;
+  for (int i = 0; i <= nu; ++i) js.J[i] = J[i];
+  long n = (long)(Mf[0] / 2) * (Mf[1] / 2) * (Mf[2] / 2);
+  MSM_NU_SWITCH(nu, (k_restrict<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
+                        Mf[0], Mf[1], Mf[2], fine, coarse, js)));
+}
+
+template <typename T>
+void launch_prolong_add(cudaStream_t s, const int Mf[3], const T *coarse,
+                        T *fine, const double *J, int nu) {
+  TwoScale js;
+  for (int i = 0; i <= nu; ++i) js.J[i] = J[i];
+  long n = (long)Mf[0] * Mf[1] * Mf[2];
+  MSM_NU_SWITCH(nu, (k_prolong<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
+                        Mf[0], Mf[1], Mf[2], coarse, fine, js)));
+}
+
+int grid_dot_blocks(size_t n) {
+  return (int)std::min<long>(1024, std::max<long>(1, ((long)n + kThreads - 1) / kThreads));
+}
+
+template <typename T>
+void launch_grid_dot(cudaStream_t s, size_t n, const T *a, const T *b,
+                     double *partials, int nparts) {
+  k_grid_dot<T><<<nparts, kThreads, 0, s>>>((long)n, a, b, partials);
+}
+
+#define MSM_INST_GRID(T)                                                       \
+  template void launch_anterpolate<T>(cudaStream_t, const int *,              \
+                                      const V4<T> *, const int *,             \
+                                      const SplineConsts<T> &, T *);          \
+  template void launch_interpolate<T>(cudaStream_t, int, const int *,         \
+                                      const V4<T> *, const int *, const T *,  \
+                                      const SplineConsts<T> &,                \
+                                      const Geometry &, V4<T> *);             \
+  template void launch_restrict<T>(cudaStream_t, const int *, const T *, T *, \
+                                   const double *, int);                      \
+  template void launch_prolong_add<T>(cudaStream_t, const int *, const T *,   \
+                                      T *, const double *, int);              \
+  template void launch_grid_dot<T>(cudaStream_t, size_t, const T *,           \
+                                   const T *, double *, int);
+MSM_INST_GRID(float)
+MSM_INST_GRID(double)
+
+}  // namespace msm

@@ -1,0 +1,120 @@
+// Short-range softened pair sum (code/forcefield1.c:240-321 over the
+// neighbour list of code/forcefield0.c:21-164), rebuilt on the GPU each call.
+//
+// Atoms are sorted by pair cell (cells at least a0/2 thick). Each atom i
+// sweeps a host-built list of neighbour-cell instances: a cell offset d and
+// the Cartesian offset of that cell's origin relative to i's home-cell origin,
+// periodic image included. Positions are stored relative to their own cell
+// origin, so r_j - r_i = (rel_j + shift_d) - rel_i is formed from small
+// numbers and stays accurate in FP32. Every (j != i, image) with r < a0 is
+// summed, each unordered pair once from each side (gather form: no atomics,
+// per-atom potential and force fall out directly).
+//
+// V(r) = 1/r - tau(r^2/a0^2 - 1)/a0,  F_i = q_i q_j (-1/r^3 - 2 tau'(s)/a0^3) r.
+#include "kernels.h"
+
+namespace msm {
+namespace {
+
+constexpr int kPairThreads = 128;
+
+template <typename T, int NU, bool COMPENSATE>
+__global__ void __launch_bounds__(kPairThreads)
+k_pair(int N, const V4<T> *__restrict__ ps, const int *__restrict__ pcs,
+       const int *__restrict__ start, int nc0, int nc1, int nc2,
+       const CellOffset<T> *__restrict__ off, int noff, PairConsts<T> pc,
+       V4<T> *__restrict__ out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  const V4<T> ai = ps[k];
+  const int c = pcs[k];
+  const int cz = c % nc2, cy = (c / nc2) % nc1, cx = c / (nc1 * nc2);
+  Acc<T> fx, fy, fz, ph;
+  fx.zero();
+  fy.zero();
+  fz.zero();
+  ph.zero();
+  for (int o = 0; o < noff; ++o) {
+    const CellOffset<T> co = off[o];
+    const int ux = pwrap(cx + co.d[0], nc0), uy = pwrap(cy + co.d[1], nc1),
+              uz = pwrap(cz + co.d[2], nc2);
+    const int cw = (ux * nc1 + uy) * nc2 + uz;
+    const int b = start[cw], e = start[cw + 1];
+    const T sx = co.shift[0] - ai.x, sy = co.shift[1] - ai.y,
+            sz = co.shift[2] - ai.z;
+    T px = 0, py = 0, pz = 0, pp = 0;
+    for (int j = b; j < e; ++j) {
+      const V4<T> aj = ps[j];
+      const T dx = aj.x + sx, dy = aj.y + sy, dz = aj.z + sz;
+      const T r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 < pc.a02 && j != k) {
+        const T s = r2 * pc.inv_a02 - T(1);
+        T ts = pc.tau[NU - 1], t1 = T(0);
+#pragma unroll
+        for (int m = NU - 2; m >= 0; --m) {
+          t1 = ts + s * t1;
+          ts = pc.tau[m] + s * ts;
+        }
+        const T rinv = rsqrt_t<T>(r2);
+        pp += aj.w * (rinv - ts * pc.inv_a0);
+        const T cf = aj.w * (-rinv * rinv * rinv - t1 * pc.two_inv_a03);
+        px += cf * dx;
+        py += cf * dy;
+        pz += cf * dz;
+      }
+    }
+    if (COMPENSATE) {
+      fx.add(px);
+      fy.add(py);
+      fz.add(pz);
+      ph.add(pp);
+    } else {
+      fx.s += px;
+      fy.s += py;
+      fz.s += pz;
+      ph.s += pp;
+    }
+  }
+  V4<T> r;
+  r.x = ai.w * fx.value();
+  r.y = ai.w * fy.value();
+  r.z = ai.w * fz.value();
+  r.w = ph.value();
+  out[k] = r;
+}
+
+template <typename T, int NU>
+void launch_nu(cudaStream_t s, int N, const V4<T> *ps, const int *pcs,
+               const int *start, const Geometry &g, const CellOffset<T> *off,
+               int noff, const PairConsts<T> &pc, V4<T> *out) {
+  int blocks = (N + kPairThreads - 1) / kPairThreads;
+  if (blocks < 1) blocks = 1;
+  k_pair<T, NU, true><<<blocks, kPairThreads, 0, s>>>(
+      N, ps, pcs, start, g.nc[0], g.nc[1], g.nc[2], off, noff, pc, out);
+}
+
+}  // namespace
+
+template <typename T>
+void launch_pair(cudaStream_t s, int N, const V4<T> *ps, const int *pcs,
+                 const int *start, const Geometry &g,
+                 const CellOffset<T> *off, int noff, const PairConsts<T> &pc,
+                 V4<T> *out) {
+  switch (pc.nu) {
+    case 4: launch_nu<T, 4>(s, N, ps, pcs, start, g, off, noff, pc, out); break;
+    case 6: launch_nu<T, 6>(s, N, ps, pcs, start, g, off, noff, pc, out); break;
+    case 8: launch_nu<T, 8>(s, N, ps, pcs, start, g, off, noff, pc, out); break;
+    default: launch_nu<T, 10>(s, N, ps, pcs, start, g, off, noff, pc, out); break;
+  }
+}
+
+template void launch_pair<float>(cudaStream_t, int, const V4<float> *,
+                                 const int *, const int *, const Geometry &,
+                                 const CellOffset<float> *, int,
+                                 const PairConsts<float> &, V4<float> *);
+template void launch_pair<double>(cudaStream_t, int, const V4<double> *,
+                                  const int *, const int *, const Geometry &,
+                                  const CellOffset<double> *, int,
+                                  const PairConsts<double> &, V4<double> *);
+
+}  // namespace msm

@@ -1,0 +1,142 @@
+// Host-side launchers of the MSM kernels. Each launcher enqueues work on the
+// given stream and never synchronises; all pointers are device pointers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace msm {
+
+constexpr int kMaxNeighbourOffsets = 4096;
+
+// Box geometry and binning parameters (FP64)
+struct Geometry {
+  double A[9], Ai[9];  // row-major; columns of A are the box edge vectors
+  int nc[3];           // pair cells per axis
+  int M1[3];           // finest grid dims
+};
+
+// One neighbour-cell instance of the pair sweep: cell offset and the
+// Cartesian offset of its origin relative to the home cell's origin
+// (this includes the periodic image shift).
+template <typename T>
+struct CellOffset {
+  int d[3];
+  int pad;
+  T shift[3];
+  T pad2;
+};
+
+// Short-range kernel constants
+template <typename T>
+struct PairConsts {
+  T a02, inv_a02, inv_a0, two_inv_a03;
+  T tau[16];
+  int nu;
+};
+
+// B-spline piece coefficients for the device
+template <typename T>
+struct SplineConsts {
+  T Q[5 * 10];
+  int nu;
+};
+
+// ---- atoms: binning and sorting (k_atoms.cu) ----
+template <typename T>
+void launch_prep(cudaStream_t s, int N, const double *pos, const double *q,
+                 const Geometry &g, int *pcell, int *gcell, int *pcount,
+                 int *gcount, V4<T> *prel, V4<T> *gfrac, int *err);
+void launch_charge_stats(cudaStream_t s, int N, const double *q,
+                         double *partials, int nparts);
+// exclusive scan of n ints into out[0..n] (out[n] = total)
+size_t scan_temp_ints(int n);
+void launch_scan(cudaStream_t s, const int *in, int *out, int n, int *tmp);
+void launch_scatter(cudaStream_t s, int N, const int *cell, const int *start,
+                    int *cursor, int *perm);
+void launch_segment_sort(cudaStream_t s, int ncell, const int *start,
+                         int *perm);
+template <typename T>
+void launch_gather(cudaStream_t s, int N, const int *perm, const V4<T> *src,
+                   const int *cell, V4<T> *dst, int *cell_sorted, int *inv);
+struct CombineArgs {
+  int N;
+  double w0, coeff1, coeff2, gamma0_over_a0;
+  const double *q;
+  const double *qstats;  // [qsum, q2sum] after the final reduction
+  int nqparts;
+  const double *qparts;
+  double *force;     // N*3 or NULL
+  double *phi;       // N or NULL
+  double *epart;     // per-block partial sums of w0 * q_i * phi_short_i / 2
+};
+template <typename T>
+void launch_combine(cudaStream_t s, const CombineArgs &a, const int *pinv,
+                    const int *ginv, const V4<T> *pout, const V4<T> *gout,
+                    int nblocks);
+int combine_blocks(int N);
+struct EnergyArgs {
+  const double *qparts;  // nqparts x 2
+  int nqparts;
+  const double *short_parts;
+  int nshort;
+  const double *grid_parts;
+  int ngrid;
+  double w0, coeff1, coeff2, gamma0_over_a0;
+  double *energy;  // device scalar
+  double *qstats;  // device [qsum, q2sum]
+};
+void launch_energy_total(cudaStream_t s, const EnergyArgs &a);
+void launch_qstats_final(cudaStream_t s, const double *qparts, int nqparts,
+                         double *qstats);
+
+// ---- short-range pair sum (k_pair.cu) ----
+template <typename T>
+void launch_pair(cudaStream_t s, int N, const V4<T> *pos_sorted,
+                 const int *cell_sorted, const int *cell_start,
+                 const Geometry &g, const CellOffset<T> *offsets, int noff,
+                 const PairConsts<T> &pc, V4<T> *out);
+
+// ---- grid transfers (k_grid.cu) ----
+template <typename T>
+void launch_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
+                        const int *cell_start, const SplineConsts<T> &sc,
+                        T *grid);
+template <typename T>
+void launch_interpolate(cudaStream_t s, int N, const int M[3],
+                        const V4<T> *atoms, const int *cell_sorted,
+                        const T *grid, const SplineConsts<T> &sc,
+                        const Geometry &g, V4<T> *out);
+template <typename T>
+void launch_restrict(cudaStream_t s, const int Mf[3], const T *fine,
+                     T *coarse, const double *J, int nu);
+template <typename T>
+void launch_prolong_add(cudaStream_t s, const int Mf[3], const T *coarse,
+                        T *fine, const double *J, int nu);
+template <typename T>
+void launch_grid_dot(cudaStream_t s, size_t n, const T *a, const T *b,
+                     double *partials, int nparts);
+int grid_dot_blocks(size_t n);
+
+// ---- per-level direct stencil (k_stencil.cu) ----
+struct StencilShape {
+  int M[3];   // grid dims
+  int S[3];   // stencil dims
+  int P[3];   // padded input dims (P[2] rounded up for 16-byte rows)
+};
+template <typename T>
+void launch_pad(cudaStream_t s, const StencilShape &sh, const T *q, T *padded);
+template <typename T>
+void launch_stencil(cudaStream_t s, const StencilShape &sh, const T *padded,
+                    const T *kh, T weight, T *e, int variant);
+int stencil_padded_z(int Mz, int Sz);
+
+// ---- top-level FFT solve (k_fft.cu) ----
+bool top_solve_supported(const int M[3]);
+template <typename T>
+void launch_top_solve(cudaStream_t s, const int M[3], const T *q,
+                      const double *khat, double weight, double2 *buf0,
+                      double2 *buf1, T *e);
+
+}  // namespace msm

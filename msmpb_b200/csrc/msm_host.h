@@ -1,0 +1,59 @@
+// Host-side (FP64) setup of the MSM evaluation: parameters, coefficient
+// tables and per-level stencils that the device kernels consume.
+#pragma once
+
+#include <vector>
+
+namespace msm {
+
+constexpr int kMaxLevels = 10;  // FF's time_* arrays hold 10 levels
+
+struct Params {
+  int N = 0;
+  double A[3][3] = {}, Ai[3][3] = {}, detA = 0;
+  double estErr = 1e-3;
+  int nu = 0, L = 0;
+  int top[3] = {0, 0, 0};
+  double a0 = 0;
+  double aCut[kMaxLevels + 2] = {};
+  double relCutoff = 0;
+  int nLim = 0;
+  bool fft = true;
+};
+
+struct Tables {
+  Params p;
+  double tau[16] = {};       // softening polynomial, degree nu-1
+  double Q[5 * 10] = {};     // B-spline pieces: Q[j*nu+k] = [t^k] Q_nu(j+t)
+  double J[11] = {};         // two-scale stencil J[n + nu/2]
+  double gamma0 = 0;         // tau(-1) = gamma(0)
+  double coeff1 = 0, coeff2 = 0;
+  int grid[kMaxLevels + 2][3] = {};   // level-l grid dims
+  int sten[kMaxLevels + 2][3] = {};   // level-l stencil dims (l < L)
+  std::vector<double> omegap[kMaxLevels + 2][3];
+  std::vector<double> cL[3];
+  std::vector<double> khat[kMaxLevels + 2];  // l<L: stencil; L: multiplier
+};
+
+// Matrix helpers (reference code/forcefield0.c:709-724)
+double invert3(const double a[3][3], double ai[3][3]);
+
+// Parameter selection exactly as FF_build (code/forcefield0.c:271-367).
+// Arguments use the reference's -1 = auto convention. Returns false when the
+// parameters are unusable (error code in *err).
+bool select_params(Params &p, int N, const double *q, const double edges[3][3],
+                   double cutoff, int nu, int L, const int top[3],
+                   double estErr, bool fft, int *err);
+
+// Error model (code/forcefield0.c:521-587)
+double err_model(const Params &p, const double *q, int nu);
+double delta_f(const Params &p, const double *q);
+
+// Quasi-interpolation weights omega'_l and c_L only (code/forcefield0.c:726-767);
+// needs t.p, t.Q and t.grid.
+void build_omegap_tables(Tables &t);
+
+// All tables for a parameter set (code/forcefield0.c:369-467, :598-675).
+void build_tables(Tables &t, const Params &p);
+
+}  // namespace msm

@@ -1,0 +1,155 @@
+"""GPU parity: the CUDA library through its C ABI against the reference's own
+outputs (golden fixtures made by the patched reference build) and against
+the CPU oracle run live on the same inputs.
+
+Tolerances (per-case, stated below): the FP64 GPU form must agree with the
+FP64 reference to ~1e-10; the mixed form (FP32 bulk, FP64 FFT and sums) to
+the FP32 rounding level, which sits orders of magnitude below the method's
+own error (checked separately against the high-accuracy .acc/.pot data).
+"""
+import numpy as np
+import pytest
+
+from golden_cases import load, names, params, rel_rms
+from msmpb_b200 import systems
+from msmpb_b200.forcefield import ForceField
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+# (energy rel, force metric, potential rel-rms)
+TOL = {"fp64": (1e-11, 1e-10, 1e-10), "mixed": (2e-6, 2e-5, 2e-5)}
+
+
+def fref(q, edges):
+    """Force scale of the reference's error metric (code/msmpb.c:271-273)."""
+    n = len(q)
+    return (q @ q / n) / (abs(np.linalg.det(edges)) / n) ** (2.0 / 3.0)
+
+
+def force_err(f, g, q, edges):
+    """deltaF / Fref of code/msmpb.c:303-306 between two force arrays."""
+    return np.sqrt(((f - g) ** 2).sum() / len(q)) / fref(q, edges)
+
+
+def make_ff(d, precision):
+    p = params(d)
+    return ForceField(d["q"], d["pos"], d["edges"], cutoff=p["cutoff"],
+                      order=p["nu"], levels=p["levels"], top_grid=p["top_grid"],
+                      precision=precision)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", [n for n in names() if not n.startswith("Box44")])
+def test_golden(case, precision):
+    d = load(case)
+    ff = make_ff(d, precision)
+    e, f, phi = ff.energy(d["pos"], potentials=True)
+    te, tf, tp = TOL[precision]
+    scale = max(abs(float(d["energy"])), 1e-300)
+    assert abs(e - float(d["energy"])) / scale < te
+    assert force_err(f, d["force"], d["q"], d["edges"]) < tf
+    if "phi" in d:
+        assert rel_rms(phi, d["phi"]) < tp
+    # U = 1/2 sum q_i phi_i holds for the quadratic form
+    assert abs(0.5 * d["q"] @ phi - e) / scale < te * 10
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_box44_table2(precision):
+    """Box44 (65,850 atoms), L=2, M=18, a0=12, nu=6: the published Table II
+    energy (results/TableII.json) and the reference's force checksum."""
+    d = load("Box44_L2_M18_a12_nu6")
+    ff = make_ff(d, precision)
+    e, f = ff.energy(d["pos"])
+    te, _, _ = TOL[precision]
+    assert abs(e - (-13831.986893278543)) / 13831.98 < te
+    cs = d["force_checksum"]
+    assert abs((f ** 2).sum() - cs[1]) / cs[1] < (1e-10 if precision == "fp64" else 1e-5)
+
+
+def _oracle_case(name):
+    q, pos, edges, kw = systems.config(name)
+    return q, pos, edges, kw
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("name", ["water300", "rocksalt4096"])
+def test_synthetic_vs_oracle(name, precision):
+    q, pos, edges, kw = _oracle_case(name)
+    o = Oracle(q, edges, cutoff=kw.get("cutoff", -1), nu=kw.get("order", -1),
+               levels=kw.get("levels", -1), top_grid=kw.get("top_grid"))
+    eo, fo, po = o.energy(pos)
+    ff = ForceField(q, pos, edges, **kw, precision=precision)
+    assert (ff.cutoff, ff.order, ff.levels, ff.top_grid) == (o.cutoff, o.nu, o.levels, o.top_grid)
+    e, f, phi = ff.energy(pos, potentials=True)
+    te, tf, tp = TOL[precision]
+    assert abs(e - eo) / abs(eo) < te
+    assert force_err(f, fo, q, edges) < tf
+    assert rel_rms(phi, po) < tp
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_three_levels_truncated_stencil(precision):
+    """L=3 with a truncated level-1 stencil (sd < M) and a full-period
+    level-2 stencil (sd = M)."""
+    q, pos, edges = systems.water(8000, 62.0, 11)
+    kw = dict(cutoff=9.0, order=6, levels=3, top_grid=6)
+    o = Oracle(q, edges, cutoff=9.0, nu=6, levels=3, top_grid=6)
+    ff = ForceField(q, pos, edges, **kw, precision=precision)
+    s1 = ff.khat(1).shape
+    assert s1[0] < 24 and ff.khat(2).shape[0] == 12
+    eo, fo, po = o.energy(pos)
+    e, f, phi = ff.energy(pos, potentials=True)
+    te, tf, tp = TOL[precision]
+    assert abs(e - eo) / abs(eo) < te
+    assert force_err(f, fo, q, edges) < tf
+    assert rel_rms(phi, po) < tp
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_level_weights(precision):
+    """Weighted evaluation is linear in each level weight (the oracle's
+    definition; the reference only defines unit weights)."""
+    d = load("spceN900_L3_M6_a8_nu8")
+    p = params(d)
+    o = Oracle(d["q"], d["edges"], cutoff=p["cutoff"], nu=p["nu"],
+               levels=p["levels"], top_grid=p["top_grid"])
+    w = np.array([0.5, 1.5, -0.25, 2.0])
+    eo, fo, po = o.energy(d["pos"], weight=w)
+    ff = make_ff(d, precision)
+    e, f, phi = ff.energy(d["pos"], weights=w, potentials=True)
+    te, tf, tp = TOL[precision]
+    assert abs(e - eo) / abs(eo) < te * 10
+    assert force_err(f, fo, d["q"], d["edges"]) < tf
+    assert rel_rms(phi, po) < tp
+
+
+def test_repeat_and_charge_update():
+    """Repeated calls give identical results; charge edits between calls
+    are seen (FF_new keeps the caller's pointer, code/forcefield0.c:172)."""
+    d = load("spceN600_M20_a8_nu6")
+    ff = make_ff(d, "mixed")
+    e1, f1 = ff.energy(d["pos"])
+    e2, f2 = ff.energy(d["pos"])
+    assert e1 == e2 and np.array_equal(f1, f2)
+    q2 = d["q"] * 0.5
+    e3, _ = ff.energy(d["pos"], charges=q2)
+    assert abs(e3 - 0.25 * e1) / abs(e1) < 1e-5
+
+
+def test_rebuild_box_change():
+    """FF_rebuild with a new box keeps the parameters and matches a fresh
+    build with those parameters."""
+    d = load("spceN600_M20_a8_nu6")
+    p = params(d)
+    ff = make_ff(d, "fp64")
+    edges2 = d["edges"] * 1.03
+    pos2 = d["pos"] * 1.03
+    ff.rebuild(edges2, pos2)
+    e, f = ff.energy(pos2)
+    o = Oracle(d["q"], edges2, cutoff=p["cutoff"], nu=p["nu"], levels=1,
+               top_grid=p["top_grid"])
+    eo, fo, _ = o.energy(pos2)
+    assert abs(e - eo) / abs(eo) < 1e-10
+    assert force_err(f, fo, d["q"], edges2) < 1e-10
