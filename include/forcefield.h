@@ -93,6 +93,7 @@ typedef struct FF {
   int last_error;
   int precision;
   int device;
+  int timing;                 /* fill time_* from per-phase CUDA events */
   double margin;
 } FF;
 

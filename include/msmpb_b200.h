@@ -70,6 +70,19 @@ int FF_phase_times(FF *ff, double *ms, int n);
 /* Number of kernel launches one evaluation issues (for accounting). */
 int FF_kernel_launches(FF *ff);
 
+/* Per-level direct-stencil kernel time (ms) of the last evaluation run with
+ * timing on, levels 1..maxLevel-1. Returns the number of entries written. */
+int FF_stencil_times(FF *ff, double *ms, int n);
+
+/* Timing on (default; MSMPB_TIMING=0 in the environment turns it off):
+ * host-API evaluations launch eagerly with per-phase events and fill the
+ * time_* members. Off: the evaluation replays a captured CUDA graph. */
+void FF_set_timing(FF *ff, int enabled);
+
+/* Measured FP32 FMA throughput of `device` in TFLOP/s: a pure-FFMA kernel
+ * on every SM for about `milliseconds` (the FP32-pipe roofline peak). */
+double msmpb_measure_fp32_tflops(int device, int milliseconds);
+
 #ifdef __cplusplus
 }
 #endif

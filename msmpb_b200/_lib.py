@@ -38,6 +38,7 @@ EXPORTED = [
     "FF_last_error", "FF_error_string", "FF_set_precision",
     "FF_get_precision", "FF_set_device", "FF_energy_potentials",
     "FF_energy_device", "FF_sync", "FF_phase_times", "FF_kernel_launches",
+    "FF_stencil_times", "FF_set_timing", "msmpb_measure_fp32_tflops",
 ]
 
 _lib = None
@@ -70,7 +71,7 @@ class FFStruct(C.Structure):
         ("time_padding", C.c_double * 10),
         ("dev", C.c_void_p), ("host_state", C.c_void_p),
         ("last_error", C.c_int), ("precision", C.c_int), ("device", C.c_int),
-        ("margin", C.c_double),
+        ("timing", C.c_int), ("margin", C.c_double),
     ]
 
 
@@ -117,6 +118,9 @@ def load():
         "FF_sync": (C.c_int, [P]),
         "FF_phase_times": (C.c_int, [P, _dp, C.c_int]),
         "FF_kernel_launches": (C.c_int, [P]),
+        "FF_stencil_times": (C.c_int, [P, _dp, C.c_int]),
+        "FF_set_timing": (None, [P, C.c_int]),
+        "msmpb_measure_fp32_tflops": (C.c_double, [C.c_int, C.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -14,6 +14,8 @@
 // replayed; the graph is re-captured only when pointers or weights change.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -28,6 +30,7 @@ struct FFDevice {
   virtual int sync() = 0;
   virtual int phase_times(double *ms, int n) = 0;
   virtual int launches() = 0;
+  virtual int level_times(double *ms, int n) = 0;
 };
 
 namespace msm {
@@ -86,20 +89,51 @@ class Plan : public FFDevice {
   int sync() override;
   int phase_times(double *ms, int n) override;
   int launches() override { return nlaunch_; }
+  // stencil kernel time per level of the last timed evaluation
+  int level_times(double *ms, int n) override {
+    if (!timed_) return 0;
+    cudaStreamSynchronize(stream_);
+    int m = 0;
+    for (int l = 1; l < L_ && m < n; ++l) {
+      float t = 0;
+      cudaEventElapsedTime(&t, lev_ev_[l][0], lev_ev_[l][1]);
+      ms[m++] = t;
+    }
+    cudaGetLastError();
+    return m;
+  }
 
  private:
   int set_tables(const Tables &t);
+  int launch_graph(const EvalRequest &r, cudaStream_t s, const double *pos,
+                   const double *q, double *force, double *phi, double *edev);
   int enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
               const double *q, double *force, double *phi, double *energy);
+  // Phase boundary: optional event, and with MSMPB_DEBUG_SYNC=1 (eager
+  // launches only) a synchronising check that names the failing phase.
   void mark(cudaStream_t s, int phase, bool timing) {
+    if (debug_sync_ && timing) {
+      cudaError_t e = cudaStreamSynchronize(s);
+      if (e == cudaSuccess) e = cudaGetLastError();
+      if (e != cudaSuccess)
+        std::fprintf(stderr, "msmpb_b200: CUDA error before phase %d: %s\n",
+                     phase, cudaGetErrorString(e));
+    }
     if (timing) cudaEventRecord(ev_[phase], s);
   }
+  bool debug_sync_ = std::getenv("MSMPB_DEBUG_SYNC") != nullptr;
+  // MSMPB_ANTERP=simple selects the one-point-per-thread anterpolation
+  int anterp_variant_ = [] {
+    const char *v = std::getenv("MSMPB_ANTERP");
+    return (v && v[0] == 's') ? 1 : 0;
+  }();
 
   int device_ = 0;
   cudaStream_t stream_ = nullptr;
   int N_ = 0, L_ = 0, nu_ = 0;
   int grid_[kMaxLevels + 2][3] = {};
   StencilShape sh_[kMaxLevels + 2] = {};
+  StencilTile tile_[kMaxLevels + 2] = {};
   Geometry geom_{};
   PairConsts<T> pc_{};
   SplineConsts<T> sc_{};
@@ -132,6 +166,7 @@ class Plan : public FFDevice {
   GraphKey key_{};
   bool have_graph_ = false;
   cudaEvent_t ev_[kNumPhases + 1] = {};
+  cudaEvent_t lev_ev_[kMaxLevels + 2][2] = {};
   bool timed_ = false;
   int nlaunch_ = 0;
 };
@@ -142,6 +177,9 @@ Plan<T>::~Plan() {
   if (exec_) cudaGraphExecDestroy(exec_);
   for (auto &e : ev_)
     if (e) cudaEventDestroy(e);
+  for (auto &pr : lev_ev_)
+    for (auto &e : pr)
+      if (e) cudaEventDestroy(e);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -151,6 +189,8 @@ int Plan<T>::init(const Tables &t, int device) {
   MSM_CUDA_TRY(cudaSetDevice(device));
   MSM_CUDA_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   for (auto &e : ev_) MSM_CUDA_TRY(cudaEventCreate(&e));
+  for (auto &pr : lev_ev_)
+    for (auto &e : pr) MSM_CUDA_TRY(cudaEventCreate(&e));
   const Params &p = t.p;
   N_ = p.N;
   L_ = p.L;
@@ -170,6 +210,8 @@ int Plan<T>::init(const Tables &t, int device) {
   ncp_ = (int)ncell;
   ncg_ = grid_[1][0] * grid_[1][1] * grid_[1][2];
   if (!top_solve_supported(p.top)) return MSMPB_ERR_UNSUPPORTED;
+  top_solve_prepare();
+  anterpolate_prepare<T>();
   int err = set_tables(t);
   if (err) return err;
   // stencil shapes
@@ -180,9 +222,16 @@ int Plan<T>::init(const Tables &t, int device) {
       s.M[k] = grid_[l][k];
       s.S[k] = t.sten[l][k];
     }
-    s.P[0] = s.M[0] + s.S[0] - 1;
-    s.P[1] = s.M[1] + s.S[1] - 1;
-    s.P[2] = stencil_padded_z(s.M[2], s.S[2]);
+    const bool fp64 = sizeof(T) == 8;
+    tile_[l] = stencil_default_tile(s, fp64);
+    if (!stencil_templated(s) || stencil_prepare<T>(s, tile_[l]) < 0) {
+      tile_[l] = StencilTile();  // reference-form sweep
+      s.P[0] = s.M[0] + s.S[0] - 1;
+      s.P[1] = s.M[1] + s.S[1] - 1;
+      s.P[2] = s.M[2] + s.S[2] - 1;
+    } else {
+      stencil_padded_dims(s, tile_[l], fp64, s.P);
+    }
     pad_max = std::max(pad_max, (size_t)s.P[0] * s.P[1] * s.P[2]);
   }
   const size_t n = N_;
@@ -339,7 +388,8 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   launch_pair<T>(s, N_, psorted_, pcs_, pstart_, geom_, off_d_, noff_, pc_, pout_);
   nl += 1;
   mark(s, kPhaseAnterp, tm);
-  launch_anterpolate<T>(s, grid_[1], gsorted_, gstart_, sc_, qg_[1]);
+  launch_anterpolate<T>(s, grid_[1], gsorted_, gstart_, sc_, qg_[1],
+                        anterp_variant_, err_d_);
   nl += 1;
   mark(s, kPhaseRestrict, tm);
   for (int l = 1; l < L_; ++l) {
@@ -360,7 +410,10 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
     launch_prolong_add<T>(s, grid_[l], eg_[l + 1], eg_[l], J_, nu_);
     mark(s, kPhaseStencil, tm && l == L_ - 1);
     launch_pad<T>(s, sh_[l], qg_[l], padded_);
-    launch_stencil<T>(s, sh_[l], padded_, kh_[l], (T)w[l], eg_[l], 0);
+    if (tm) cudaEventRecord(lev_ev_[l][0], s);
+    launch_stencil<T>(s, sh_[l], tile_[l], padded_, kh_[l], sh_[l].S[2],
+                      (T)w[l], eg_[l]);
+    if (tm) cudaEventRecord(lev_ev_[l][1], s);
     nl += 3;
   }
   mark(s, kPhaseInterp, tm);
@@ -399,7 +452,12 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   nl += 2;
   mark(s, kNumPhases, tm);
   nlaunch_ = nl;
-  return cudaGetLastError() == cudaSuccess ? MSMPB_OK : MSMPB_ERR_CUDA;
+  cudaError_t ce = cudaGetLastError();
+  if (ce != cudaSuccess) {
+    std::fprintf(stderr, "msmpb_b200: launch error: %s\n", cudaGetErrorString(ce));
+    return MSMPB_ERR_CUDA;
+  }
+  return MSMPB_OK;
 }
 
 template <typename T>
@@ -419,6 +477,38 @@ int Plan<T>::evaluate(const EvalRequest &r, double *energy) {
     phi = r.phi ? phi_s_ : nullptr;
   }
   double *edev = r.host ? energy_ : (r.energy_dev ? r.energy_dev : energy_);
+  cudaGetLastError();  // never inherit an earlier, unrelated error
+  if (r.timing) {
+    // Per-phase timing uses events between eager launches (events recorded
+    // by graph nodes cannot be timed); untimed calls replay the graph.
+    int st = enqueue(r, s, pos, q, force, phi, edev);
+    if (st != MSMPB_OK) return st;
+  } else {
+    int st = launch_graph(r, s, pos, q, force, phi, edev);
+    if (st != MSMPB_OK) return st;
+  }
+  timed_ = r.timing;
+  if (r.host) {
+    if (r.force)
+      MSM_CUDA_TRY(cudaMemcpyAsync(r.force, force_s_, 3 * (size_t)N_ * sizeof(double),
+                                   cudaMemcpyDeviceToHost, s));
+    if (r.phi)
+      MSM_CUDA_TRY(cudaMemcpyAsync(r.phi, phi_s_, (size_t)N_ * sizeof(double),
+                                   cudaMemcpyDeviceToHost, s));
+    double e = 0;
+    MSM_CUDA_TRY(cudaMemcpyAsync(&e, energy_, sizeof(double),
+                                 cudaMemcpyDeviceToHost, s));
+    int st = sync();
+    if (energy) *energy = e;
+    return st;
+  }
+  return MSMPB_OK;
+}
+
+template <typename T>
+int Plan<T>::launch_graph(const EvalRequest &r, cudaStream_t s,
+                          const double *pos, const double *q, double *force,
+                          double *phi, double *edev) {
   GraphKey key{};
   key.pos = pos;
   key.q = q;
@@ -426,7 +516,7 @@ int Plan<T>::evaluate(const EvalRequest &r, double *energy) {
   key.phi = phi;
   key.energy = edev;
   for (int l = 0; l <= L_; ++l) key.w[l] = r.weight ? r.weight[l] : 1.0;
-  key.timing = r.timing;
+  key.timing = false;
   if (!have_graph_ || !(key == key_)) {
     if (exec_) {
       cudaGraphExecDestroy(exec_);
@@ -435,7 +525,9 @@ int Plan<T>::evaluate(const EvalRequest &r, double *energy) {
     have_graph_ = false;
     cudaGraph_t g = nullptr;
     MSM_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    int st = enqueue(r, s, pos, q, force, phi, edev);
+    EvalRequest untimed = r;
+    untimed.timing = false;
+    int st = enqueue(untimed, s, pos, q, force, phi, edev);
     cudaError_t ce = cudaStreamEndCapture(s, &g);
     if (st != MSMPB_OK || ce != cudaSuccess) {
       if (g) cudaGraphDestroy(g);
@@ -452,21 +544,6 @@ int Plan<T>::evaluate(const EvalRequest &r, double *energy) {
     have_graph_ = true;
   }
   MSM_CUDA_TRY(cudaGraphLaunch(exec_, s));
-  timed_ = r.timing;
-  if (r.host) {
-    if (r.force)
-      MSM_CUDA_TRY(cudaMemcpyAsync(r.force, force_s_, 3 * (size_t)N_ * sizeof(double),
-                                   cudaMemcpyDeviceToHost, s));
-    if (r.phi)
-      MSM_CUDA_TRY(cudaMemcpyAsync(r.phi, phi_s_, (size_t)N_ * sizeof(double),
-                                   cudaMemcpyDeviceToHost, s));
-    double e = 0;
-    MSM_CUDA_TRY(cudaMemcpyAsync(&e, energy_, sizeof(double),
-                                 cudaMemcpyDeviceToHost, s));
-    int st = sync();
-    if (energy) *energy = e;
-    return st;
-  }
   return MSMPB_OK;
 }
 
@@ -511,6 +588,7 @@ int Plan<T>::phase_times(double *ms, int n) {
   cudaEventElapsedTime(&tot, ev_[kPhaseBin], ev_[kNumPhases]);
   out[kNumPhases] = tot;
   (void)order;
+  cudaGetLastError();
   int m = std::min(n, kNumPhases + 1);
   for (int k = 0; k < m; ++k) ms[k] = out[k];
   return m;
@@ -565,4 +643,10 @@ int engine_phase_times(FFDevice *d, double *ms, int n) {
 
 int engine_kernel_launches(FFDevice *d) { return d->launches(); }
 
+}  // namespace msm
+
+namespace msm {
+int engine_level_times(FFDevice *d, double *ms, int n) {
+  return d->level_times(ms, n);
+}
 }  // namespace msm

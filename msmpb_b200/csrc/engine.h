@@ -53,5 +53,7 @@ int engine_sync(FFDevice *d);
 // Phase times of the last timed evaluation (ms), kNumPhases + total.
 int engine_phase_times(FFDevice *d, double *ms, int n);
 int engine_kernel_launches(FFDevice *d);
+// Stencil kernel time per level (1..L-1) of the last timed evaluation
+int engine_level_times(FFDevice *d, double *ms, int n);
 
 }  // namespace msm

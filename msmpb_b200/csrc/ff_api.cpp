@@ -165,6 +165,7 @@ FF *FF_new(int N, double *q) {
   if (pv && (std::strcmp(pv, "fp64") == 0 || std::strcmp(pv, "FP64") == 0))
     ff->precision = MSMPB_PRECISION_FP64;
   ff->device = 0;
+  ff->timing = timing_enabled() ? 1 : 0;
   ff->host_state = new (std::nothrow) HostState();
   if (N <= 0 || !q) ff->last_error = MSMPB_ERR_ARGUMENT;
   return ff;
@@ -274,7 +275,7 @@ double FF_energy_potentials(FF *ff, double (*force)[3], double (*position)[3],
   r.weight = weight;
   r.force = force ? &force[0][0] : nullptr;
   r.phi = potential;
-  r.timing = timing_enabled();
+  r.timing = ff->timing != 0;
   double e = NAN;
   int st = msm::engine_evaluate(ff->dev, r, &e);
   if (st != MSMPB_OK) {
@@ -308,7 +309,7 @@ int FF_energy_device(FF *ff, const double *position_d, const double *charge_d,
   r.phi = potential_d;
   r.energy_dev = energy_d;
   r.stream = static_cast<cudaStream_t>(stream);
-  r.timing = false;
+  r.timing = ff->timing != 0;
   int st = msm::engine_evaluate(ff->dev, r, nullptr);
   if (st != MSMPB_OK) ff->last_error = st;
   return st;
@@ -329,6 +330,12 @@ int FF_phase_times(FF *ff, double *ms, int n) {
 int FF_kernel_launches(FF *ff) {
   return ff->dev ? msm::engine_kernel_launches(ff->dev) : 0;
 }
+
+int FF_stencil_times(FF *ff, double *ms, int n) {
+  return ff->dev ? msm::engine_level_times(ff->dev, ms, n) : 0;
+}
+
+void FF_set_timing(FF *ff, int enabled) { ff->timing = enabled ? 1 : 0; }
 
 int FF_last_error(const FF *ff) { return ff ? ff->last_error : MSMPB_ERR_ARGUMENT; }
 

@@ -176,14 +176,22 @@ void run_pass(cudaStream_t s, const FftLines &f, int mode, const T *rin,
               T *rout, double scale) {
   size_t smem = 2 * (size_t)f.lpb * f.n * sizeof(double2);
   int blocks = (f.nlines + f.lpb - 1) / f.lpb;
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_fft_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
   k_fft_pass<T><<<blocks, kThreads, smem, s>>>(f, mode, rin, in, out, khat, w,
                                                rout, scale);
 }
 
 }  // namespace
+
+// One-time kernel attribute: lines up to 4096 points need 128 KB of
+// shared memory (two buffers of one line). Called outside stream capture.
+void top_solve_prepare() {
+  static bool done = false;
+  if (done) return;
+  const int bytes = 2 * 4096 * (int)sizeof(double2);
+  cudaFuncSetAttribute(k_fft_pass<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_fft_pass<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  done = true;
+}
 
 // largest supported line length (radix factors <= kMaxRadix, smem <= 128 KB)
 bool top_solve_supported(const int M[3]) {

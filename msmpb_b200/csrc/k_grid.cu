@@ -82,6 +82,145 @@ k_anterpolate(int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
   grid[idx] = acc.value();
 }
 
+// Anterpolation as a slab-staged gather (the fast path).
+//
+// A CTA owns BX x BY x BZ grid points; thread (tz, ty) accumulates the BX
+// points (x0+xo, y0+ty, z0+tz) in registers. The atoms that can reach the
+// block lie in the halo cells x0-nu/2 .. x0+BX+nu/2-2 (same in y, z). The
+// halo is streamed one x-slab hx at a time: the slab's cells are counted
+// and scanned, their atoms (contiguous per cell in cell-sorted order) are
+// staged in shared memory with their B-spline weights (q folded into the x
+// weights), then every thread adds, for its nu halo rows hy = ty + b and nu
+// halo z-cells hz = tz + c, the contributions q wx[hx-xo] wy[b] wz[c].
+// Every grid point is written by one thread, atoms are visited in a fixed
+// order: no atomics, deterministic sums. Slabs whose atoms exceed the
+// staging capacity are processed in row chunks.
+template <typename T, int NU, int BX>
+__global__ void __launch_bounds__(512)
+k_anterpolate_slab(int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
+                   const int *__restrict__ start, SplineConsts<T> sc, int cap,
+                   T *__restrict__ grid, int *err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int BZ = blockDim.x, BY = blockDim.y;
+  const int tz = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * BZ + tz, nth = BZ * BY;
+  const int EY = BY + NU - 1, EZ = BZ + NU - 1, ncell = EY * EZ;
+  const int x0 = blockIdx.z * BX, y0 = blockIdx.y * BY, z0 = blockIdx.x * BZ;
+  // shared layout: pre[ncell+1] | hz[cap] | wx[NU][cap] | wy[NU][cap] | wz[NU][cap]
+  int *pre = reinterpret_cast<int *>(smem_raw);
+  int *shz = pre + ((ncell + 1 + 3) & ~3);
+  T *wbase = reinterpret_cast<T *>(shz + ((cap + 3) & ~3));
+  T *swx = wbase, *swy = wbase + NU * cap, *swz = wbase + 2 * NU * cap;
+  __shared__ int warp_tot[16];
+
+  T acc[BX];
+#pragma unroll
+  for (int a = 0; a < BX; ++a) acc[a] = T(0);
+
+  for (int hx = 0; hx < BX + NU - 1; ++hx) {
+    const int mx = pwrap(x0 - NU / 2 + hx, M0);
+    // 1) per-cell counts of this slab, exclusive scan into pre[]
+    const int per = (ncell + nth - 1) / nth;
+    const int k0 = tid * per;
+    int local = 0;
+    for (int k = k0; k < min(k0 + per, ncell); ++k) {
+      const int hy = k / EZ, hz = k - hy * EZ;
+      const int my = pwrap(y0 - NU / 2 + hy, M1), mz = pwrap(z0 - NU / 2 + hz, M2);
+      const long c = ((long)mx * M1 + my) * M2 + mz;
+      const int n = start[c + 1] - start[c];
+      pre[k] = n;
+      local += n;
+    }
+    // block exclusive scan of the per-thread totals; the last warp may be
+    // partial (small tiles), so the shuffle mask covers only its lanes
+    const int lane = tid & 31, warp = tid >> 5;
+    const int wsize = min(32, nth - warp * 32);
+    const unsigned mask = wsize == 32 ? 0xffffffffu : ((1u << wsize) - 1u);
+    int incl = local;
+    for (int o = 1; o < 32; o <<= 1) {
+      int v = __shfl_up_sync(mask, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == wsize - 1) warp_tot[warp] = incl;
+    __syncthreads();
+    int wbefore = 0, total = 0;
+    for (int w = 0; w < (nth + 31) / 32; ++w) {
+      if (w < warp) wbefore += warp_tot[w];
+      total += warp_tot[w];
+    }
+    int run = wbefore + incl - local;
+    for (int k = k0; k < min(k0 + per, ncell); ++k) {
+      const int n = pre[k];
+      pre[k] = run;
+      run += n;
+    }
+    if (tid == 0) pre[ncell] = total;
+    __syncthreads();
+    // 2) stage in row chunks that fit the capacity
+    int r0 = 0;
+    while (r0 < EY) {
+      int r1 = r0 + 1;
+      while (r1 < EY && pre[(r1 + 1) * EZ] - pre[r0 * EZ] <= cap) ++r1;
+      const int lo = pre[r0 * EZ];
+      int hi = pre[r1 * EZ];
+      if (hi - lo > cap) {  // one row alone exceeds the capacity
+        flag_error(err, kCheckOverflow);
+        hi = lo;
+      }
+      for (int k = r0 * EZ + tid; k < r1 * EZ && hi > lo; k += nth) {
+        const int hy = k / EZ, hz = k - hy * EZ;
+        const int my = pwrap(y0 - NU / 2 + hy, M1), mz = pwrap(z0 - NU / 2 + hz, M2);
+        const long c = ((long)mx * M1 + my) * M2 + mz;
+        const int b = start[c];
+        const int n = start[c + 1] - b;
+        const int slot0 = pre[k] - lo;
+        if (slot0 < 0 || slot0 + n > hi - lo) {  // self-check, never expected
+          flag_error(err, kCheckIndex);
+          continue;
+        }
+        for (int u = 0; u < n; ++u) {
+          const V4<T> at = atoms[b + u];
+          const int s = slot0 + u;
+          shz[s] = hz;
+#pragma unroll
+          for (int i = 0; i < NU; ++i) {
+            swx[i * cap + s] = at.w * bspline<T, NU>(sc, i, at.x);
+            swy[i * cap + s] = bspline<T, NU>(sc, i, at.y);
+            swz[i * cap + s] = bspline<T, NU>(sc, i, at.z);
+          }
+        }
+      }
+      __syncthreads();
+      // 3) accumulate from the staged rows
+      for (int bb = 0; bb < NU; ++bb) {
+        const int hy = ty + bb;
+        if (hy < r0 || hy >= r1 || hi == lo) continue;
+        const int s0 = max(0, pre[hy * EZ + tz] - lo);
+        const int s1 = min(hi - lo, pre[hy * EZ + tz + NU] - lo);
+        for (int s = s0; s < s1; ++s) {
+          const int c = shz[s] - tz;
+          if ((unsigned)c >= (unsigned)NU) continue;  // never taken
+          const T wyz = swy[bb * cap + s] * swz[c * cap + s];
+#pragma unroll
+          for (int xo = 0; xo < BX; ++xo) {
+            const int a = hx - xo;
+            if (a >= 0 && a < NU) acc[xo] = fma(wyz, swx[a * cap + s], acc[xo]);
+          }
+        }
+      }
+      __syncthreads();
+      r0 = r1;
+    }
+  }
+  const int y = y0 + ty, z = z0 + tz;
+  if (y >= M1 || z >= M2) return;
+#pragma unroll
+  for (int xo = 0; xo < BX; ++xo) {
+    const int x = x0 + xo;
+    if (x < M0) grid[((long)x * M1 + y) * M2 + z] = acc[xo];
+  }
+}
+
 // Field and potential at each atom (code/forcefield1.c:570-607), separable:
 // z sums first, then y, then x. Output E in Cartesian components
 // (E = A^-T (M * grad_u)) and phi_long.
@@ -234,16 +373,74 @@ inline int blocks_for(long n) {
     case 8: { constexpr int NU = 8; CALL; } break;  \
     default: { constexpr int NU = 10; CALL; } break; \
   }
+#define MSM_NU_SWITCH_ALL(CALL)                 \
+  { constexpr int NU = 4; CALL; }               \
+  { constexpr int NU = 6; CALL; }               \
+  { constexpr int NU = 8; CALL; }               \
+  { constexpr int NU = 10; CALL; }
+
+constexpr int kAnterpBX = 4;
+constexpr int kAnterpSmemBudget = 96 * 1024;
+
+struct AnterpTile {
+  int bz, by, cap;
+  size_t smem;
+};
+
+// z extent: the candidate (<= 64) that wastes the fewest points; y fills
+// up to 512 threads (at most 8 rows); staging capacity fills the budget.
+template <typename T>
+AnterpTile anterp_tile(const int M[3], int nu) {
+  AnterpTile t{};
+  int best = 32;
+  double best_waste = 1e30;
+  for (int bz : {64, 48, 32, 56, 40, 24, 16}) {
+    int b = std::min(bz, M[2]);
+    double waste = (double)((M[2] + b - 1) / b * b) / M[2] + (b < 32 ? 0.05 : 0.0);
+    if (waste < best_waste - 1e-9) {
+      best_waste = waste;
+      best = b;
+    }
+  }
+  t.bz = best;
+  t.by = std::max(1, std::min(std::min(8, M[1]), 512 / t.bz));
+  const int ncell = (t.by + nu - 1) * (t.bz + nu - 1);
+  const size_t fixed = 4 * (size_t)((ncell + 1 + 3) & ~3);
+  int cap = (int)((kAnterpSmemBudget - fixed - 64) / (3 * nu * sizeof(T) + 4));
+  cap &= ~3;
+  t.cap = std::max(4, cap);
+  t.smem = fixed + 4 * (size_t)t.cap + 3 * (size_t)nu * t.cap * sizeof(T);
+  return t;
+}
 
 }  // namespace
 
 template <typename T>
 void launch_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
                         const int *cell_start, const SplineConsts<T> &sc,
-                        T *grid) {
-  long n = (long)M[0] * M[1] * M[2];
-  MSM_NU_SWITCH(sc.nu, (k_anterpolate<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
-                           M[0], M[1], M[2], atoms, cell_start, sc, grid)));
+                        T *grid, int variant, int *err) {
+  if (variant == 1) {  // one grid point per thread, runtime loops
+    long n = (long)M[0] * M[1] * M[2];
+    MSM_NU_SWITCH(sc.nu, (k_anterpolate<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
+                             M[0], M[1], M[2], atoms, cell_start, sc, grid)));
+    return;
+  }
+  const AnterpTile t = anterp_tile<T>(M, sc.nu);
+  dim3 block(t.bz, t.by);
+  dim3 g((M[2] + t.bz - 1) / t.bz, (M[1] + t.by - 1) / t.by,
+         (M[0] + kAnterpBX - 1) / kAnterpBX);
+  MSM_NU_SWITCH(sc.nu, (k_anterpolate_slab<T, NU, kAnterpBX><<<g, block, t.smem, s>>>(
+                           M[0], M[1], M[2], atoms, cell_start, sc, t.cap, grid, err)));
+}
+
+template <typename T>
+void anterpolate_prepare() {
+  static bool done = false;
+  if (done) return;
+  MSM_NU_SWITCH_ALL(cudaFuncSetAttribute(k_anterpolate_slab<T, NU, kAnterpBX>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kAnterpSmemBudget));
+  done = true;
 }
 
 template <typename T>
@@ -288,7 +485,9 @@ void launch_grid_dot(cudaStream_t s, size_t n, const T *a, const T *b,
 #define MSM_INST_GRID(T)                                                       \
   template void launch_anterpolate<T>(cudaStream_t, const int *,              \
                                       const V4<T> *, const int *,             \
-                                      const SplineConsts<T> &, T *);          \
+                                      const SplineConsts<T> &, T *, int,      \
+                                      int *);                                 \
+  template void anterpolate_prepare<T>();                                     \
   template void launch_interpolate<T>(cudaStream_t, int, const int *,         \
                                       const V4<T> *, const int *, const T *,  \
                                       const SplineConsts<T> &,                \

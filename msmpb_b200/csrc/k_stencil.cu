@@ -3,8 +3,23 @@
 // The periodic wrap is materialised once per level as a padded copy
 // P[a][b][c] = q[(a - S0/2) mod M0][(b - S1/2) mod M1][(c - S2/2) mod M2]
 // (the reference pads the same way, code/forcefield1.c:58-99), so the sweep
-// itself reads a dense box with no index arithmetic modulo M.
+// reads dense boxes with no modular index arithmetic.
+//
+// Tiled sweep (FP32 CUDA cores; a single-channel stencil is not a GEMM):
+//  - a CTA owns TX x TY x (NZ*R) outputs; thread (tz, ty) keeps TX*R
+//    accumulators in registers (R consecutive z outputs for each of TX
+//    x-planes);
+//  - input x-planes stream through a double-buffered shared-memory slice
+//    ((TY+S1-1) x (NZ*R+S2-1)) filled with cp.async 16-byte copies while
+//    the previous plane is consumed; plane p feeds output planes x0+xo with
+//    tap plane i = p - x0 - xo;
+//  - per (plane, tap row j) a thread loads one input row segment of
+//    R+S2-1 values into registers once and reuses it for all TX output
+//    planes; the S2 taps of row (i, j) are uniform across the CTA (L1
+//    broadcast). The z extent S2 is a template parameter so the R x S2
+//    FMA block is fully unrolled with register-resident operands.
 #include <algorithm>
+#include <mutex>
 
 #include "kernels.h"
 
@@ -12,6 +27,7 @@ namespace msm {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kMaxTemplatedS = 33;
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
@@ -28,10 +44,11 @@ k_pad(StencilShape sh, const T *__restrict__ q, T *__restrict__ p) {
 }
 
 // Reference-form sweep: one output per thread, all loops at run time.
+// Used for stencil widths beyond the templated range.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_stencil_simple(StencilShape sh, const T *__restrict__ p,
-                 const T *__restrict__ kh, T w, T *__restrict__ e) {
+                 const T *__restrict__ kh, int khz, T w, T *__restrict__ e) {
   long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long n = (long)sh.M[0] * sh.M[1] * sh.M[2];
   if (idx >= n) return;
@@ -43,7 +60,7 @@ k_stencil_simple(StencilShape sh, const T *__restrict__ p,
     T pl = 0;
     for (int j = 0; j < sh.S[1]; ++j) {
       const T *row = p + ((long)(x + i) * sh.P[1] + (y + j)) * sh.P[2] + z;
-      const T *kr = kh + ((long)i * sh.S[1] + j) * sh.S[2];
+      const T *kr = kh + ((long)i * sh.S[1] + j) * khz;
       T r = 0;
       for (int k = 0; k < sh.S[2]; ++k) r += kr[k] * row[k];
       pl += r;
@@ -53,15 +70,218 @@ k_stencil_simple(StencilShape sh, const T *__restrict__ p,
   e[idx] += w * acc.value();
 }
 
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::);
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// Copies input plane `plane` of the tile into the shared slice (rows of W).
+template <typename T>
+__device__ __forceinline__ void stage_plane(const T *__restrict__ P,
+                                            const StencilShape &sh, int plane,
+                                            int y0, int z0, int H, int W,
+                                            T *slice) {
+  constexpr int V = 16 / sizeof(T);
+  const int wv = W / V;
+  const int nthreads = blockDim.x * blockDim.y;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const T *src = P + ((long)plane * sh.P[1] + y0) * sh.P[2] + z0;
+  for (int t = tid; t < H * wv; t += nthreads) {
+    const int row = t / wv, c = t - row * wv;
+    cp_async16(slice + row * W + c * V, src + (long)row * sh.P[2] + c * V);
+  }
+  cp_async_commit();
+}
+
+template <typename T, int S, int R, int TX>
+__global__ void __launch_bounds__(kThreads)
+k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
+                const T *__restrict__ kh, int khz, T w, T *__restrict__ e) {
+  constexpr int V = 16 / sizeof(T);
+  constexpr int RL = R + S - 1;                  // row values per thread
+  constexpr int RLV = (RL + V - 1) / V * V;      // rounded to 16-byte loads
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *smem = reinterpret_cast<T *>(smem_raw);
+  const int NZ = blockDim.x, TY = blockDim.y;
+  const int tz = threadIdx.x, ty = threadIdx.y;
+  const int S0 = sh.S[0], S1 = sh.S[1];
+  const int z0 = blockIdx.x * NZ * R, y0 = blockIdx.y * TY, x0 = blockIdx.z * TX;
+  const int H = TY + S1 - 1;
+  const int W = (NZ * R + S - 1 + V - 1) / V * V;
+  const int slice_elems = H * W + V;  // +V: tail reads of the last row
+  T *buf[2] = {smem, smem + slice_elems};
+
+  T acc[TX][R];
+#pragma unroll
+  for (int a = 0; a < TX; ++a)
+#pragma unroll
+    for (int r = 0; r < R; ++r) acc[a][r] = T(0);
+
+  const int nplanes = TX + S0 - 1;
+  stage_plane(P, sh, x0, y0, z0, H, W, buf[0]);
+  for (int pi = 0; pi < nplanes; ++pi) {
+    if (pi + 1 < nplanes) {
+      stage_plane(P, sh, x0 + pi + 1, y0, z0, H, W, buf[(pi + 1) & 1]);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const T *slice = buf[pi & 1];
+    for (int j = 0; j < S1; ++j) {
+      const T *rp = slice + (ty + j) * W + tz * R;
+      T row[RLV];
+#pragma unroll
+      for (int v = 0; v < RLV; v += V) {
+        if constexpr (sizeof(T) == 4) {
+          const float4 q4 = *reinterpret_cast<const float4 *>(rp + v);
+          row[v] = (T)q4.x;
+          row[v + 1] = (T)q4.y;
+          row[v + 2] = (T)q4.z;
+          row[v + 3] = (T)q4.w;
+        } else {
+          const double2 q2 = *reinterpret_cast<const double2 *>(rp + v);
+          row[v] = (T)q2.x;
+          row[v + 1] = (T)q2.y;
+        }
+      }
+#pragma unroll
+      for (int xo = 0; xo < TX; ++xo) {
+        const int i = pi - xo;
+        if (i < 0 || i >= S0) continue;  // uniform across the CTA
+        const T *kp = kh + ((long)i * S1 + j) * khz;
+#pragma unroll
+        for (int k = 0; k < S; ++k) {
+          const T t = __ldg(kp + k);
+#pragma unroll
+          for (int r = 0; r < R; ++r) acc[xo][r] = fma(t, row[r + k], acc[xo][r]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  const int y = y0 + ty;
+  if (y >= sh.M[1]) return;
+#pragma unroll
+  for (int xo = 0; xo < TX; ++xo) {
+    const int x = x0 + xo;
+    if (x >= sh.M[0]) continue;
+    T *out = e + ((long)x * sh.M[1] + y) * sh.M[2];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int z = z0 + tz * R + r;
+      if (z < sh.M[2]) out[z] += w * acc[xo][r];
+    }
+  }
+}
+
+template <typename T> struct TileDefaults;
+template <> struct TileDefaults<float> { static constexpr int R = 8, TX = 4; };
+template <> struct TileDefaults<double> { static constexpr int R = 4, TX = 4; };
+
+template <typename T, int S>
+void launch_tiled(cudaStream_t s, const StencilShape &sh, const StencilTile &tl,
+                  const T *p, const T *kh, int khz, T w, T *e) {
+  constexpr int R = TileDefaults<T>::R, TX = TileDefaults<T>::TX;
+  constexpr int V = 16 / sizeof(T);
+  const int H = tl.ty + sh.S[1] - 1;
+  const int W = (tl.nz * R + S - 1 + V - 1) / V * V;
+  const size_t smem = 2 * (size_t)(H * W + V) * sizeof(T);
+  dim3 block(tl.nz, tl.ty);
+  dim3 grid((sh.M[2] + tl.nz * R - 1) / (tl.nz * R), (sh.M[1] + tl.ty - 1) / tl.ty,
+            (sh.M[0] + TX - 1) / TX);
+  k_stencil_tiled<T, S, R, TX><<<grid, block, smem, s>>>(sh, p, kh, khz, w, e);
+}
+
+// Levels (and plans) that share an instantiation need the largest request:
+// the attribute is per kernel function, so it is only ever raised.
+template <typename T, int S>
+void set_smem_attr(int bytes) {
+  constexpr int R = TileDefaults<T>::R, TX = TileDefaults<T>::TX;
+  static std::mutex mu;
+  static int current = 48 * 1024;
+  std::lock_guard<std::mutex> lock(mu);
+  if (bytes <= current) return;
+  if (cudaFuncSetAttribute(k_stencil_tiled<T, S, R, TX>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           bytes) == cudaSuccess)
+    current = bytes;
+}
+
+#define MSM_S_CASES(X) \
+  X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) \
+  X(15) X(16) X(17) X(18) X(19) X(20) X(21) X(22) X(23) X(24) X(25) X(26)    \
+  X(27) X(28) X(29) X(30) X(31) X(32) X(33)
+
 inline int blocks_for(long n) {
   return (int)std::max<long>(1, (n + kThreads - 1) / kThreads);
 }
 
 }  // namespace
 
-int stencil_padded_z(int Mz, int Sz) {
-  int pz = Mz + Sz - 1;
-  return (pz + 3) / 4 * 4;  // 16-byte rows for FP32 tiles
+StencilTile stencil_default_tile(const StencilShape &sh, bool fp64) {
+  const int R = fp64 ? TileDefaults<double>::R : TileDefaults<float>::R;
+  StencilTile t;
+  // z: smallest thread count whose span covers M2 in the fewest tiles
+  int best_nz = 1;
+  double best_cost = 1e30;
+  for (int nz = 2; nz <= 8; ++nz) {
+    const int span = nz * R;
+    const int tiles = (sh.M[2] + span - 1) / span;
+    const double cost = (double)tiles * span / sh.M[2] + 0.02 * (8 - nz);
+    if (cost < best_cost) {
+      best_cost = cost;
+      best_nz = nz;
+    }
+  }
+  t.nz = std::min(best_nz, std::max(1, (sh.M[2] + R - 1) / R));
+  int ty = std::max(1, std::min(16, kThreads / t.nz));
+  if (ty > sh.M[1]) ty = sh.M[1];
+  t.ty = ty;
+  t.tx = fp64 ? TileDefaults<double>::TX : TileDefaults<float>::TX;
+  return t;
+}
+
+bool stencil_templated(const StencilShape &sh) {
+  return sh.S[2] >= 1 && sh.S[2] <= kMaxTemplatedS;
+}
+
+void stencil_padded_dims(const StencilShape &sh, const StencilTile &tl,
+                         bool fp64, int P[3]) {
+  const int R = fp64 ? TileDefaults<double>::R : TileDefaults<float>::R;
+  const int V = fp64 ? 2 : 4;
+  const int span = tl.nz * R;
+  const int mz = (sh.M[2] + span - 1) / span * span;
+  const int my = (sh.M[1] + tl.ty - 1) / tl.ty * tl.ty;
+  const int mx = (sh.M[0] + tl.tx - 1) / tl.tx * tl.tx;
+  P[0] = mx + sh.S[0] - 1;
+  P[1] = my + sh.S[1] - 1;
+  P[2] = ((mz + sh.S[2] - 1 + V - 1) / V) * V + V;
+}
+
+template <typename T>
+int stencil_prepare(const StencilShape &sh, const StencilTile &tl) {
+  if (!stencil_templated(sh)) return 0;
+  constexpr int R = TileDefaults<T>::R;
+  constexpr int V = 16 / sizeof(T);
+  const int H = tl.ty + sh.S[1] - 1;
+  const int W = (tl.nz * R + sh.S[2] - 1 + V - 1) / V * V;
+  const int bytes = 2 * (H * W + V) * (int)sizeof(T);
+  if (bytes > 200 * 1024) return -1;
+  switch (sh.S[2]) {
+#define X(SS) \
+  case SS: set_smem_attr<T, SS>(bytes); break;
+    MSM_S_CASES(X)
+#undef X
+  }
+  return 0;
 }
 
 template <typename T>
@@ -71,11 +291,19 @@ void launch_pad(cudaStream_t s, const StencilShape &sh, const T *q, T *p) {
 }
 
 template <typename T>
-void launch_stencil(cudaStream_t s, const StencilShape &sh, const T *p,
-                    const T *kh, T w, T *e, int variant) {
-  (void)variant;
-  long n = (long)sh.M[0] * sh.M[1] * sh.M[2];
-  k_stencil_simple<T><<<blocks_for(n), kThreads, 0, s>>>(sh, p, kh, w, e);
+void launch_stencil(cudaStream_t s, const StencilShape &sh, const StencilTile &tl,
+                    const T *p, const T *kh, int khz, T w, T *e) {
+  if (!stencil_templated(sh) || tl.nz <= 0) {
+    long n = (long)sh.M[0] * sh.M[1] * sh.M[2];
+    k_stencil_simple<T><<<blocks_for(n), kThreads, 0, s>>>(sh, p, kh, khz, w, e);
+    return;
+  }
+  switch (sh.S[2]) {
+#define X(SS) \
+  case SS: launch_tiled<T, SS>(s, sh, tl, p, kh, khz, w, e); break;
+    MSM_S_CASES(X)
+#undef X
+  }
 }
 
 template void launch_pad<float>(cudaStream_t, const StencilShape &,
@@ -83,10 +311,12 @@ template void launch_pad<float>(cudaStream_t, const StencilShape &,
 template void launch_pad<double>(cudaStream_t, const StencilShape &,
                                  const double *, double *);
 template void launch_stencil<float>(cudaStream_t, const StencilShape &,
-                                    const float *, const float *, float,
-                                    float *, int);
+                                    const StencilTile &, const float *,
+                                    const float *, int, float, float *);
 template void launch_stencil<double>(cudaStream_t, const StencilShape &,
-                                     const double *, const double *, double,
-                                     double *, int);
+                                     const StencilTile &, const double *,
+                                     const double *, int, double, double *);
+template int stencil_prepare<float>(const StencilShape &, const StencilTile &);
+template int stencil_prepare<double>(const StencilShape &, const StencilTile &);
 
 }  // namespace msm

@@ -99,10 +99,13 @@ void launch_pair(cudaStream_t s, int N, const V4<T> *pos_sorted,
                  const PairConsts<T> &pc, V4<T> *out);
 
 // ---- grid transfers (k_grid.cu) ----
+// variant 0: slab-staged gather; 1: one grid point per thread (reference form)
 template <typename T>
 void launch_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
                         const int *cell_start, const SplineConsts<T> &sc,
-                        T *grid);
+                        T *grid, int variant, int *err);
+template <typename T>
+void anterpolate_prepare();
 template <typename T>
 void launch_interpolate(cudaStream_t s, int N, const int M[3],
                         const V4<T> *atoms, const int *cell_sorted,
@@ -125,15 +128,29 @@ struct StencilShape {
   int S[3];   // stencil dims
   int P[3];   // padded input dims (P[2] rounded up for 16-byte rows)
 };
+// CTA tile of the stencil sweep: nz x ty threads, each with tx x R outputs
+struct StencilTile {
+  int nz = 0, ty = 0, tx = 0;
+};
+StencilTile stencil_default_tile(const StencilShape &sh, bool fp64);
+bool stencil_templated(const StencilShape &sh);
+// padded input dims that keep every tile load of `tile` inside the buffer
+void stencil_padded_dims(const StencilShape &sh, const StencilTile &tile,
+                         bool fp64, int P[3]);
+// one-time kernel attributes (dynamic shared memory); <0 if unsupported
+template <typename T>
+int stencil_prepare(const StencilShape &sh, const StencilTile &tile);
 template <typename T>
 void launch_pad(cudaStream_t s, const StencilShape &sh, const T *q, T *padded);
+// kh: S0 x S1 x khz taps (z fastest)
 template <typename T>
-void launch_stencil(cudaStream_t s, const StencilShape &sh, const T *padded,
-                    const T *kh, T weight, T *e, int variant);
-int stencil_padded_z(int Mz, int Sz);
+void launch_stencil(cudaStream_t s, const StencilShape &sh,
+                    const StencilTile &tile, const T *padded, const T *kh,
+                    int khz, T weight, T *e);
 
 // ---- top-level FFT solve (k_fft.cu) ----
 bool top_solve_supported(const int M[3]);
+void top_solve_prepare();
 template <typename T>
 void launch_top_solve(cudaStream_t s, const int M[3], const T *q,
                       const double *khat, double weight, double2 *buf0,

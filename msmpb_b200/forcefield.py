@@ -44,9 +44,17 @@ class ForceField:
 
     def __init__(self, charges, positions, edges, cutoff=None, order=None,
                  levels=None, top_grid=None, est_err=None, fft=True,
-                 margin=0.0, precision="mixed", device=0):
+                 margin=0.0, precision="mixed", device=0, charges_buffer=None):
         self._lib = L.load()
-        self.q = _f64(charges).copy()  # FF_new keeps this pointer
+        # FF_new keeps this pointer: the library re-reads the charges every
+        # evaluation. charges_buffer (a contiguous float64 array, e.g. a
+        # pinned one) is used in place instead of a private copy.
+        if charges_buffer is not None:
+            if charges_buffer.dtype != np.float64 or not charges_buffer.flags.c_contiguous:
+                raise ValueError("charges_buffer must be contiguous float64")
+            self.q = charges_buffer
+        else:
+            self.q = _f64(charges).copy()
         self.N = int(self.q.shape[0])
         pos = _f64(positions).reshape(self.N, 3)
         self.edges = _f64(np.asarray(edges, dtype=np.float64).reshape(3, 3)).copy()
@@ -170,6 +178,17 @@ class ForceField:
 
     def kernel_launches(self):
         return self._lib.FF_kernel_launches(self.ff)
+
+    def stencil_times(self):
+        """Per-level stencil kernel ms of the last timed evaluation."""
+        ms = (C.c_double * 16)()
+        n = self._lib.FF_stencil_times(self.ff, ms, 16)
+        return [ms[k] for k in range(n)]
+
+    def set_timing(self, enabled):
+        """True: eager launches with per-phase events (fills time_*);
+        False: replay of the captured CUDA graph."""
+        self._lib.FF_set_timing(self.ff, 1 if enabled else 0)
 
     def set_precision(self, precision):
         self._lib.FF_set_precision(self.ff, L.PRECISION_FP64 if precision == "fp64"
