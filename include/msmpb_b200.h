@@ -47,8 +47,11 @@ void FF_set_device(FF *ff, int device);
 double FF_energy_potentials(FF *ff, double (*force)[3], double (*position)[3],
                             double *weight, double *potential);
 
-/* Device-resident evaluation, asynchronous on `stream` (a cudaStream_t, NULL
- * = the library's own stream). position_d: N*3 doubles; charge_d: N doubles;
+/* Device-resident evaluation, asynchronous and ordered on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream). The launch sequence is
+ * captured once on a private stream and replayed as a CUDA graph on `stream`
+ * (timing off), or launched eagerly on `stream` with per-phase events
+ * (timing on). position_d: N*3 doubles; charge_d: N doubles;
  * weight: host array of maxLevel+1 doubles or NULL; force_d (N*3),
  * potential_d (N) and energy_d (1) are device outputs, each may be NULL.
  * Returns MSMPB_OK or an error code; kernel-side checks are reported by the

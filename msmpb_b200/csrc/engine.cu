@@ -130,6 +130,7 @@ class Plan : public FFDevice {
 
   int device_ = 0;
   cudaStream_t stream_ = nullptr;
+  cudaStream_t last_stream_ = nullptr;
   int N_ = 0, L_ = 0, nu_ = 0;
   int grid_[kMaxLevels + 2][3] = {};
   StencilShape sh_[kMaxLevels + 2] = {};
@@ -153,8 +154,11 @@ class Plan : public FFDevice {
       *ginv_ = nullptr, *pcs_ = nullptr, *gcs_ = nullptr;
   V4<T> *prel_ = nullptr, *gfrac_ = nullptr, *psorted_ = nullptr,
         *gsorted_ = nullptr, *pout_ = nullptr, *gout_ = nullptr;
+  // FP64 cell-relative positions for the close pairs of the mixed form
+  V4<double> *prel64_ = nullptr, *psorted64_ = nullptr;
+  static constexpr bool kMixed = sizeof(T) == 4;
   T *qg_[kMaxLevels + 2] = {}, *eg_[kMaxLevels + 2] = {};
-  T *padded_ = nullptr, *kh_[kMaxLevels + 2] = {};
+  T *padded_ = nullptr, *part_ = nullptr, *kh_[kMaxLevels + 2] = {};
   double *khat_top_ = nullptr;
   double2 *fft_ = nullptr;
   double *qparts_ = nullptr, *short_parts_ = nullptr, *grid_parts_ = nullptr,
@@ -215,7 +219,7 @@ int Plan<T>::init(const Tables &t, int device) {
   int err = set_tables(t);
   if (err) return err;
   // stencil shapes
-  size_t pad_max = 1;
+  size_t pad_max = 1, part_max = 1;
   for (int l = 1; l < L_; ++l) {
     StencilShape &s = sh_[l];
     for (int k = 0; k < 3; ++k) {
@@ -233,6 +237,8 @@ int Plan<T>::init(const Tables &t, int device) {
       stencil_padded_dims(s, tile_[l], fp64, s.P);
     }
     pad_max = std::max(pad_max, (size_t)s.P[0] * s.P[1] * s.P[2]);
+    if (tile_[l].nsplit > 1)
+      part_max = std::max(part_max, (size_t)tile_[l].nsplit * s.M[0] * s.M[1] * s.M[2]);
   }
   const size_t n = N_;
   nq_ = std::min(1024, std::max(1, (N_ + 255) / 256));
@@ -254,14 +260,20 @@ int Plan<T>::init(const Tables &t, int device) {
   a.want(&scan_tmp_, std::max(scan_temp_ints(ncp_), scan_temp_ints(ncg_)) * sizeof(int));
   for (V4<T> **b : {&prel_, &gfrac_, &psorted_, &gsorted_, &pout_, &gout_})
     a.want(b, n * sizeof(V4<T>));
+  if (kMixed) {
+    a.want(&prel64_, n * sizeof(V4<double>));
+    a.want(&psorted64_, n * sizeof(V4<double>));
+  }
   for (int l = 1; l <= L_; ++l) {
     size_t g = (size_t)grid_[l][0] * grid_[l][1] * grid_[l][2];
     a.want(&qg_[l], g * sizeof(T));
     a.want(&eg_[l], g * sizeof(T));
     if (l < L_)
-      a.want(&kh_[l], (size_t)sh_[l].S[0] * sh_[l].S[1] * sh_[l].S[2] * sizeof(T));
+      a.want(&kh_[l], (size_t)sh_[l].S[0] * sh_[l].S[1] *
+                          stencil_tap_pitch(sh_[l].S[2], !kMixed) * sizeof(T));
   }
   a.want(&padded_, pad_max * sizeof(T));
+  a.want(&part_, part_max * sizeof(T));
   size_t ntop = (size_t)grid_[L_][0] * grid_[L_][1] * grid_[L_][2];
   a.want(&khat_top_, ntop * sizeof(double));
   a.want(&fft_, ntop * sizeof(double2));
@@ -287,6 +299,14 @@ int Plan<T>::set_tables(const Tables &t) {
   pc_.inv_a0 = (T)(1. / p.a0);
   pc_.two_inv_a03 = (T)(2. / (p.a0 * p.a0 * p.a0));
   for (int k = 0; k < 16; ++k) pc_.tau[k] = (T)t.tau[k];
+  // pairs closer than 2.5 A (bonded and hydrogen-bonded distances) are
+  // summed in FP64 in the mixed form
+  pc_.close2 = kMixed ? (T)(2.5 * 2.5) : (T)0;
+  pc_.a02d = p.a0 * p.a0;
+  pc_.inv_a02d = 1. / (p.a0 * p.a0);
+  pc_.inv_a0d = 1. / p.a0;
+  pc_.two_inv_a03d = 2. / (p.a0 * p.a0 * p.a0);
+  for (int k = 0; k < 16; ++k) pc_.taud[k] = t.tau[k];
   for (int k = 0; k < 50; ++k) sc_.Q[k] = (T)t.Q[k];
   for (int k = 0; k < 11; ++k) J_[k] = t.J[k];
   return MSMPB_OK;
@@ -334,6 +354,7 @@ int Plan<T>::update(const Tables &t) {
           double v = 0;
           for (int c = 0; c < 3; ++c) v += p.A[r][c] * ((double)d[c] / geom_.nc[c]);
           o.shift[r] = (T)v;
+          o.shift64[r] = v;
         }
         offsets_.push_back(o);
       }
@@ -343,7 +364,14 @@ int Plan<T>::update(const Tables &t) {
   MSM_CUDA_TRY(cudaMemcpy(off_d_, offsets_.data(), noff_ * sizeof(CellOffset<T>),
                           cudaMemcpyHostToDevice));
   for (int l = 1; l < L_; ++l) {
-    std::vector<T> kh(t.khat[l].begin(), t.khat[l].end());
+    // rows of S2 taps padded to a 16-byte pitch (zeros), z fastest
+    const int S0 = sh_[l].S[0], S1 = sh_[l].S[1], S2 = sh_[l].S[2];
+    const int sp = stencil_tap_pitch(S2, !kMixed);
+    std::vector<T> kh((size_t)S0 * S1 * sp, T(0));
+    for (int i = 0; i < S0; ++i)
+      for (int j = 0; j < S1; ++j)
+        for (int k = 0; k < S2; ++k)
+          kh[((size_t)i * S1 + j) * sp + k] = (T)t.khat[l][((size_t)i * S1 + j) * S2 + k];
     MSM_CUDA_TRY(cudaMemcpy(kh_[l], kh.data(), kh.size() * sizeof(T),
                             cudaMemcpyHostToDevice));
   }
@@ -374,7 +402,7 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   launch_charge_stats(s, N_, q, qparts_, nq_);
   launch_qstats_final(s, qparts_, nq_, qstats_);
   launch_prep<T>(s, N_, pos, q, geom_, pcell_, gcell_, pcount_, gcount_, prel_,
-                 gfrac_, err_d_);
+                 gfrac_, prel64_, err_d_);
   launch_scan(s, pcount_, pstart_, ncp_, scan_tmp_);
   launch_scan(s, gcount_, gstart_, ncg_, scan_tmp_);
   launch_scatter(s, N_, pcell_, pstart_, pcursor_, pperm_);
@@ -382,10 +410,12 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   launch_segment_sort(s, ncp_, pstart_, pperm_);
   launch_segment_sort(s, ncg_, gstart_, gperm_);
   launch_gather<T>(s, N_, pperm_, prel_, pcell_, psorted_, pcs_, pinv_);
+  if (kMixed) launch_permute64(s, N_, pperm_, prel64_, psorted64_);
   launch_gather<T>(s, N_, gperm_, gfrac_, gcell_, gsorted_, gcs_, ginv_);
   nl += 3 + 6 + 2 + 2 + 2;
   mark(s, kPhasePair, tm);
-  launch_pair<T>(s, N_, psorted_, pcs_, pstart_, geom_, off_d_, noff_, pc_, pout_);
+  launch_pair<T>(s, N_, psorted_, psorted64_, pcs_, pstart_, geom_, off_d_, noff_,
+                 pc_, pout_);
   nl += 1;
   mark(s, kPhaseAnterp, tm);
   launch_anterpolate<T>(s, grid_[1], gsorted_, gstart_, sc_, qg_[1],
@@ -411,8 +441,9 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
     mark(s, kPhaseStencil, tm && l == L_ - 1);
     launch_pad<T>(s, sh_[l], qg_[l], padded_);
     if (tm) cudaEventRecord(lev_ev_[l][0], s);
-    launch_stencil<T>(s, sh_[l], tile_[l], padded_, kh_[l], sh_[l].S[2],
-                      (T)w[l], eg_[l]);
+    launch_stencil<T>(s, sh_[l], tile_[l], padded_, kh_[l],
+                      stencil_tap_pitch(sh_[l].S[2], !kMixed), (T)w[l], eg_[l],
+                      part_);
     if (tm) cudaEventRecord(lev_ev_[l][1], s);
     nl += 3;
   }
@@ -463,7 +494,10 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
 template <typename T>
 int Plan<T>::evaluate(const EvalRequest &r, double *energy) {
   MSM_CUDA_TRY(cudaSetDevice(device_));
-  cudaStream_t s = (r.host || !r.stream) ? stream_ : r.stream;
+  // Host calls run on the library's stream; device calls are ordered on the
+  // caller's stream (0 = the legacy default stream).
+  cudaStream_t s = r.host ? stream_ : r.stream;
+  last_stream_ = s;
   const double *pos = r.pos, *q = r.q;
   double *force = r.force, *phi = r.phi;
   if (r.host) {
@@ -524,11 +558,14 @@ int Plan<T>::launch_graph(const EvalRequest &r, cudaStream_t s,
     }
     have_graph_ = false;
     cudaGraph_t g = nullptr;
-    MSM_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    // capture on the private stream (the legacy default stream cannot be
+    // captured); the graph is then launched on the caller's stream
+    MSM_CUDA_TRY(cudaStreamSynchronize(stream_));
+    MSM_CUDA_TRY(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
     EvalRequest untimed = r;
     untimed.timing = false;
-    int st = enqueue(untimed, s, pos, q, force, phi, edev);
-    cudaError_t ce = cudaStreamEndCapture(s, &g);
+    int st = enqueue(untimed, stream_, pos, q, force, phi, edev);
+    cudaError_t ce = cudaStreamEndCapture(stream_, &g);
     if (st != MSMPB_OK || ce != cudaSuccess) {
       if (g) cudaGraphDestroy(g);
       cudaGetLastError();
@@ -551,6 +588,7 @@ template <typename T>
 int Plan<T>::sync() {
   MSM_CUDA_TRY(cudaSetDevice(device_));
   MSM_CUDA_TRY(cudaStreamSynchronize(stream_));
+  if (last_stream_ != stream_) MSM_CUDA_TRY(cudaStreamSynchronize(last_stream_));
   int flag = 0;
   MSM_CUDA_TRY(cudaMemcpy(&flag, err_d_, sizeof(int), cudaMemcpyDeviceToHost));
   if (flag) {

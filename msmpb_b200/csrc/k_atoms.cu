@@ -23,7 +23,8 @@ __global__ void __launch_bounds__(kThreads)
 k_prep(int N, const double *__restrict__ pos, const double *__restrict__ q,
        Geometry g, int *__restrict__ pcell, int *__restrict__ gcell,
        int *__restrict__ pcount, int *__restrict__ gcount,
-       V4<T> *__restrict__ prel, V4<T> *__restrict__ gfrac, int *err) {
+       V4<T> *__restrict__ prel, V4<T> *__restrict__ gfrac,
+       V4<double> *__restrict__ prel64, int *err) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double r0 = pos[3 * i], r1 = pos[3 * i + 1], r2 = pos[3 * i + 2];
@@ -56,12 +57,23 @@ k_prep(int N, const double *__restrict__ pos, const double *__restrict__ q,
   gcell[i] = gc;
   atomicAdd(pcount + pc, 1);
   atomicAdd(gcount + gc, 1);
+  const double rx = matvec_row(g.A, 0, frac[0], frac[1], frac[2]);
+  const double ry = matvec_row(g.A, 1, frac[0], frac[1], frac[2]);
+  const double rz = matvec_row(g.A, 2, frac[0], frac[1], frac[2]);
   V4<T> a;
-  a.x = (T)matvec_row(g.A, 0, frac[0], frac[1], frac[2]);
-  a.y = (T)matvec_row(g.A, 1, frac[0], frac[1], frac[2]);
-  a.z = (T)matvec_row(g.A, 2, frac[0], frac[1], frac[2]);
+  a.x = (T)rx;
+  a.y = (T)ry;
+  a.z = (T)rz;
   a.w = (T)qi;
   prel[i] = a;
+  if (prel64) {
+    V4<double> a64;
+    a64.x = rx;
+    a64.y = ry;
+    a64.z = rz;
+    a64.w = qi;
+    prel64[i] = a64;
+  }
   V4<T> b;
   b.x = (T)t[0];
   b.y = (T)t[1];
@@ -218,6 +230,13 @@ k_gather(int N, const int *__restrict__ perm, const V4<T> *__restrict__ src,
   inv[i] = k;
 }
 
+__global__ void __launch_bounds__(kThreads)
+k_permute64(int N, const int *__restrict__ perm, const V4<double> *__restrict__ src,
+            V4<double> *__restrict__ dst) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < N) dst[k] = src[perm[k]];
+}
+
 // Per atom in input order: F_i = w0 F_short + q_i E_i and
 // phi_i = w0 (q_i c1 - Q c2 - q_i gamma0/a0 + phi_short) + phi_long.
 template <typename T>
@@ -226,8 +245,7 @@ k_combine(CombineArgs a, const int *__restrict__ pinv,
           const int *__restrict__ ginv, const V4<T> *__restrict__ pout,
           const V4<T> *__restrict__ gout) {
   __shared__ double red[kThreads];
-  double qsum = 0.;
-  for (int b = 0; b < a.nqparts; ++b) qsum += a.qparts[2 * b];
+  const double qsum = a.qstats[0];  // reduced by k_qstats_final
   double e = 0.;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < a.N) {
@@ -319,9 +337,15 @@ inline int blocks_for(long n, int threads) {
 template <typename T>
 void launch_prep(cudaStream_t s, int N, const double *pos, const double *q,
                  const Geometry &g, int *pcell, int *gcell, int *pcount,
-                 int *gcount, V4<T> *prel, V4<T> *gfrac, int *err) {
+                 int *gcount, V4<T> *prel, V4<T> *gfrac, V4<double> *prel64,
+                 int *err) {
   k_prep<T><<<blocks_for(N, kThreads), kThreads, 0, s>>>(
-      N, pos, q, g, pcell, gcell, pcount, gcount, prel, gfrac, err);
+      N, pos, q, g, pcell, gcell, pcount, gcount, prel, gfrac, prel64, err);
+}
+
+void launch_permute64(cudaStream_t s, int N, const int *perm,
+                      const V4<double> *src, V4<double> *dst) {
+  k_permute64<<<blocks_for(N, kThreads), kThreads, 0, s>>>(N, perm, src, dst);
 }
 
 void launch_charge_stats(cudaStream_t s, int N, const double *q,
@@ -378,7 +402,8 @@ void launch_energy_total(cudaStream_t s, const EnergyArgs &a) {
 #define MSM_INST_ATOMS(T)                                                     \
   template void launch_prep<T>(cudaStream_t, int, const double *,            \
                                const double *, const Geometry &, int *,      \
-                               int *, int *, int *, V4<T> *, V4<T> *, int *); \
+                               int *, int *, int *, V4<T> *, V4<T> *,         \
+                               V4<double> *, int *);                          \
   template void launch_gather<T>(cudaStream_t, int, const int *,             \
                                  const V4<T> *, const int *, V4<T> *, int *,  \
                                  int *);                                      \

@@ -244,6 +244,12 @@ k_interpolate(int N, int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
   int zi[NU];
 #pragma unroll
   for (int i = 0; i < NU; ++i) zi[i] = pwrap(mz - (i - NU / 2), M2);
+  // The sums run over e - e_c, e_c the potential at the atom's own grid
+  // point: the derivative weights sum to zero and the value weights to one,
+  // so the results are unchanged in exact arithmetic, while the rounded
+  // products are of differences (about h |E|) rather than of potentials,
+  // which are much larger than h |E|.
+  const T ec = grid[((long)mx * M1 + my) * M2 + mz];
   T phi = 0, ex = 0, ey = 0, ez = 0;
   for (int a = 0; a < NU; ++a) {
     const int gx = pwrap(mx - (a - NU / 2), M0);
@@ -254,7 +260,7 @@ k_interpolate(int N, int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
       T s0 = 0, s1 = 0;
 #pragma unroll
       for (int i = 0; i < NU; ++i) {
-        const T e = row[zi[i]];
+        const T e = row[zi[i]] - ec;
         s0 += wz[i] * e;
         s1 += dz[i] * e;
       }
@@ -272,7 +278,7 @@ k_interpolate(int N, int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
   r.x = (T)(g.Ai[0] * gxv + g.Ai[3] * gyv + g.Ai[6] * gzv);
   r.y = (T)(g.Ai[1] * gxv + g.Ai[4] * gyv + g.Ai[7] * gzv);
   r.z = (T)(g.Ai[2] * gxv + g.Ai[5] * gyv + g.Ai[8] * gzv);
-  r.w = phi;
+  r.w = phi + ec;
   out[k] = r;
 }
 
@@ -320,26 +326,23 @@ k_prolong(int F0, int F1, int F2, const T *__restrict__ coarse,
   long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (long)F0 * F1 * F2) return;
   const int z = idx % F2, y = (idx / F2) % F1, x = idx / ((long)F1 * F2);
+  // tap n = x - 2m in [-NU/2, NU/2]: the first n with the parity of x
+  const int nx0 = -NU / 2 + ((x + NU / 2) & 1);
+  const int ny0 = -NU / 2 + ((y + NU / 2) & 1);
+  const int nz0 = -NU / 2 + ((z + NU / 2) & 1);
   T acc = 0;
-  for (int a = 0; a <= NU; ++a) {
-    const int n = a - NU / 2;
-    if (((x - n) & 1) != 0) continue;
-    const int cx = pwrap((x - n) / 2, C0);
+  for (int n = nx0; n <= NU / 2; n += 2) {
+    const int cx = pwrap((x - n) >> 1, C0);
     T ay = 0;
-    for (int b = 0; b <= NU; ++b) {
-      const int nb = b - NU / 2;
-      if (((y - nb) & 1) != 0) continue;
-      const int cy = pwrap((y - nb) / 2, C1);
+    for (int nb = ny0; nb <= NU / 2; nb += 2) {
+      const int cy = pwrap((y - nb) >> 1, C1);
       const T *row = coarse + ((long)cx * C1 + cy) * C2;
       T az = 0;
-      for (int c = 0; c <= NU; ++c) {
-        const int nc = c - NU / 2;
-        if (((z - nc) & 1) != 0) continue;
-        az += (T)js.J[c] * row[pwrap((z - nc) / 2, C2)];
-      }
-      ay += (T)js.J[b] * az;
+      for (int nc = nz0; nc <= NU / 2; nc += 2)
+        az += (T)js.J[nc + NU / 2] * row[pwrap((z - nc) >> 1, C2)];
+      ay += (T)js.J[nb + NU / 2] * az;
     }
-    acc += (T)js.J[a] * ay;
+    acc += (T)js.J[n + NU / 2] * ay;
   }
   fine[idx] += acc;
 }

@@ -11,6 +11,14 @@
 // per-atom potential and force fall out directly).
 //
 // V(r) = 1/r - tau(r^2/a0^2 - 1)/a0,  F_i = q_i q_j (-1/r^3 - 2 tau'(s)/a0^3) r.
+//
+// Mixed form: FP32 arithmetic with compensated (Kahan) accumulation across
+// neighbour cells, except pairs closer than sqrt(close2) (2.5 A): their
+// displacement is formed from FP64 cell-relative positions and FP64 cell
+// offsets and the pair is summed in FP64. Those pairs carry the largest
+// forces, and an FP32 coordinate rounds by up to 2.4e-7 A, which is a
+// relative error of 2.4e-7 on a 1 A bond; everywhere else the FP32 result
+// is within rounding of the FP64 one.
 #include "kernels.h"
 
 namespace msm {
@@ -18,15 +26,18 @@ namespace {
 
 constexpr int kPairThreads = 128;
 
-template <typename T, int NU, bool COMPENSATE>
+template <typename T, int NU, bool COMPENSATE, bool CLOSE>
 __global__ void __launch_bounds__(kPairThreads)
-k_pair(int N, const V4<T> *__restrict__ ps, const int *__restrict__ pcs,
-       const int *__restrict__ start, int nc0, int nc1, int nc2,
-       const CellOffset<T> *__restrict__ off, int noff, PairConsts<T> pc,
-       V4<T> *__restrict__ out) {
+k_pair(int N, const V4<T> *__restrict__ ps, const V4<double> *__restrict__ ps64,
+       const int *__restrict__ pcs, const int *__restrict__ start, int nc0,
+       int nc1, int nc2, const CellOffset<T> *__restrict__ off, int noff,
+       PairConsts<T> pc, V4<T> *__restrict__ out) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= N) return;
   const V4<T> ai = ps[k];
+  V4<double> ai64;
+  if (CLOSE) ai64 = ps64[k];
+  double cfx = 0., cfy = 0., cfz = 0., cph = 0.;  // close pairs (FP64)
   const int c = pcs[k];
   const int cz = c % nc2, cy = (c / nc2) % nc1, cx = c / (nc1 * nc2);
   Acc<T> fx, fy, fz, ph;
@@ -48,6 +59,27 @@ k_pair(int N, const V4<T> *__restrict__ ps, const int *__restrict__ pcs,
       const T dx = aj.x + sx, dy = aj.y + sy, dz = aj.z + sz;
       const T r2 = dx * dx + dy * dy + dz * dz;
       if (r2 < pc.a02 && j != k) {
+        if (CLOSE && r2 < pc.close2) {
+          const V4<double> aj = ps64[j];
+          const double ex = (aj.x + co.shift64[0]) - ai64.x;
+          const double ey = (aj.y + co.shift64[1]) - ai64.y;
+          const double ez = (aj.z + co.shift64[2]) - ai64.z;
+          const double d2 = ex * ex + ey * ey + ez * ez;
+          const double sd = d2 * pc.inv_a02d - 1.0;
+          double ts = pc.taud[NU - 1], t1 = 0.0;
+#pragma unroll
+          for (int m = NU - 2; m >= 0; --m) {
+            t1 = ts + sd * t1;
+            ts = pc.taud[m] + sd * ts;
+          }
+          const double rinv = 1.0 / sqrt(d2);
+          cph += aj.w * (rinv - ts * pc.inv_a0d);
+          const double cf = aj.w * (-rinv * rinv * rinv - t1 * pc.two_inv_a03d);
+          cfx += cf * ex;
+          cfy += cf * ey;
+          cfz += cf * ez;
+          continue;
+        }
         const T s = r2 * pc.inv_a02 - T(1);
         T ts = pc.tau[NU - 1], t1 = T(0);
 #pragma unroll
@@ -76,45 +108,55 @@ k_pair(int N, const V4<T> *__restrict__ ps, const int *__restrict__ pcs,
     }
   }
   V4<T> r;
-  r.x = ai.w * fx.value();
-  r.y = ai.w * fy.value();
-  r.z = ai.w * fz.value();
-  r.w = ph.value();
+  if (CLOSE) {
+    const double qi = ai64.w;
+    r.x = (T)(qi * ((double)fx.value() + cfx));
+    r.y = (T)(qi * ((double)fy.value() + cfy));
+    r.z = (T)(qi * ((double)fz.value() + cfz));
+    r.w = (T)((double)ph.value() + cph);
+  } else {
+    r.x = ai.w * fx.value();
+    r.y = ai.w * fy.value();
+    r.z = ai.w * fz.value();
+    r.w = ph.value();
+  }
   out[k] = r;
 }
 
 template <typename T, int NU>
-void launch_nu(cudaStream_t s, int N, const V4<T> *ps, const int *pcs,
-               const int *start, const Geometry &g, const CellOffset<T> *off,
-               int noff, const PairConsts<T> &pc, V4<T> *out) {
+void launch_nu(cudaStream_t s, int N, const V4<T> *ps, const V4<double> *ps64,
+               const int *pcs, const int *start, const Geometry &g,
+               const CellOffset<T> *off, int noff, const PairConsts<T> &pc,
+               V4<T> *out) {
   int blocks = (N + kPairThreads - 1) / kPairThreads;
   if (blocks < 1) blocks = 1;
-  k_pair<T, NU, true><<<blocks, kPairThreads, 0, s>>>(
-      N, ps, pcs, start, g.nc[0], g.nc[1], g.nc[2], off, noff, pc, out);
+  constexpr bool kMixed = sizeof(T) == 4;
+  k_pair<T, NU, kMixed, kMixed><<<blocks, kPairThreads, 0, s>>>(
+      N, ps, ps64, pcs, start, g.nc[0], g.nc[1], g.nc[2], off, noff, pc, out);
 }
 
 }  // namespace
 
 template <typename T>
-void launch_pair(cudaStream_t s, int N, const V4<T> *ps, const int *pcs,
-                 const int *start, const Geometry &g,
+void launch_pair(cudaStream_t s, int N, const V4<T> *ps, const V4<double> *ps64,
+                 const int *pcs, const int *start, const Geometry &g,
                  const CellOffset<T> *off, int noff, const PairConsts<T> &pc,
                  V4<T> *out) {
   switch (pc.nu) {
-    case 4: launch_nu<T, 4>(s, N, ps, pcs, start, g, off, noff, pc, out); break;
-    case 6: launch_nu<T, 6>(s, N, ps, pcs, start, g, off, noff, pc, out); break;
-    case 8: launch_nu<T, 8>(s, N, ps, pcs, start, g, off, noff, pc, out); break;
-    default: launch_nu<T, 10>(s, N, ps, pcs, start, g, off, noff, pc, out); break;
+    case 4: launch_nu<T, 4>(s, N, ps, ps64, pcs, start, g, off, noff, pc, out); break;
+    case 6: launch_nu<T, 6>(s, N, ps, ps64, pcs, start, g, off, noff, pc, out); break;
+    case 8: launch_nu<T, 8>(s, N, ps, ps64, pcs, start, g, off, noff, pc, out); break;
+    default: launch_nu<T, 10>(s, N, ps, ps64, pcs, start, g, off, noff, pc, out); break;
   }
 }
 
 template void launch_pair<float>(cudaStream_t, int, const V4<float> *,
-                                 const int *, const int *, const Geometry &,
-                                 const CellOffset<float> *, int,
+                                 const V4<double> *, const int *, const int *,
+                                 const Geometry &, const CellOffset<float> *, int,
                                  const PairConsts<float> &, V4<float> *);
 template void launch_pair<double>(cudaStream_t, int, const V4<double> *,
-                                  const int *, const int *, const Geometry &,
-                                  const CellOffset<double> *, int,
+                                  const V4<double> *, const int *, const int *,
+                                  const Geometry &, const CellOffset<double> *, int,
                                   const PairConsts<double> &, V4<double> *);
 
 }  // namespace msm

@@ -29,6 +29,10 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kMaxTemplatedS = 33;
 
+inline int blocks_for(long n) {
+  return (int)std::max<long>(1, (n + kThreads - 1) / kThreads);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_pad(StencilShape sh, const T *__restrict__ q, T *__restrict__ p) {
@@ -97,26 +101,52 @@ __device__ __forceinline__ void stage_plane(const T *__restrict__ P,
     const int row = t / wv, c = t - row * wv;
     cp_async16(slice + row * W + c * V, src + (long)row * sh.P[2] + c * V);
   }
-  cp_async_commit();
 }
 
+// Copies one tap plane (S1 rows of SP, contiguous in global) to shared memory.
+template <typename T>
+__device__ __forceinline__ void stage_taps(const T *__restrict__ kh, int plane,
+                                           int n, T *dst) {
+  constexpr int V = 16 / sizeof(T);
+  const int nthreads = blockDim.x * blockDim.y;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const T *src = kh + (long)plane * n;
+  for (int t = tid; t < n / V; t += nthreads) cp_async16(dst + t * V, src + t * V);
+}
+
+// Split over tap planes: CTA z-index = x-tile + ntx * chunk index; chunk k
+// sums tap planes i in [k*chunk, min(S0, (k+1)*chunk)). With one chunk the
+// result is added to e directly; otherwise each chunk stores its partial sum
+// in part[k] and k_split_reduce adds them in fixed order (deterministic).
+//
+// Taps: kh holds S0 x S1 rows of SP (S rounded up to 16 bytes, zero padded).
+// The tap planes in use live in a shared ring of TX+1 planes: step pi uses
+// planes i_lo+pi-TX+1 .. i_lo+pi and prefetches plane i_lo+pi+1 into the one
+// free slot, together with the next input plane.
 template <typename T, int S, int R, int TX>
 __global__ void __launch_bounds__(kThreads)
 k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
-                const T *__restrict__ kh, int khz, T w, T *__restrict__ e) {
+                const T *__restrict__ kh, T w, T *__restrict__ e,
+                int ntx, int chunk, T *__restrict__ part) {
   constexpr int V = 16 / sizeof(T);
+  constexpr int SP = (S + V - 1) / V * V;        // tap row pitch
   constexpr int RL = R + S - 1;                  // row values per thread
   constexpr int RLV = (RL + V - 1) / V * V;      // rounded to 16-byte loads
+  constexpr int NRING = TX + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *smem = reinterpret_cast<T *>(smem_raw);
   const int NZ = blockDim.x, TY = blockDim.y;
   const int tz = threadIdx.x, ty = threadIdx.y;
   const int S0 = sh.S[0], S1 = sh.S[1];
-  const int z0 = blockIdx.x * NZ * R, y0 = blockIdx.y * TY, x0 = blockIdx.z * TX;
+  const int xt = blockIdx.z % ntx, kc = blockIdx.z / ntx;
+  const int i_lo = kc * chunk, i_hi = min(S0, i_lo + chunk);
+  const int z0 = blockIdx.x * NZ * R, y0 = blockIdx.y * TY, x0 = xt * TX;
   const int H = TY + S1 - 1;
   const int W = (NZ * R + S - 1 + V - 1) / V * V;
   const int slice_elems = H * W + V;  // +V: tail reads of the last row
-  T *buf[2] = {smem, smem + slice_elems};
+  const int tap_elems = S1 * SP;
+  T *buf0 = smem, *buf1 = smem + slice_elems;
+  T *ring = smem + 2 * slice_elems;
 
   T acc[TX][R];
 #pragma unroll
@@ -124,17 +154,24 @@ k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[a][r] = T(0);
 
-  const int nplanes = TX + S0 - 1;
-  stage_plane(P, sh, x0, y0, z0, H, W, buf[0]);
+  const int nplanes = TX + (i_hi - i_lo) - 1;
+  const int p0 = x0 + i_lo;  // first input plane
+  stage_plane(P, sh, p0, y0, z0, H, W, buf0);
+  stage_taps(kh, i_lo, tap_elems, ring + (i_lo % NRING) * tap_elems);
+  cp_async_commit();
   for (int pi = 0; pi < nplanes; ++pi) {
     if (pi + 1 < nplanes) {
-      stage_plane(P, sh, x0 + pi + 1, y0, z0, H, W, buf[(pi + 1) & 1]);
+      stage_plane(P, sh, p0 + pi + 1, y0, z0, H, W, (pi & 1) ? buf0 : buf1);
+      const int inext = i_lo + pi + 1;
+      if (inext < i_hi)
+        stage_taps(kh, inext, tap_elems, ring + (inext % NRING) * tap_elems);
+      cp_async_commit();
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
     }
     __syncthreads();
-    const T *slice = buf[pi & 1];
+    const T *slice = (pi & 1) ? buf1 : buf0;
     for (int j = 0; j < S1; ++j) {
       const T *rp = slice + (ty + j) * W + tz * R;
       T row[RLV];
@@ -154,14 +191,31 @@ k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
       }
 #pragma unroll
       for (int xo = 0; xo < TX; ++xo) {
-        const int i = pi - xo;
-        if (i < 0 || i >= S0) continue;  // uniform across the CTA
-        const T *kp = kh + ((long)i * S1 + j) * khz;
+        const int i = i_lo + pi - xo;
+        if (i < i_lo || i >= i_hi) continue;  // uniform across the CTA
+        const T *kp = ring + (i % NRING) * tap_elems + j * SP;
 #pragma unroll
-        for (int k = 0; k < S; ++k) {
-          const T t = __ldg(kp + k);
+        for (int kk = 0; kk < SP; kk += V) {
+          T t[V];
+          if constexpr (sizeof(T) == 4) {
+            const float4 t4 = *reinterpret_cast<const float4 *>(kp + kk);
+            t[0] = (T)t4.x;
+            t[1] = (T)t4.y;
+            t[2] = (T)t4.z;
+            t[3] = (T)t4.w;
+          } else {
+            const double2 t2 = *reinterpret_cast<const double2 *>(kp + kk);
+            t[0] = (T)t2.x;
+            t[1] = (T)t2.y;
+          }
 #pragma unroll
-          for (int r = 0; r < R; ++r) acc[xo][r] = fma(t, row[r + k], acc[xo][r]);
+          for (int u = 0; u < V; ++u) {
+            if (kk + u < S) {
+#pragma unroll
+              for (int r = 0; r < R; ++r)
+                acc[xo][r] = fma(t[u], row[r + kk + u], acc[xo][r]);
+            }
+          }
         }
       }
     }
@@ -169,17 +223,34 @@ k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
   }
   const int y = y0 + ty;
   if (y >= sh.M[1]) return;
+  const long mtot = (long)sh.M[0] * sh.M[1] * sh.M[2];
 #pragma unroll
   for (int xo = 0; xo < TX; ++xo) {
     const int x = x0 + xo;
     if (x >= sh.M[0]) continue;
-    T *out = e + ((long)x * sh.M[1] + y) * sh.M[2];
+    const long row0 = ((long)x * sh.M[1] + y) * sh.M[2];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int z = z0 + tz * R + r;
-      if (z < sh.M[2]) out[z] += w * acc[xo][r];
+      if (z >= sh.M[2]) continue;
+      if (part)
+        part[kc * mtot + row0 + z] = acc[xo][r];
+      else
+        e[row0 + z] += w * acc[xo][r];
     }
   }
+}
+
+// e += w * sum_k part[k], chunks added in index order
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_split_reduce(long n, int nsplit, const T *__restrict__ part, T w,
+               T *__restrict__ e) {
+  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n) return;
+  T s = part[idx];
+  for (int k = 1; k < nsplit; ++k) s += part[k * n + idx];
+  e[idx] += w * s;
 }
 
 template <typename T> struct TileDefaults;
@@ -188,16 +259,27 @@ template <> struct TileDefaults<double> { static constexpr int R = 4, TX = 4; };
 
 template <typename T, int S>
 void launch_tiled(cudaStream_t s, const StencilShape &sh, const StencilTile &tl,
-                  const T *p, const T *kh, int khz, T w, T *e) {
+                  const T *p, const T *kh, int khz, T w, T *e, T *part) {
   constexpr int R = TileDefaults<T>::R, TX = TileDefaults<T>::TX;
   constexpr int V = 16 / sizeof(T);
   const int H = tl.ty + sh.S[1] - 1;
   const int W = (tl.nz * R + S - 1 + V - 1) / V * V;
-  const size_t smem = 2 * (size_t)(H * W + V) * sizeof(T);
+  const size_t smem = (2 * (size_t)(H * W + V) +
+                       (size_t)(TX + 1) * sh.S[1] * stencil_tap_pitch(S, sizeof(T) == 8)) *
+                      sizeof(T);
+  const int ntx = (sh.M[0] + TX - 1) / TX;
+  const int nsplit = std::max(1, tl.nsplit);
+  const int chunk = (sh.S[0] + nsplit - 1) / nsplit;
   dim3 block(tl.nz, tl.ty);
   dim3 grid((sh.M[2] + tl.nz * R - 1) / (tl.nz * R), (sh.M[1] + tl.ty - 1) / tl.ty,
-            (sh.M[0] + TX - 1) / TX);
-  k_stencil_tiled<T, S, R, TX><<<grid, block, smem, s>>>(sh, p, kh, khz, w, e);
+            ntx * nsplit);
+  (void)khz;  // the tiled kernel reads rows of the padded pitch
+  k_stencil_tiled<T, S, R, TX><<<grid, block, smem, s>>>(
+      sh, p, kh, w, e, ntx, chunk, nsplit > 1 ? part : nullptr);
+  if (nsplit > 1) {
+    const long n = (long)sh.M[0] * sh.M[1] * sh.M[2];
+    k_split_reduce<T><<<blocks_for(n), kThreads, 0, s>>>(n, nsplit, part, w, e);
+  }
 }
 
 // Levels (and plans) that share an instantiation need the largest request:
@@ -220,33 +302,45 @@ void set_smem_attr(int bytes) {
   X(15) X(16) X(17) X(18) X(19) X(20) X(21) X(22) X(23) X(24) X(25) X(26)    \
   X(27) X(28) X(29) X(30) X(31) X(32) X(33)
 
-inline int blocks_for(long n) {
-  return (int)std::max<long>(1, (n + kThreads - 1) / kThreads);
-}
-
 }  // namespace
 
 StencilTile stencil_default_tile(const StencilShape &sh, bool fp64) {
   const int R = fp64 ? TileDefaults<double>::R : TileDefaults<float>::R;
+  const int TX = fp64 ? TileDefaults<double>::TX : TileDefaults<float>::TX;
   StencilTile t;
-  // z: smallest thread count whose span covers M2 in the fewest tiles
-  int best_nz = 1;
-  double best_cost = 1e30;
-  for (int nz = 2; nz <= 8; ++nz) {
-    const int span = nz * R;
-    const int tiles = (sh.M[2] + span - 1) / span;
-    const double cost = (double)tiles * span / sh.M[2] + 0.02 * (8 - nz);
-    if (cost < best_cost) {
-      best_cost = cost;
-      best_nz = nz;
+  t.tx = TX;
+  // Tile shape: least padding waste, then least shared-memory traffic per
+  // output (halo ratio), with at least two warps per CTA where possible.
+  double best = 1e30;
+  for (int nz = 1; nz <= 16; ++nz)
+    for (int ty : {16, 12, 8, 6, 4, 2, 1}) {
+      const int th = nz * ty;
+      if (th > kThreads || (ty > sh.M[1] && ty > 1)) continue;
+      const int span = nz * R;
+      if (span > sh.M[2] + R - 1 && nz > 1) continue;
+      const double wz = (double)((sh.M[2] + span - 1) / span * span) / sh.M[2];
+      const double wy = (double)((sh.M[1] + ty - 1) / ty * ty) / sh.M[1];
+      const double halo = (double)(ty + sh.S[1] - 1) * (span + sh.S[2] - 1) / (ty * span);
+      const double score = wz * wy * (1.0 + 0.03 * halo) + (th < 64 ? 0.25 : 0.0);
+      if (score < best - 1e-12) {
+        best = score;
+        t.nz = nz;
+        t.ty = ty;
+      }
     }
-  }
-  t.nz = std::min(best_nz, std::max(1, (sh.M[2] + R - 1) / R));
-  int ty = std::max(1, std::min(16, kThreads / t.nz));
-  if (ty > sh.M[1]) ty = sh.M[1];
-  t.ty = ty;
-  t.tx = fp64 ? TileDefaults<double>::TX : TileDefaults<float>::TX;
+  // Split the tap planes over CTAs until the grid fills the GPU (about four
+  // CTAs per SM); every chunk keeps at least one plane.
+  const long tiles = (long)((sh.M[2] + t.nz * R - 1) / (t.nz * R)) *
+                     ((sh.M[1] + t.ty - 1) / t.ty) * ((sh.M[0] + TX - 1) / TX);
+  int ns = (int)std::min<long>(sh.S[0], std::max<long>(1, (148L * 4 + tiles - 1) / tiles));
+  const int chunk = (sh.S[0] + ns - 1) / ns;
+  t.nsplit = (sh.S[0] + chunk - 1) / chunk;
   return t;
+}
+
+int stencil_tap_pitch(int S2, bool fp64) {
+  const int V = fp64 ? 2 : 4;
+  return (S2 + V - 1) / V * V;
 }
 
 bool stencil_templated(const StencilShape &sh) {
@@ -273,7 +367,9 @@ int stencil_prepare(const StencilShape &sh, const StencilTile &tl) {
   constexpr int V = 16 / sizeof(T);
   const int H = tl.ty + sh.S[1] - 1;
   const int W = (tl.nz * R + sh.S[2] - 1 + V - 1) / V * V;
-  const int bytes = 2 * (H * W + V) * (int)sizeof(T);
+  const int bytes = (2 * (H * W + V) +
+                     (tl.tx + 1) * sh.S[1] * stencil_tap_pitch(sh.S[2], sizeof(T) == 8)) *
+                    (int)sizeof(T);
   if (bytes > 200 * 1024) return -1;
   switch (sh.S[2]) {
 #define X(SS) \
@@ -292,7 +388,7 @@ void launch_pad(cudaStream_t s, const StencilShape &sh, const T *q, T *p) {
 
 template <typename T>
 void launch_stencil(cudaStream_t s, const StencilShape &sh, const StencilTile &tl,
-                    const T *p, const T *kh, int khz, T w, T *e) {
+                    const T *p, const T *kh, int khz, T w, T *e, T *part) {
   if (!stencil_templated(sh) || tl.nz <= 0) {
     long n = (long)sh.M[0] * sh.M[1] * sh.M[2];
     k_stencil_simple<T><<<blocks_for(n), kThreads, 0, s>>>(sh, p, kh, khz, w, e);
@@ -300,7 +396,7 @@ void launch_stencil(cudaStream_t s, const StencilShape &sh, const StencilTile &t
   }
   switch (sh.S[2]) {
 #define X(SS) \
-  case SS: launch_tiled<T, SS>(s, sh, tl, p, kh, khz, w, e); break;
+  case SS: launch_tiled<T, SS>(s, sh, tl, p, kh, khz, w, e, part); break;
     MSM_S_CASES(X)
 #undef X
   }
@@ -312,10 +408,11 @@ template void launch_pad<double>(cudaStream_t, const StencilShape &,
                                  const double *, double *);
 template void launch_stencil<float>(cudaStream_t, const StencilShape &,
                                     const StencilTile &, const float *,
-                                    const float *, int, float, float *);
+                                    const float *, int, float, float *, float *);
 template void launch_stencil<double>(cudaStream_t, const StencilShape &,
                                      const StencilTile &, const double *,
-                                     const double *, int, double, double *);
+                                     const double *, int, double, double *,
+                                     double *);
 template int stencil_prepare<float>(const StencilShape &, const StencilTile &);
 template int stencil_prepare<double>(const StencilShape &, const StencilTile &);
 

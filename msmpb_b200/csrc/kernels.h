@@ -26,13 +26,20 @@ struct CellOffset {
   int pad;
   T shift[3];
   T pad2;
+  double shift64[3];  // the same offset in FP64 (close pairs)
+  double pad3;
 };
 
-// Short-range kernel constants
+// Short-range kernel constants. Pairs closer than sqrt(close2) are summed
+// in FP64 from FP64 cell-relative positions in the mixed form: their
+// forces are the largest and most sensitive to position rounding.
 template <typename T>
 struct PairConsts {
   T a02, inv_a02, inv_a0, two_inv_a03;
   T tau[16];
+  T close2;
+  double a02d, inv_a02d, inv_a0d, two_inv_a03d;
+  double taud[16];
   int nu;
 };
 
@@ -44,10 +51,15 @@ struct SplineConsts {
 };
 
 // ---- atoms: binning and sorting (k_atoms.cu) ----
+// prel64 (may be null): FP64 position relative to the pair-cell origin, q
 template <typename T>
 void launch_prep(cudaStream_t s, int N, const double *pos, const double *q,
                  const Geometry &g, int *pcell, int *gcell, int *pcount,
-                 int *gcount, V4<T> *prel, V4<T> *gfrac, int *err);
+                 int *gcount, V4<T> *prel, V4<T> *gfrac, V4<double> *prel64,
+                 int *err);
+// dst[k] = src[perm[k]]
+void launch_permute64(cudaStream_t s, int N, const int *perm,
+                      const V4<double> *src, V4<double> *dst);
 void launch_charge_stats(cudaStream_t s, int N, const double *q,
                          double *partials, int nparts);
 // exclusive scan of n ints into out[0..n] (out[n] = total)
@@ -92,10 +104,13 @@ void launch_qstats_final(cudaStream_t s, const double *qparts, int nqparts,
                          double *qstats);
 
 // ---- short-range pair sum (k_pair.cu) ----
+// pos64_sorted: FP64 cell-relative positions in the same order (used for
+// close pairs in the mixed form; may be null for T = double)
 template <typename T>
 void launch_pair(cudaStream_t s, int N, const V4<T> *pos_sorted,
-                 const int *cell_sorted, const int *cell_start,
-                 const Geometry &g, const CellOffset<T> *offsets, int noff,
+                 const V4<double> *pos64_sorted, const int *cell_sorted,
+                 const int *cell_start, const Geometry &g,
+                 const CellOffset<T> *offsets, int noff,
                  const PairConsts<T> &pc, V4<T> *out);
 
 // ---- grid transfers (k_grid.cu) ----
@@ -131,9 +146,12 @@ struct StencilShape {
 // CTA tile of the stencil sweep: nz x ty threads, each with tx x R outputs
 struct StencilTile {
   int nz = 0, ty = 0, tx = 0;
+  int nsplit = 1;  // CTAs sharing one output tile, each over a run of tap planes
 };
 StencilTile stencil_default_tile(const StencilShape &sh, bool fp64);
 bool stencil_templated(const StencilShape &sh);
+// row pitch of the tap array: S2 rounded up to 16 bytes (rows zero padded)
+int stencil_tap_pitch(int S2, bool fp64);
 // padded input dims that keep every tile load of `tile` inside the buffer
 void stencil_padded_dims(const StencilShape &sh, const StencilTile &tile,
                          bool fp64, int P[3]);
@@ -142,11 +160,12 @@ template <typename T>
 int stencil_prepare(const StencilShape &sh, const StencilTile &tile);
 template <typename T>
 void launch_pad(cudaStream_t s, const StencilShape &sh, const T *q, T *padded);
-// kh: S0 x S1 x khz taps (z fastest)
+// kh: S0 x S1 x khz taps (z fastest); part: tile.nsplit x M0*M1*M2
+// scratch for split tap sums (unused when nsplit == 1)
 template <typename T>
 void launch_stencil(cudaStream_t s, const StencilShape &sh,
                     const StencilTile &tile, const T *padded, const T *kh,
-                    int khz, T weight, T *e);
+                    int khz, T weight, T *e, T *part);
 
 // ---- top-level FFT solve (k_fft.cu) ----
 bool top_solve_supported(const int M[3]);
