@@ -105,6 +105,7 @@ class Plan : public FFDevice {
 
  private:
   int set_tables(const Tables &t);
+  int tune_levels(size_t pad_cap, size_t part_cap);
   int launch_graph(const EvalRequest &r, cudaStream_t s, const double *pos,
                    const double *q, double *force, double *phi, double *edev);
   int enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
@@ -122,6 +123,12 @@ class Plan : public FFDevice {
     if (timing) cudaEventRecord(ev_[phase], s);
   }
   bool debug_sync_ = std::getenv("MSMPB_DEBUG_SYNC") != nullptr;
+  // MSMPB_PAIR=cells selects the cell-staged pair kernel with compacted
+  // hits (default: one thread per atom)
+  int pair_variant_ = [] {
+    const char *v = std::getenv("MSMPB_PAIR");
+    return (v && v[0] == 'c') ? 0 : 1;
+  }();
   // MSMPB_ANTERP=simple selects the one-point-per-thread anterpolation
   int anterp_variant_ = [] {
     const char *v = std::getenv("MSMPB_ANTERP");
@@ -135,6 +142,7 @@ class Plan : public FFDevice {
   int grid_[kMaxLevels + 2][3] = {};
   StencilShape sh_[kMaxLevels + 2] = {};
   StencilTile tile_[kMaxLevels + 2] = {};
+  bool tune_[kMaxLevels + 2] = {};
   Geometry geom_{};
   PairConsts<T> pc_{};
   SplineConsts<T> sc_{};
@@ -239,6 +247,17 @@ int Plan<T>::init(const Tables &t, int device) {
     pad_max = std::max(pad_max, (size_t)s.P[0] * s.P[1] * s.P[2]);
     if (tile_[l].nsplit > 1)
       part_max = std::max(part_max, (size_t)tile_[l].nsplit * s.M[0] * s.M[1] * s.M[2]);
+    // levels worth tuning: size the scratch for every candidate tile
+    const double gflop = 2e-9 * s.M[0] * s.M[1] * s.M[2] * (double)s.S[0] * s.S[1] * s.S[2];
+    tune_[l] = tile_[l].nz > 0 && gflop >= 1.0 && stencil_tuning_enabled();
+    if (tune_[l])
+      for (const StencilTile &c : stencil_candidates(s, fp64)) {
+        int P[3];
+        stencil_padded_dims(s, c, fp64, P);
+        pad_max = std::max(pad_max, (size_t)P[0] * P[1] * P[2]);
+        if (c.nsplit > 1)
+          part_max = std::max(part_max, (size_t)c.nsplit * s.M[0] * s.M[1] * s.M[2]);
+      }
   }
   const size_t n = N_;
   nq_ = std::min(1024, std::max(1, (N_ + 255) / 256));
@@ -286,7 +305,28 @@ int Plan<T>::init(const Tables &t, int device) {
   a.want(&err_d_, sizeof(int));
   if ((err = a.commit())) return err;
   MSM_CUDA_TRY(cudaMemset(err_d_, 0, sizeof(int)));
-  return update(t);
+  if ((err = update(t))) return err;
+  return tune_levels(pad_max, part_max);
+}
+
+// Empirical tile choice for the levels with the most work (see tune.cu)
+template <typename T>
+int Plan<T>::tune_levels(size_t pad_cap, size_t part_cap) {
+  MSM_CUDA_TRY(cudaMemsetAsync(padded_, 0, pad_cap * sizeof(T), stream_));
+  const int khz_fp64 = !kMixed;
+  for (int l = 1; l < L_; ++l) {
+    if (!tune_[l]) continue;
+    double ms = 0;
+    StencilTile best = stencil_autotune<T>(
+        stream_, device_, sh_[l], tile_[l], padded_, pad_cap, kh_[l],
+        stencil_tap_pitch(sh_[l].S[2], khz_fp64), eg_[l], part_, part_cap, &ms);
+    if (stencil_prepare<T>(sh_[l], best) < 0) continue;
+    tile_[l] = best;
+    stencil_padded_dims(sh_[l], best, !kMixed, sh_[l].P);
+  }
+  MSM_CUDA_TRY(cudaStreamSynchronize(stream_));
+  cudaGetLastError();
+  return MSMPB_OK;
 }
 
 // Constants that depend only on the parameter set (not on the box)
@@ -414,12 +454,16 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   launch_gather<T>(s, N_, gperm_, gfrac_, gcell_, gsorted_, gcs_, ginv_);
   nl += 3 + 6 + 2 + 2 + 2;
   mark(s, kPhasePair, tm);
-  launch_pair<T>(s, N_, psorted_, psorted64_, pcs_, pstart_, geom_, off_d_, noff_,
-                 pc_, pout_);
+  if (pair_variant_ == 0 && pair_cells_supported(noff_, N_))
+    launch_pair_cells<T>(s, ncp_, psorted_, psorted64_, pstart_, geom_, off_d_,
+                         noff_, pc_, pout_, err_d_);
+  else
+    launch_pair<T>(s, N_, psorted_, psorted64_, pcs_, pstart_, geom_, off_d_,
+                   noff_, pc_, pout_);
   nl += 1;
   mark(s, kPhaseAnterp, tm);
   launch_anterpolate<T>(s, grid_[1], gsorted_, gstart_, sc_, qg_[1],
-                        anterp_variant_, err_d_);
+                        anterp_variant_, err_d_, N_);
   nl += 1;
   mark(s, kPhaseRestrict, tm);
   for (int l = 1; l < L_; ++l) {

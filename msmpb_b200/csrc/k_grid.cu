@@ -393,7 +393,7 @@ struct AnterpTile {
 // z extent: the candidate (<= 64) that wastes the fewest points; y fills
 // up to 512 threads (at most 8 rows); staging capacity fills the budget.
 template <typename T>
-AnterpTile anterp_tile(const int M[3], int nu) {
+AnterpTile anterp_tile(const int M[3], int nu, long natoms) {
   AnterpTile t{};
   int best = 32;
   double best_waste = 1e30;
@@ -409,7 +409,12 @@ AnterpTile anterp_tile(const int M[3], int nu) {
   t.by = std::max(1, std::min(std::min(8, M[1]), 512 / t.bz));
   const int ncell = (t.by + nu - 1) * (t.bz + nu - 1);
   const size_t fixed = 4 * (size_t)((ncell + 1 + 3) & ~3);
+  // capacity: twice the expected atoms of one halo slab (at least 256),
+  // at most the budget; denser slabs are staged in row chunks
+  const double per_cell = (double)natoms / ((double)M[0] * M[1] * M[2]);
+  const int want = (int)(2.0 * per_cell * ncell) + 64;
   int cap = (int)((kAnterpSmemBudget - fixed - 64) / (3 * nu * sizeof(T) + 4));
+  cap = std::min(cap, std::max(256, want));
   cap &= ~3;
   t.cap = std::max(4, cap);
   t.smem = fixed + 4 * (size_t)t.cap + 3 * (size_t)nu * t.cap * sizeof(T);
@@ -421,14 +426,14 @@ AnterpTile anterp_tile(const int M[3], int nu) {
 template <typename T>
 void launch_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
                         const int *cell_start, const SplineConsts<T> &sc,
-                        T *grid, int variant, int *err) {
+                        T *grid, int variant, int *err, long natoms) {
   if (variant == 1) {  // one grid point per thread, runtime loops
     long n = (long)M[0] * M[1] * M[2];
     MSM_NU_SWITCH(sc.nu, (k_anterpolate<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
                              M[0], M[1], M[2], atoms, cell_start, sc, grid)));
     return;
   }
-  const AnterpTile t = anterp_tile<T>(M, sc.nu);
+  const AnterpTile t = anterp_tile<T>(M, sc.nu, natoms);
   dim3 block(t.bz, t.by);
   dim3 g((M[2] + t.bz - 1) / t.bz, (M[1] + t.by - 1) / t.by,
          (M[0] + kAnterpBX - 1) / kAnterpBX);
@@ -489,7 +494,7 @@ void launch_grid_dot(cudaStream_t s, size_t n, const T *a, const T *b,
   template void launch_anterpolate<T>(cudaStream_t, const int *,              \
                                       const V4<T> *, const int *,             \
                                       const SplineConsts<T> &, T *, int,      \
-                                      int *);                                 \
+                                      int *, long);                           \
   template void anterpolate_prepare<T>();                                     \
   template void launch_interpolate<T>(cudaStream_t, int, const int *,         \
                                       const V4<T> *, const int *, const T *,  \

@@ -38,6 +38,10 @@ k_pair(int N, const V4<T> *__restrict__ ps, const V4<double> *__restrict__ ps64,
   V4<double> ai64;
   if (CLOSE) ai64 = ps64[k];
   double cfx = 0., cfy = 0., cfz = 0., cph = 0.;  // close pairs (FP64)
+  // close pairs found during the sweep, evaluated in FP64 after it
+  constexpr int kCloseList = 12;
+  int close_j[CLOSE ? kCloseList : 1], close_o[CLOSE ? kCloseList : 1];
+  int nclose = 0;
   const int c = pcs[k];
   const int cz = c % nc2, cy = (c / nc2) % nc1, cx = c / (nc1 * nc2);
   Acc<T> fx, fy, fz, ph;
@@ -59,7 +63,13 @@ k_pair(int N, const V4<T> *__restrict__ ps, const V4<double> *__restrict__ ps64,
       const T dx = aj.x + sx, dy = aj.y + sy, dz = aj.z + sz;
       const T r2 = dx * dx + dy * dy + dz * dz;
       if (r2 < pc.a02 && j != k) {
-        if (CLOSE && r2 < pc.close2) {
+        if (CLOSE && r2 < pc.close2 && nclose < kCloseList) {
+          close_j[nclose] = j;
+          close_o[nclose] = o;
+          ++nclose;
+          continue;
+        }
+        if (CLOSE && r2 < pc.close2) {  // list full: evaluate now
           const V4<double> aj = ps64[j];
           const double ex = (aj.x + co.shift64[0]) - ai64.x;
           const double ey = (aj.y + co.shift64[1]) - ai64.y;
@@ -105,6 +115,30 @@ k_pair(int N, const V4<T> *__restrict__ ps, const V4<double> *__restrict__ ps64,
       fy.s += py;
       fz.s += pz;
       ph.s += pp;
+    }
+  }
+  if constexpr (CLOSE) {
+    for (int t = 0; t < nclose; ++t) {
+      const int j = close_j[t];
+      const CellOffset<T> &co = off[close_o[t]];
+      const V4<double> aj = ps64[j];
+      const double ex = (aj.x + co.shift64[0]) - ai64.x;
+      const double ey = (aj.y + co.shift64[1]) - ai64.y;
+      const double ez = (aj.z + co.shift64[2]) - ai64.z;
+      const double d2 = ex * ex + ey * ey + ez * ez;
+      const double sd = d2 * pc.inv_a02d - 1.0;
+      double ts = pc.taud[NU - 1], t1 = 0.0;
+#pragma unroll
+      for (int m = NU - 2; m >= 0; --m) {
+        t1 = ts + sd * t1;
+        ts = pc.taud[m] + sd * ts;
+      }
+      const double rinv = 1.0 / sqrt(d2);
+      cph += aj.w * (rinv - ts * pc.inv_a0d);
+      const double cf = aj.w * (-rinv * rinv * rinv - t1 * pc.two_inv_a03d);
+      cfx += cf * ex;
+      cfy += cf * ey;
+      cfz += cf * ez;
     }
   }
   V4<T> r;

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "device.cuh"
 
 namespace msm {
@@ -113,12 +115,20 @@ void launch_pair(cudaStream_t s, int N, const V4<T> *pos_sorted,
                  const CellOffset<T> *offsets, int noff,
                  const PairConsts<T> &pc, V4<T> *out);
 
+// cell-staged form with compacted hits (k_pair_cells.cu): one CTA per cell
+bool pair_cells_supported(int noff, long natoms);
+template <typename T>
+void launch_pair_cells(cudaStream_t s, int ncell, const V4<T> *pos_sorted,
+                       const V4<double> *pos64_sorted, const int *cell_start,
+                       const Geometry &g, const CellOffset<T> *offsets, int noff,
+                       const PairConsts<T> &pc, V4<T> *out, int *err);
+
 // ---- grid transfers (k_grid.cu) ----
 // variant 0: slab-staged gather; 1: one grid point per thread (reference form)
 template <typename T>
 void launch_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
                         const int *cell_start, const SplineConsts<T> &sc,
-                        T *grid, int variant, int *err);
+                        T *grid, int variant, int *err, long natoms);
 template <typename T>
 void anterpolate_prepare();
 template <typename T>
@@ -160,6 +170,14 @@ template <typename T>
 int stencil_prepare(const StencilShape &sh, const StencilTile &tile);
 template <typename T>
 void launch_pad(cudaStream_t s, const StencilShape &sh, const T *q, T *padded);
+// tile autotuner (tune.cu)
+bool stencil_tuning_enabled();
+std::vector<StencilTile> stencil_candidates(const StencilShape &sh, bool fp64);
+template <typename T>
+StencilTile stencil_autotune(cudaStream_t s, int device, const StencilShape &sh,
+                             const StencilTile &fallback, const T *padded,
+                             size_t padded_cap, const T *kh, int khz, T *e,
+                             T *part, size_t part_cap, double *best_ms);
 // kh: S0 x S1 x khz taps (z fastest); part: tile.nsplit x M0*M1*M2
 // scratch for split tap sums (unused when nsplit == 1)
 template <typename T>

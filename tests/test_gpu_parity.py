@@ -151,6 +151,23 @@ def test_level_weights(precision):
     assert rel_rms(phi, po) < tp
 
 
+@pytest.mark.parametrize("variant", [("MSMPB_PAIR", "cells"), ("MSMPB_ANTERP", "simple")])
+@pytest.mark.parametrize("case", ["spceN900_L3_M6_a8_nu8", "changaN512_L2_M8_a0.25_nu6",
+                                  "CsClN16_auto"])
+def test_alternative_kernels(case, variant, monkeypatch):
+    """The alternative kernels (cell-staged pair sum with compacted hits, one
+    thread per grid point for anterpolation) give the same results."""
+    monkeypatch.setenv(*variant)
+    d = load(case)
+    for precision in ("fp64", "mixed"):
+        ff = make_ff(d, precision)
+        e, f = ff.energy(d["pos"])
+        te, tf, _ = TOL[precision]
+        assert abs(e - float(d["energy"])) / abs(float(d["energy"])) < te
+        assert force_err(f, d["force"], d["q"], d["edges"]) < tf
+        ff.close()
+
+
 def test_repeat_and_charge_update():
     """Repeated calls give identical results; charge edits between calls
     are seen (FF_new keeps the caller's pointer, code/forcefield0.c:172)."""
