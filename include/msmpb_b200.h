@@ -86,6 +86,43 @@ void FF_set_timing(FF *ff, int enabled);
  * on every SM for about `milliseconds` (the FP32-pipe roofline peak). */
 double msmpb_measure_fp32_tflops(int device, int milliseconds);
 
+/* Size of the fixed scratch array of msmpb_level_stencil_noalloc (per device). */
+#define MSMPB_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* One periodic level stencil that allocates no memory. No counterpart in the
+ * reference, which allocates its work arrays in FF_build.
+ *
+ * For callers that cannot let a library allocate device memory: MD engines
+ * and frameworks that own all of it through their own pool allocator (a
+ * cudaMalloc behind the pool escapes its budget, and cudaMalloc / cudaFree
+ * may synchronise the whole device in the middle of their step). Computes,
+ * in FP64, asynchronously on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream) of the current device,
+ *   e[x] += weight * sum_{d in [0,S)^3} k[d] * q[(x + d - S/2) mod M]
+ * (S/2 rounded down per axis) for x in [0,M)^3: the direct stencil of one
+ * level of FF_energy_device. q (charge_grid_d) and e (potential_grid_d) are
+ * M0*M1*M2 doubles, k (stencil_d) S0*S1*S2 doubles, all row-major with the
+ * last index fastest, on the current device; 1 <= S[a] <= M[a]. e is added
+ * to, so clear it for a plain result.
+ *
+ * Scratch (tap copy, padded grid, partial sums) lives in one array of
+ * MSMPB_NOALLOC_SCRATCH_BYTES compiled into the library. The tap copy and
+ * the padded grid, about S0*S1*S2 + (M0+S0+3)(M1+S1+15)(M2+S2+5) doubles,
+ * must fit in it (a 96^3 grid with a 25^3 stencil fits); larger sizes
+ * return MSMPB_ERR_UNSUPPORTED and launch nothing. Nothing in the array has
+ * to start at zero: every call rewrites what it reads.
+ *
+ * The first call on a device looks up the array's address there
+ * (cudaGetSymbolAddress, which may load the library's GPU code); make it
+ * before any stream capture. All calls on a device share the array: calls
+ * whose GPU work overlaps race, so order them on one stream or with events.
+ * Returns MSMPB_OK, MSMPB_ERR_ARGUMENT, MSMPB_ERR_UNSUPPORTED, or
+ * MSMPB_ERR_NODEVICE / MSMPB_ERR_CUDA when a CUDA call fails. */
+int msmpb_level_stencil_noalloc(const int M[3], const int S[3],
+                                const double *charge_grid_d,
+                                const double *stencil_d, double weight,
+                                double *potential_grid_d, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -39,6 +39,7 @@ EXPORTED = [
     "FF_get_precision", "FF_set_device", "FF_energy_potentials",
     "FF_energy_device", "FF_sync", "FF_phase_times", "FF_kernel_launches",
     "FF_stencil_times", "FF_set_timing", "msmpb_measure_fp32_tflops",
+    "msmpb_level_stencil_noalloc",
 ]
 
 _lib = None
