@@ -123,11 +123,14 @@ class Plan : public FFDevice {
     if (timing) cudaEventRecord(ev_[phase], s);
   }
   bool debug_sync_ = std::getenv("MSMPB_DEBUG_SYNC") != nullptr;
-  // MSMPB_PAIR=cells selects the cell-staged pair kernel with compacted
-  // hits (default: one thread per atom)
+  // Pair sum: 2 = clusters (default), MSMPB_PAIR=thread selects one
+  // thread per atom, MSMPB_PAIR=cells the cell-staged kernel with
+  // compacted hits
   int pair_variant_ = [] {
     const char *v = std::getenv("MSMPB_PAIR");
-    return (v && v[0] == 'c') ? 0 : 1;
+    if (v && v[0] == 'c') return 0;
+    if (v && v[0] == 't') return 1;
+    return 2;
   }();
   // MSMPB_ANTERP=simple selects the one-point-per-thread anterpolation
   int anterp_variant_ = [] {
@@ -149,8 +152,12 @@ class Plan : public FFDevice {
   double J_[11] = {};
   double coeff1_ = 0, coeff2_ = 0, gamma0_a0_ = 0;
   int ncp_ = 0, ncg_ = 0, noff_ = 0;
+  int ncol_ = 0, maxcl_ = 0, ncoloff_ = 0, K2_ = 0;
+  bool clusters_ok_ = false;
+  double cz_[3] = {};
   int nq_ = 0, ncomb_ = 0, ngrid_ = 0;
   std::vector<CellOffset<T>> offsets_;
+  std::vector<ColumnOffset> coloffs_;
   Arena arena_;
   // device buffers
   double *pos_s_ = nullptr, *q_s_ = nullptr, *force_s_ = nullptr,
@@ -172,6 +179,13 @@ class Plan : public FFDevice {
   double *qparts_ = nullptr, *short_parts_ = nullptr, *grid_parts_ = nullptr,
          *qstats_ = nullptr, *energy_ = nullptr;
   CellOffset<T> *off_d_ = nullptr;
+  // clusters
+  ColumnOffset *coloff_d_ = nullptr;
+  int *clcount_ = nullptr, *clstart_ = nullptr;
+  V4<T> *cpos_ = nullptr;
+  V4<double> *cpos64_ = nullptr;
+  ClusterInfo *cinfo_ = nullptr;
+  UnitBox *cubox_ = nullptr;
   int *err_d_ = nullptr;
   // graph
   cudaGraphExec_t exec_ = nullptr;
@@ -220,6 +234,8 @@ int Plan<T>::init(const Tables &t, int device) {
     geom_.M1[k] = t.grid[1][k];
   }
   ncp_ = (int)ncell;
+  ncol_ = geom_.nc[0] * geom_.nc[1];
+  maxcl_ = cluster_capacity(N_, ncol_);
   ncg_ = grid_[1][0] * grid_[1][1] * grid_[1][2];
   if (!top_solve_supported(p.top)) return MSMPB_ERR_UNSUPPORTED;
   top_solve_prepare();
@@ -302,6 +318,13 @@ int Plan<T>::init(const Tables &t, int device) {
   a.want(&qstats_, 2 * sizeof(double));
   a.want(&energy_, sizeof(double));
   a.want(&off_d_, kMaxNeighbourOffsets * sizeof(CellOffset<T>));
+  a.want(&coloff_d_, kMaxColumnOffsets * sizeof(ColumnOffset));
+  a.want(&clcount_, (ncol_ + 1) * sizeof(int));
+  a.want(&clstart_, (ncol_ + 1) * sizeof(int));
+  a.want(&cpos_, (size_t)maxcl_ * 8 * sizeof(V4<T>));
+  if (kMixed) a.want(&cpos64_, (size_t)maxcl_ * 8 * sizeof(V4<double>));
+  a.want(&cinfo_, (size_t)maxcl_ * sizeof(ClusterInfo));
+  a.want(&cubox_, (size_t)maxcl_ * 2 * sizeof(UnitBox));
   a.want(&err_d_, sizeof(int));
   if ((err = a.commit())) return err;
   MSM_CUDA_TRY(cudaMemset(err_d_, 0, sizeof(int)));
@@ -400,6 +423,34 @@ int Plan<T>::update(const Tables &t) {
       }
   if ((int)offsets_.size() > kMaxNeighbourOffsets) return MSMPB_ERR_UNSUPPORTED;
   noff_ = (int)offsets_.size();
+  // neighbour columns of the cluster form: (du, dv) with the same bounds
+  // (and, for orthorhombic boxes, the same gap pruning in x and y); along
+  // the column every cell within K2 of the cluster's cells is a candidate
+  coloffs_.clear();
+  for (int du = -K[0]; du <= K[0]; ++du)
+    for (int dv = -K[1]; dv <= K[1]; ++dv) {
+      if (ortho) {
+        const double gx = std::max(0, std::abs(du) - 1) * std::fabs(p.A[0][0]) / geom_.nc[0];
+        const double gy = std::max(0, std::abs(dv) - 1) * std::fabs(p.A[1][1]) / geom_.nc[1];
+        if (gx * gx + gy * gy >= p.a0 * p.a0) continue;
+      }
+      ColumnOffset c{};
+      c.du = du;
+      c.dv = dv;
+      for (int r = 0; r < 3; ++r)
+        c.base[r] = p.A[r][0] * ((double)du / geom_.nc[0]) +
+                    p.A[r][1] * ((double)dv / geom_.nc[1]);
+      coloffs_.push_back(c);
+    }
+  ncoloff_ = (int)coloffs_.size();
+  K2_ = K[2];
+  for (int r = 0; r < 3; ++r) cz_[r] = p.A[r][2] / geom_.nc[2];
+  // the close-pair record packs the column index in 23 bits and the image
+  // index along the column in 8
+  clusters_ok_ = ncoloff_ <= kMaxColumnOffsets && K2_ / geom_.nc[2] + 2 < 120;
+  if (clusters_ok_)
+    MSM_CUDA_TRY(cudaMemcpy(coloff_d_, coloffs_.data(), ncoloff_ * sizeof(ColumnOffset),
+                            cudaMemcpyHostToDevice));
   MSM_CUDA_TRY(cudaSetDevice(device_));
   MSM_CUDA_TRY(cudaMemcpy(off_d_, offsets_.data(), noff_ * sizeof(CellOffset<T>),
                           cudaMemcpyHostToDevice));
@@ -447,19 +498,49 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   launch_scan(s, gcount_, gstart_, ncg_, scan_tmp_);
   launch_scatter(s, N_, pcell_, pstart_, pcursor_, pperm_);
   launch_scatter(s, N_, gcell_, gstart_, gcursor_, gperm_);
-  launch_segment_sort(s, ncp_, pstart_, pperm_);
+  launch_segment_sort_z<T>(s, ncp_, pstart_, pperm_, prel_);
   launch_segment_sort(s, ncg_, gstart_, gperm_);
   launch_gather<T>(s, N_, pperm_, prel_, pcell_, psorted_, pcs_, pinv_);
   if (kMixed) launch_permute64(s, N_, pperm_, prel64_, psorted64_);
   launch_gather<T>(s, N_, gperm_, gfrac_, gcell_, gsorted_, gcs_, ginv_);
   nl += 3 + 6 + 2 + 2 + 2;
   mark(s, kPhasePair, tm);
-  if (pair_variant_ == 0 && pair_cells_supported(noff_, N_))
+  if (pair_variant_ == 2 && clusters_ok_) {
+    const V4<double> *src64 =
+        kMixed ? psorted64_ : reinterpret_cast<const V4<double> *>(psorted_);
+    launch_column_clusters(s, ncol_, geom_.nc[2], pstart_, clcount_);
+    launch_scan(s, clcount_, clstart_, ncol_, scan_tmp_);
+    launch_cluster_fill<T>(s, maxcl_, ncol_, geom_.nc[2], pstart_, clstart_, pcs_,
+                           src64, cz_, cpos_, cpos64_, cinfo_, cubox_);
+    PairClusterArgs<T> ca{};
+    ca.maxcl = maxcl_;
+    ca.ncol = ncol_;
+    ca.nc0 = geom_.nc[0];
+    ca.nc1 = geom_.nc[1];
+    ca.nc2 = geom_.nc[2];
+    ca.K2 = K2_;
+    ca.ncoloff = ncoloff_;
+    const double rb = std::sqrt((double)pc_.a02) * (1.0 + 1e-4) + 1e-6;
+    ca.rbox2 = (float)(rb * rb);
+    for (int r = 0; r < 3; ++r) ca.cz[r] = cz_[r];
+    ca.start = pstart_;
+    ca.clstart = clstart_;
+    ca.coloff = coloff_d_;
+    ca.info = cinfo_;
+    ca.ubox = cubox_;
+    ca.cpos = cpos_;
+    ca.cpos64 = cpos64_;
+    ca.out = pout_;
+    ca.err = err_d_;
+    launch_pair_clusters<T>(s, ca, pc_);
+    nl += 1 + 3 + 1;
+  } else if (pair_variant_ == 0 && pair_cells_supported(noff_, N_)) {
     launch_pair_cells<T>(s, ncp_, psorted_, psorted64_, pstart_, geom_, off_d_,
                          noff_, pc_, pout_, err_d_);
-  else
+  } else {
     launch_pair<T>(s, N_, psorted_, psorted64_, pcs_, pstart_, geom_, off_d_,
                    noff_, pc_, pout_);
+  }
   nl += 1;
   mark(s, kPhaseAnterp, tm);
   launch_anterpolate<T>(s, grid_[1], gsorted_, gstart_, sc_, qg_[1],

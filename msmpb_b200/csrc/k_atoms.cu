@@ -217,6 +217,31 @@ k_segment_sort(int ncell, const int *__restrict__ start, int *__restrict__ perm)
   }
 }
 
+// Orders each pair cell's atoms along z (key[atom].z, the position relative
+// to the cell origin), ties by atom index: every column of cells becomes one
+// z-ordered run, and the order depends only on the input.
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_segment_sort_z(int ncell, const int *__restrict__ start, int *__restrict__ perm,
+                 const V4<T> *__restrict__ key) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  int b = start[c], e = start[c + 1];
+  for (int k = b + 1; k < e; ++k) {
+    const int v = perm[k];
+    const T kv = key[v].z;
+    int j = k - 1;
+    while (j >= b) {
+      const int pj = perm[j];
+      const T kj = key[pj].z;
+      if (kj < kv || (kj == kv && pj < v)) break;
+      perm[j + 1] = pj;
+      --j;
+    }
+    perm[j + 1] = v;
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_gather(int N, const int *__restrict__ perm, const V4<T> *__restrict__ src,
@@ -380,6 +405,13 @@ void launch_segment_sort(cudaStream_t s, int ncell, const int *start,
 }
 
 template <typename T>
+void launch_segment_sort_z(cudaStream_t s, int ncell, const int *start,
+                           int *perm, const V4<T> *key) {
+  k_segment_sort_z<T><<<blocks_for(ncell, kThreads), kThreads, 0, s>>>(ncell, start,
+                                                                       perm, key);
+}
+
+template <typename T>
 void launch_gather(cudaStream_t s, int N, const int *perm, const V4<T> *src,
                    const int *cell, V4<T> *dst, int *cell_sorted, int *inv) {
   k_gather<T><<<blocks_for(N, kThreads), kThreads, 0, s>>>(
@@ -409,7 +441,9 @@ void launch_energy_total(cudaStream_t s, const EnergyArgs &a) {
                                  int *);                                      \
   template void launch_combine<T>(cudaStream_t, const CombineArgs &,         \
                                   const int *, const int *, const V4<T> *,    \
-                                  const V4<T> *, int);
+                                  const V4<T> *, int);                        \
+  template void launch_segment_sort_z<T>(cudaStream_t, int, const int *,     \
+                                         int *, const V4<T> *);
 MSM_INST_ATOMS(float)
 MSM_INST_ATOMS(double)
 

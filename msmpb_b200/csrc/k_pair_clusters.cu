@@ -1,0 +1,450 @@
+// Short-range pair sum over atom clusters (the same sum as k_pair.cu:
+// code/forcefield1.c:240-321 over the pairs of code/forcefield0.c:21-164).
+//
+// Layout. Pair cells are columns (cx, cy) of cells cz, z fastest, and every
+// cell is sorted along z, so each column is one z-ordered run of atoms. A
+// cluster is 8 consecutive atoms of a column; its atoms are stored relative
+// to the origin of the cell of its first atom (FP32 in the mixed form, plus
+// an FP64 copy for close pairs), padded with far-away, uncharged dummies. A
+// unit is half a cluster (4 atoms) with its own bounding box.
+//
+// Sweep. One warp per i-cluster; lane = ii + 8 jq holds i-atom ii and
+// j-atom jq of the current unit (an 8 x 4 pair tile per step). For every
+// neighbour column (host list) and periodic image along the column, the
+// candidate units are those of the clusters whose cells lie within K2 cells
+// of the i-cluster's cells; they are tested 32 at a time, one per lane, box
+// against box, the passing ones queued in shared memory with their FP32
+// image shift, and the tiles of the queue evaluated by the whole warp. Every
+// atom pair within the cutoff is summed once from each side (gather form:
+// no atomics, fixed order, deterministic); per-column partial sums are added
+// with compensation in the mixed form, and pairs closer than sqrt(close2)
+// are queued per lane and summed in FP64 after the sweep.
+#include "kernels.h"
+
+namespace msm {
+namespace {
+
+constexpr int kWarps = 4;  // i-clusters per CTA
+constexpr int kCloseCap = 8;
+constexpr float kFar = 1e15f;
+
+template <typename T> struct V3 { T x, y, z; };
+
+// Bounding box test with a relative margin that covers the FP32 rounding of
+// boxes and shifts (the exact per-pair test follows).
+__device__ __forceinline__ bool box_near(const float4 &ic, const float4 &ih,
+                                         const float4 &jc, const float4 &jh,
+                                         float sx, float sy, float sz, float r2) {
+  const float gx = fmaxf(fabsf(jc.x + sx - ic.x) - ih.x - jh.x, 0.f);
+  const float gy = fmaxf(fabsf(jc.y + sy - ic.y) - ih.y - jh.y, 0.f);
+  const float gz = fmaxf(fabsf(jc.z + sz - ic.z) - ih.z - jh.z, 0.f);
+  return gx * gx + gy * gy + gz * gz < r2;
+}
+
+__device__ __forceinline__ int floor_div(int a, int n) {
+  return a >= 0 ? a / n : -((-a + n - 1) / n);
+}
+
+// ---- cluster build: 8 threads per cluster ----
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_cluster_fill(int maxcl, int ncol, int nc2, const int *__restrict__ start,
+               const int *__restrict__ clstart, const int *__restrict__ pcs,
+               const V4<double> *__restrict__ src64, double cz0, double cz1,
+               double cz2, V4<T> *__restrict__ cpos, V4<double> *__restrict__ cpos64,
+               ClusterInfo *__restrict__ info, UnitBox *__restrict__ ubox) {
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int u = (int)(s >> 3), l = (int)(s & 7);
+  const int total = clstart[ncol];
+  const bool valid = u < maxcl && u < total;
+  float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
+  int n = 0, a0 = 0, czf = 0, col = 0;
+  if (valid) {
+    int a = 0, b = ncol;  // last column with clstart[col] <= u
+    while (b - a > 1) {
+      const int m = (a + b) >> 1;
+      if (clstart[m] <= u) a = m; else b = m;
+    }
+    col = a;
+    const int cs = start[col * nc2], ce = start[(col + 1) * nc2];
+    a0 = cs + 8 * (u - clstart[col]);
+    n = min(8, ce - a0);
+    czf = pcs[a0] % nc2;
+    V4<T> p;
+    if (l < n) {
+      const V4<double> r = src64[a0 + l];
+      const double dz = (double)(pcs[a0 + l] % nc2 - czf);
+      V4<double> c;
+      c.x = r.x + dz * cz0;
+      c.y = r.y + dz * cz1;
+      c.z = r.z + dz * cz2;
+      c.w = r.w;
+      p.x = (T)c.x;
+      p.y = (T)c.y;
+      p.z = (T)c.z;
+      p.w = (T)c.w;
+      if (cpos64) cpos64[s] = c;
+      lo[0] = hi[0] = (float)p.x;
+      lo[1] = hi[1] = (float)p.y;
+      lo[2] = hi[2] = (float)p.z;
+    } else {
+      p.x = p.y = p.z = (T)kFar;
+      p.w = T(0);
+      if (cpos64) cpos64[s] = V4<double>{(double)kFar, (double)kFar, (double)kFar, 0.};
+    }
+    cpos[s] = p;
+  }
+  // half boxes (4 lanes), then the whole cluster (8 lanes)
+  float hlo[3], hhi[3];
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 1; o < 4; o <<= 1) {
+      lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+    }
+    hlo[k] = lo[k];
+    hhi[k] = hi[k];
+    lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], 4));
+    hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], 4));
+  }
+  if (!valid) return;
+  if ((l & 3) == 0) {
+    UnitBox b;
+    if (l < n) {
+      b.c = make_float4(0.5f * (hlo[0] + hhi[0]), 0.5f * (hlo[1] + hhi[1]),
+                        0.5f * (hlo[2] + hhi[2]), __int_as_float(czf));
+      b.h = make_float4(0.5f * (hhi[0] - hlo[0]), 0.5f * (hhi[1] - hlo[1]),
+                        0.5f * (hhi[2] - hlo[2]), 0.f);
+    } else {  // empty unit: never near anything
+      b.c = make_float4(kFar, kFar, kFar, __int_as_float(czf));
+      b.h = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    ubox[2 * u + (l >> 2)] = b;
+  }
+  if (l == 0) {
+    ClusterInfo ci;
+    ci.first = a0;
+    ci.n = n;
+    ci.col = col;
+    ci.czf = czf;
+    ci.czl = pcs[a0 + n - 1] % nc2;
+    ci.pad[0] = ci.pad[1] = ci.pad[2] = 0;
+    ci.c = make_float4(0.5f * (lo[0] + hi[0]), 0.5f * (lo[1] + hi[1]),
+                       0.5f * (lo[2] + hi[2]), 0.f);
+    ci.h = make_float4(0.5f * (hi[0] - lo[0]), 0.5f * (hi[1] - lo[1]),
+                       0.5f * (hi[2] - lo[2]), 0.f);
+    info[u] = ci;
+  }
+}
+
+__global__ void k_column_clusters(int ncol, int nc2, const int *__restrict__ start,
+                                  int *__restrict__ count) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  count[c] = (start[(c + 1) * nc2] - start[c * nc2] + 7) >> 3;
+}
+
+template <typename T, int NU>
+__device__ __forceinline__ void pair_terms(const PairConsts<T> &pc, T r2, T qj,
+                                           T &pot, T &fs) {
+  const T s = r2 * pc.inv_a02 - T(1);
+  T ts = pc.tau[NU - 1], t1 = T(0);
+#pragma unroll
+  for (int m = NU - 2; m >= 0; --m) {
+    t1 = ts + s * t1;
+    ts = pc.tau[m] + s * ts;
+  }
+  const T rinv = rsqrt_t<T>(r2);
+  pot = qj * (rinv - ts * pc.inv_a0);
+  fs = qj * (-rinv * rinv * rinv - t1 * pc.two_inv_a03);
+}
+
+// One pair in FP64 from FP64 cluster-frame positions and the FP64 shift of
+// the j cluster's frame (close pairs of the mixed form).
+template <int NU>
+__device__ __forceinline__ void close_pair64(const PairConsts<float> &pc,
+                                             const V4<double> &ai, const V4<double> &aj,
+                                             double sx, double sy, double sz,
+                                             double &fx, double &fy, double &fz,
+                                             double &p) {
+  const double ex = (aj.x + sx) - ai.x;
+  const double ey = (aj.y + sy) - ai.y;
+  const double ez = (aj.z + sz) - ai.z;
+  const double d2 = ex * ex + ey * ey + ez * ez;
+  const double sd = d2 * pc.inv_a02d - 1.0;
+  double ts = pc.taud[NU - 1], t1 = 0.0;
+#pragma unroll
+  for (int m = NU - 2; m >= 0; --m) {
+    t1 = ts + sd * t1;
+    ts = pc.taud[m] + sd * ts;
+  }
+  const double rinv = 1.0 / sqrt(d2);
+  p += aj.w * (rinv - ts * pc.inv_a0d);
+  const double cf = aj.w * (-rinv * rinv * rinv - t1 * pc.two_inv_a03d);
+  fx += cf * ex;
+  fy += cf * ey;
+  fz += cf * ez;
+}
+
+template <typename T> struct QueueEntry;
+template <> struct alignas(16) QueueEntry<float> { int unit; float sx, sy, sz; };
+template <> struct alignas(16) QueueEntry<double> { int unit, pad; double sx, sy, sz, pad2; };
+
+// One 8 x 4 tile: lane (ii, jq) takes pair (i-atom ii, j-atom jq of the
+// unit). Close pairs (mixed form) are recorded for the FP64 pass while the
+// lane's record has room, else summed here in FP32.
+template <typename T, int NU, bool MIXED>
+__device__ __forceinline__ void tile(const PairConsts<T> &pc, const V4<T> &ai,
+                                     const V4<T> &aj, T sx, T sy, T sz, int jslot,
+                                     int islot, int code, int2 *closeq, int &nclose,
+                                     T &px, T &py, T &pz, T &pp) {
+  const T dx = aj.x + (sx - ai.x), dy = aj.y + (sy - ai.y), dz = aj.z + (sz - ai.z);
+  const T r2 = dx * dx + dy * dy + dz * dz;
+  // the atom itself (same slot, zero shift) is the only pair at r2 == 0
+  if (r2 < pc.a02 && (jslot != islot || r2 != T(0))) {
+    if constexpr (MIXED) {
+      if (r2 < pc.close2 && nclose < kCloseCap) {
+        closeq[nclose++] = make_int2(jslot, code);
+        return;
+      }
+    }
+    T pot, fs;
+    pair_terms<T, NU>(pc, r2, aj.w, pot, fs);
+    pp += pot;
+    px += fs * dx;
+    py += fs * dy;
+    pz += fs * dz;
+  }
+}
+
+template <typename T, int NU, bool MIXED>
+__global__ void __launch_bounds__(kWarps * 32)
+k_pair_clusters(PairClusterArgs<T> a, PairConsts<T> pc) {
+  __shared__ QueueEntry<T> queue[kWarps][32];
+  __shared__ int qcode[kWarps][32];
+  __shared__ int item_off[kWarps][32], item_u0[kWarps][32], item_code[kWarps][32];
+  __shared__ int2 closeq[MIXED ? kWarps : 1][MIXED ? 32 * kCloseCap : 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int u = blockIdx.x * kWarps + warp;
+  if (u >= a.maxcl || u >= a.clstart[a.ncol]) return;  // whole warp
+  const ClusterInfo ci = a.info[u];
+  const int ii = lane & 7, jq = lane >> 3;
+  const int islot = u * 8 + ii;
+  V4<T> ai = a.cpos[islot];
+  if (ii >= ci.n) ai.x = ai.y = ai.z = -(T)kFar;
+  const int cx = ci.col / a.nc1, cy = ci.col - cx * a.nc1;
+  const unsigned lt = (1u << lane) - 1u;
+  // cells along the column within K2 of the cluster's cells, split at the
+  // periodic boundary into segments k (image k of the column)
+  const int lo = ci.czf - a.K2, hi = ci.czl + a.K2;
+  const int klo = floor_div(lo, a.nc2);
+  const int nseg = floor_div(hi, a.nc2) - klo + 1;
+  const int nitems = a.ncoloff * nseg;
+  Acc<T> fx, fy, fz, ph;
+  fx.zero();
+  fy.zero();
+  fz.zero();
+  ph.zero();
+  int nclose = 0;
+  int2 *myclose = MIXED ? &closeq[MIXED ? warp : 0][lane * kCloseCap] : nullptr;
+  double cfx = 0., cfy = 0., cfz = 0., cph = 0.;
+
+  for (int i0 = 0; i0 < nitems; i0 += 32) {
+    // Phase A: one (column, segment) item per lane -> its run of units
+    int nun = 0, uu0 = 0, code = 0;
+    const int it = i0 + lane;
+    if (it < nitems) {
+      const int o = nseg == 1 ? it : it / nseg;
+      const int k = klo + (it - o * nseg);
+      const int2 d = *reinterpret_cast<const int2 *>(&a.coloff[o].du);
+      int x = cx + d.x, y = cy + d.y;
+      while (x < 0) x += a.nc0;
+      while (x >= a.nc0) x -= a.nc0;
+      while (y < 0) y += a.nc1;
+      while (y >= a.nc1) y -= a.nc1;
+      const int col = x * a.nc1 + y;
+      const int cb = col * a.nc2;
+      const int c0 = max(lo, k * a.nc2) - k * a.nc2;
+      const int c1 = min(hi, k * a.nc2 + a.nc2 - 1) - k * a.nc2;
+      const int A = a.start[cb + c0], B = a.start[cb + c1 + 1];
+      const int cs = a.start[cb], clb = a.clstart[col];
+      if (A < B) {
+        const int u0 = clb + ((A - cs) >> 3), u1 = clb + ((B - 1 - cs) >> 3);
+        nun = 2 * (u1 - u0 + 1);
+        uu0 = 2 * u0;
+      }
+      code = (o << 8) | (k + 128);
+    }
+    int incl = nun;
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, dd);
+      if (lane >= dd) incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    item_off[warp][lane] = incl - nun;
+    item_u0[warp][lane] = uu0;
+    item_code[warp][lane] = code;
+    __syncwarp();
+    // Phase B: the concatenated units, 32 at a time, box-tested per lane
+    for (int b0 = 0; b0 < total; b0 += 32) {
+      const int c = b0 + lane;
+      bool pass = false;
+      QueueEntry<T> ent;
+      int ecode = 0;
+      if (c < total) {
+        int j = 0;  // last item starting at or before c
+#pragma unroll
+        for (int step = 16; step; step >>= 1)
+          if (item_off[warp][j + step] <= c) j += step;
+        const int unit = item_u0[warp][j] + (c - item_off[warp][j]);
+        ecode = item_code[warp][j];
+        const int o = ecode >> 8, k = (ecode & 255) - 128;
+        const UnitBox ub = a.ubox[unit];
+        const int dzc = __float_as_int(ub.c.w) + k * a.nc2 - ci.czf;
+        const ColumnOffset &co = a.coloff[o];
+        const double sx = co.base[0] + dzc * a.cz[0];
+        const double sy = co.base[1] + dzc * a.cz[1];
+        const double sz = co.base[2] + dzc * a.cz[2];
+        pass = box_near(ci.c, ci.h, ub.c, ub.h, (float)sx, (float)sy, (float)sz, a.rbox2);
+        ent.unit = unit;
+        ent.sx = (T)sx;
+        ent.sy = (T)sy;
+        ent.sz = (T)sz;
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, pass);
+      if (pass) {
+        const int slot = __popc(m & lt);
+        queue[warp][slot] = ent;
+        qcode[warp][slot] = ecode;
+      }
+      __syncwarp();
+      const int nq = __popc(m);
+      T px = 0, py = 0, pz = 0, pp = 0;
+      int e = 0;
+      for (; e + 2 <= nq; e += 2) {
+        const QueueEntry<T> q0 = queue[warp][e], q1 = queue[warp][e + 1];
+        const int j0 = q0.unit * 4 + jq, j1 = q1.unit * 4 + jq;
+        const V4<T> a0 = a.cpos[j0], a1 = a.cpos[j1];
+        tile<T, NU, MIXED>(pc, ai, a0, q0.sx, q0.sy, q0.sz, j0, islot, qcode[warp][e],
+                           myclose, nclose, px, py, pz, pp);
+        tile<T, NU, MIXED>(pc, ai, a1, q1.sx, q1.sy, q1.sz, j1, islot,
+                           qcode[warp][e + 1], myclose, nclose, px, py, pz, pp);
+      }
+      if (e < nq) {
+        const QueueEntry<T> q0 = queue[warp][e];
+        const int j0 = q0.unit * 4 + jq;
+        tile<T, NU, MIXED>(pc, ai, a.cpos[j0], q0.sx, q0.sy, q0.sz, j0, islot,
+                           qcode[warp][e], myclose, nclose, px, py, pz, pp);
+      }
+      __syncwarp();
+      if (MIXED) {
+        fx.add(px);
+        fy.add(py);
+        fz.add(pz);
+        ph.add(pp);
+      } else {
+        fx.s += px;
+        fy.s += py;
+        fz.s += pz;
+        ph.s += pp;
+      }
+    }
+    __syncwarp();
+  }
+  if constexpr (MIXED) {
+    // close pairs in FP64
+    const V4<double> ai64 = a.cpos64[islot];
+    for (int t = 0; t < nclose; ++t) {
+      const int2 c = myclose[t];
+      const int jslot = c.x, o = c.y >> 8, k = (c.y & 255) - 128;
+      const ColumnOffset &co = a.coloff[o];
+      const int dzc = a.info[jslot >> 3].czf + k * a.nc2 - ci.czf;
+      close_pair64<NU>(pc, ai64, a.cpos64[jslot], co.base[0] + dzc * a.cz[0],
+                       co.base[1] + dzc * a.cz[1], co.base[2] + dzc * a.cz[2], cfx,
+                       cfy, cfz, cph);
+    }
+  }
+  // the four j lanes of each i atom, in a fixed order
+  T rx = fx.value(), ry = fy.value(), rz = fz.value(), rp = ph.value();
+#pragma unroll
+  for (int o = 8; o < 32; o <<= 1) {
+    rx += __shfl_xor_sync(0xffffffffu, rx, o);
+    ry += __shfl_xor_sync(0xffffffffu, ry, o);
+    rz += __shfl_xor_sync(0xffffffffu, rz, o);
+    rp += __shfl_xor_sync(0xffffffffu, rp, o);
+    if constexpr (MIXED) {
+      cfx += __shfl_xor_sync(0xffffffffu, cfx, o);
+      cfy += __shfl_xor_sync(0xffffffffu, cfy, o);
+      cfz += __shfl_xor_sync(0xffffffffu, cfz, o);
+      cph += __shfl_xor_sync(0xffffffffu, cph, o);
+    }
+  }
+  if (jq != 0 || ii >= ci.n) return;
+  V4<T> r;
+  if constexpr (MIXED) {
+    const double qi = a.cpos64[islot].w;
+    r.x = (T)(qi * ((double)rx + cfx));
+    r.y = (T)(qi * ((double)ry + cfy));
+    r.z = (T)(qi * ((double)rz + cfz));
+    r.w = (T)((double)rp + cph);
+  } else {
+    r.x = ai.w * rx;
+    r.y = ai.w * ry;
+    r.z = ai.w * rz;
+    r.w = rp;
+  }
+  a.out[ci.first + ii] = r;
+}
+
+template <typename T, int NU>
+void launch_nu(cudaStream_t s, const PairClusterArgs<T> &a, const PairConsts<T> &pc) {
+  constexpr bool kMixed = sizeof(T) == 4;
+  const int blocks = std::max(1, (a.maxcl + kWarps - 1) / kWarps);
+  k_pair_clusters<T, NU, kMixed><<<blocks, kWarps * 32, 0, s>>>(a, pc);
+}
+
+}  // namespace
+
+int cluster_capacity(int N, int ncol) { return N / 8 + ncol + 1; }
+
+void launch_column_clusters(cudaStream_t s, int ncol, int nc2, const int *start,
+                            int *count) {
+  k_column_clusters<<<(ncol + 255) / 256, 256, 0, s>>>(ncol, nc2, start, count);
+}
+
+template <typename T>
+void launch_cluster_fill(cudaStream_t s, int maxcl, int ncol, int nc2,
+                         const int *start, const int *clstart, const int *pcs,
+                         const V4<double> *src64, const double cz[3], V4<T> *cpos,
+                         V4<double> *cpos64, ClusterInfo *info, UnitBox *ubox) {
+  const long threads = 8L * maxcl;
+  const int blocks = (int)std::max<long>(1, (threads + 255) / 256);
+  k_cluster_fill<T><<<blocks, 256, 0, s>>>(maxcl, ncol, nc2, start, clstart, pcs, src64,
+                                           cz[0], cz[1], cz[2], cpos, cpos64, info, ubox);
+}
+
+template <typename T>
+void launch_pair_clusters(cudaStream_t s, const PairClusterArgs<T> &a,
+                          const PairConsts<T> &pc) {
+  switch (pc.nu) {
+    case 4: launch_nu<T, 4>(s, a, pc); break;
+    case 6: launch_nu<T, 6>(s, a, pc); break;
+    case 8: launch_nu<T, 8>(s, a, pc); break;
+    default: launch_nu<T, 10>(s, a, pc); break;
+  }
+}
+
+template void launch_cluster_fill<float>(cudaStream_t, int, int, int, const int *,
+                                         const int *, const int *, const V4<double> *,
+                                         const double *, V4<float> *, V4<double> *,
+                                         ClusterInfo *, UnitBox *);
+template void launch_cluster_fill<double>(cudaStream_t, int, int, int, const int *,
+                                          const int *, const int *, const V4<double> *,
+                                          const double *, V4<double> *, V4<double> *,
+                                          ClusterInfo *, UnitBox *);
+template void launch_pair_clusters<float>(cudaStream_t, const PairClusterArgs<float> &,
+                                          const PairConsts<float> &);
+template void launch_pair_clusters<double>(cudaStream_t, const PairClusterArgs<double> &,
+                                           const PairConsts<double> &);
+
+}  // namespace msm

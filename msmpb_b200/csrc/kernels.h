@@ -71,6 +71,10 @@ void launch_scatter(cudaStream_t s, int N, const int *cell, const int *start,
                     int *cursor, int *perm);
 void launch_segment_sort(cudaStream_t s, int ncell, const int *start,
                          int *perm);
+// orders each cell by key[atom].z, ties by atom index
+template <typename T>
+void launch_segment_sort_z(cudaStream_t s, int ncell, const int *start,
+                           int *perm, const V4<T> *key);
 template <typename T>
 void launch_gather(cudaStream_t s, int N, const int *perm, const V4<T> *src,
                    const int *cell, V4<T> *dst, int *cell_sorted, int *inv);
@@ -122,6 +126,55 @@ void launch_pair_cells(cudaStream_t s, int ncell, const V4<T> *pos_sorted,
                        const V4<double> *pos64_sorted, const int *cell_start,
                        const Geometry &g, const CellOffset<T> *offsets, int noff,
                        const PairConsts<T> &pc, V4<T> *out, int *err);
+
+// cluster form (k_pair_clusters.cu): clusters of 8 z-ordered atoms per
+// pair-cell column, one warp per i-cluster, 8 x 4 pair tiles
+constexpr int kMaxColumnOffsets = 1024;
+// A neighbour column (du, dv) and the Cartesian offset of its origin,
+// A (du/nc0, dv/nc1, 0), periodic image included.
+struct ColumnOffset {
+  int du, dv, pad[2];
+  double base[3];
+  double pad2;
+};
+struct ClusterInfo {
+  int first;     // sorted index of the first atom
+  int n;         // atoms (1..8)
+  int col;       // column cx * nc1 + cy
+  int czf, czl;  // cell z of the first and the last atom
+  int pad[3];
+  float4 c, h;   // bounding box centre and half extents (cluster frame)
+};
+struct UnitBox {  // half cluster; c.w holds the cluster's czf (int bits)
+  float4 c, h;
+};
+template <typename T>
+struct PairClusterArgs {
+  int maxcl, ncol, nc0, nc1, nc2, K2, ncoloff;
+  float rbox2;      // squared cutoff plus margin for the box test
+  double cz[3];     // A (0, 0, 1/nc2): one cell along the column
+  const int *start;     // pair-cell starts (ncell + 1)
+  const int *clstart;   // first cluster of each column (ncol + 1)
+  const ColumnOffset *coloff;
+  const ClusterInfo *info;
+  const UnitBox *ubox;
+  const V4<T> *cpos;          // maxcl x 8 (cluster frame, charge in w)
+  const V4<double> *cpos64;   // FP64 copy (mixed form) or null
+  V4<T> *out;                 // per sorted atom: force / q_i and potential
+  int *err;
+};
+int cluster_capacity(int N, int ncol);
+void launch_column_clusters(cudaStream_t s, int ncol, int nc2, const int *start,
+                            int *count);
+// src64: FP64 cell-relative positions and charges in sorted order
+template <typename T>
+void launch_cluster_fill(cudaStream_t s, int maxcl, int ncol, int nc2,
+                         const int *start, const int *clstart, const int *pcs,
+                         const V4<double> *src64, const double cz[3], V4<T> *cpos,
+                         V4<double> *cpos64, ClusterInfo *info, UnitBox *ubox);
+template <typename T>
+void launch_pair_clusters(cudaStream_t s, const PairClusterArgs<T> &a,
+                          const PairConsts<T> &pc);
 
 // ---- grid transfers (k_grid.cu) ----
 // variant 0: slab-staged gather; 1: one grid point per thread (reference form)

@@ -151,12 +151,14 @@ def test_level_weights(precision):
     assert rel_rms(phi, po) < tp
 
 
-@pytest.mark.parametrize("variant", [("MSMPB_PAIR", "cells"), ("MSMPB_ANTERP", "simple")])
+@pytest.mark.parametrize("variant", [("MSMPB_PAIR", "cells"), ("MSMPB_PAIR", "thread"),
+                                     ("MSMPB_ANTERP", "simple")])
 @pytest.mark.parametrize("case", ["spceN900_L3_M6_a8_nu8", "changaN512_L2_M8_a0.25_nu6",
                                   "CsClN16_auto"])
 def test_alternative_kernels(case, variant, monkeypatch):
     """The alternative kernels (cell-staged pair sum with compacted hits, one
-    thread per grid point for anterpolation) give the same results."""
+    thread per atom for the pair sum, one thread per grid point for
+    anterpolation) give the same results as the default ones."""
     monkeypatch.setenv(*variant)
     d = load(case)
     for precision in ("fp64", "mixed"):
@@ -196,3 +198,20 @@ def test_rebuild_box_change():
     eo, fo, _ = o.energy(pos2)
     assert abs(e - eo) / abs(eo) < 1e-10
     assert force_err(f, fo, d["q"], edges2) < 1e-10
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_triclinic_box_vs_oracle(precision):
+    """A skewed box: every neighbour column is swept (no gap pruning) and
+    the column images carry the off-diagonal edge components."""
+    q, pos, _ = systems.water(300, 24.0, 5)
+    edges = np.array([[24.0, 0.0, 0.0], [4.0, 24.0, 0.0], [3.0, -2.5, 24.0]])
+    o = Oracle(q, edges, cutoff=9.0, nu=6, levels=2, top_grid=6)
+    eo, fo, po = o.energy(pos)
+    ff = ForceField(q, pos, edges, cutoff=9.0, order=6, levels=2, top_grid=6,
+                    precision=precision)
+    e, f, phi = ff.energy(pos, potentials=True)
+    te, tf, tp = TOL[precision]
+    assert abs(e - eo) / abs(eo) < te
+    assert force_err(f, fo, q, edges) < tf
+    assert rel_rms(phi, po) < tp
