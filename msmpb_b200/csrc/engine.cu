@@ -132,10 +132,13 @@ class Plan : public FFDevice {
     if (v && v[0] == 't') return 1;
     return 2;
   }();
-  // MSMPB_ANTERP=simple selects the one-point-per-thread anterpolation
+  // Anterpolation: tile scatter (default); MSMPB_ANTERP=simple selects one
+  // grid point per thread, MSMPB_ANTERP=gather the slab-staged gather
   int anterp_variant_ = [] {
     const char *v = std::getenv("MSMPB_ANTERP");
-    return (v && v[0] == 's') ? 1 : 0;
+    if (v && v[0] == 's') return 1;
+    if (v && v[0] == 'g') return 2;
+    return 0;
   }();
 
   int device_ = 0;
@@ -174,6 +177,8 @@ class Plan : public FFDevice {
   static constexpr bool kMixed = sizeof(T) == 4;
   T *qg_[kMaxLevels + 2] = {}, *eg_[kMaxLevels + 2] = {};
   T *padded_ = nullptr, *part_ = nullptr, *kh_[kMaxLevels + 2] = {};
+  T *anterp_scratch_ = nullptr;
+  int *fold_tab_ = nullptr;
   double *khat_top_ = nullptr;
   double2 *fft_ = nullptr;
   double *qparts_ = nullptr, *short_parts_ = nullptr, *grid_parts_ = nullptr,
@@ -308,6 +313,12 @@ int Plan<T>::init(const Tables &t, int device) {
                           stencil_tap_pitch(sh_[l].S[2], !kMixed) * sizeof(T));
   }
   a.want(&padded_, pad_max * sizeof(T));
+  std::vector<int> fold_tab;
+  if (anterp_tiles_supported(grid_[1], nu_)) {
+    a.want(&anterp_scratch_, anterp_scratch_elems(grid_[1], nu_) * sizeof(T));
+    fold_tab = anterp_fold_table(grid_[1], nu_);
+    a.want(&fold_tab_, fold_tab.size() * sizeof(int));
+  }
   a.want(&part_, part_max * sizeof(T));
   size_t ntop = (size_t)grid_[L_][0] * grid_[L_][1] * grid_[L_][2];
   a.want(&khat_top_, ntop * sizeof(double));
@@ -328,6 +339,9 @@ int Plan<T>::init(const Tables &t, int device) {
   a.want(&err_d_, sizeof(int));
   if ((err = a.commit())) return err;
   MSM_CUDA_TRY(cudaMemset(err_d_, 0, sizeof(int)));
+  if (fold_tab_)
+    MSM_CUDA_TRY(cudaMemcpy(fold_tab_, fold_tab.data(), fold_tab.size() * sizeof(int),
+                            cudaMemcpyHostToDevice));
   if ((err = update(t))) return err;
   return tune_levels(pad_max, part_max);
 }
@@ -543,9 +557,9 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   }
   nl += 1;
   mark(s, kPhaseAnterp, tm);
-  launch_anterpolate<T>(s, grid_[1], gsorted_, gstart_, sc_, qg_[1],
-                        anterp_variant_, err_d_, N_);
-  nl += 1;
+  launch_anterpolate<T>(s, grid_[1], gsorted_, gcs_, gstart_, sc_, qg_[1],
+                        anterp_variant_, err_d_, N_, anterp_scratch_, fold_tab_);
+  nl += (anterp_variant_ == 0 && anterp_scratch_) ? 2 : 1;
   mark(s, kPhaseRestrict, tm);
   for (int l = 1; l < L_; ++l) {
     launch_restrict<T>(s, grid_[l], qg_[l], qg_[l + 1], J_, nu_);

@@ -221,6 +221,197 @@ k_anterpolate_slab(int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
   }
 }
 
+// Anterpolation as a tile scatter (the default).
+//
+// One warp per tile of kAT^3 grid cells. The tile's own atoms (cell-sorted,
+// so one contiguous run per (x, y) cell row; 64 runs concatenated by a warp
+// scan) are taken 32 at a time: each lane computes one atom's 3 nu B-spline
+// weights (q folded into the x weights). The atoms are then added one after
+// another into a shared accumulator covering every grid point the tile's
+// atoms reach, (kAT + nu - 1)^3 points. The nu^3 contributions of one atom
+// go to distinct points: lane l takes the (y, z) weight pairs l, l + 32, ...
+// and loops over the nu x weights (compile-time offsets), and the pairs left
+// over after the last full pass are spread one contribution per lane. One
+// warp and a fixed atom order make every sum deterministic without atomics.
+// The accumulator is written to the tile's scratch block; k_anterp_fold then
+// adds, for each grid point, the (at most 8) blocks that cover it in a fixed
+// order.
+constexpr int kAT = 8;
+
+template <int NU>
+struct TileGeom {
+  static constexpr int E = kAT + NU - 1;  // accumulator edge
+  static constexpr int E3 = E * E * E;
+  static constexpr int NP = NU * NU;      // (y, z) weight pairs
+  static constexpr int FP = NP / 32;      // passes with a pair on every lane
+  static constexpr int RC = (NP % 32) * NU;  // contributions of the other pairs
+  static constexpr int RR = (RC + 31) / 32;  // their rounds, one per lane
+  static constexpr int NW = 3 * NU + 2;   // weight row (even: vector loads)
+};
+
+template <typename T, int NU>
+__global__ void __launch_bounds__(32)
+k_anterp_tiles(int M0, int M1, int M2, int nt1, int nt2, const V4<T> *__restrict__ atoms,
+               const int *__restrict__ cell, const int *__restrict__ start,
+               SplineConsts<T> sc, T *__restrict__ scratch) {
+  using G = TileGeom<NU>;
+  constexpr int E = G::E, NW = G::NW;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *acc = reinterpret_cast<T *>(smem_raw);  // G::E3 values
+  __shared__ __align__(16) T w[32 * NW];
+  __shared__ int base[32];
+  __shared__ int rowbeg[64], rowoff[64];
+  const int lane = threadIdx.x;
+  const int tile = blockIdx.x;
+  const int tz = tile % nt2, ty = (tile / nt2) % nt1, tx = tile / (nt2 * nt1);
+  const int X0 = tx * kAT, Y0 = ty * kAT, Z0 = tz * kAT;
+  const int nx = min(kAT, M0 - X0), ny = min(kAT, M1 - Y0), nz = min(kAT, M2 - Z0);
+  for (int i = lane; i < G::E3; i += 32) acc[i] = T(0);
+  // this lane's pairs of the full passes, and its leftover contributions
+  int poff[G::FP > 0 ? G::FP : 1], pwb[G::FP > 0 ? G::FP : 1], pwc[G::FP > 0 ? G::FP : 1];
+#pragma unroll
+  for (int f = 0; f < G::FP; ++f) {
+    const int pr = f * 32 + lane, b = pr / NU, c = pr % NU;
+    poff[f] = b * E + c;
+    pwb[f] = NU + b;
+    pwc[f] = 2 * NU + c;
+  }
+  int roff[G::RR > 0 ? G::RR : 1], ra[G::RR > 0 ? G::RR : 1], rb[G::RR > 0 ? G::RR : 1],
+      rc[G::RR > 0 ? G::RR : 1];
+#pragma unroll
+  for (int r = 0; r < G::RR; ++r) {
+    const int ci = r * 32 + lane;
+    roff[r] = -1;
+    ra[r] = rb[r] = rc[r] = 0;
+    if (ci < G::RC) {
+      const int pr = G::FP * 32 + ci / NU, a = ci % NU, b = pr / NU, c = pr % NU;
+      roff[r] = a * E * E + b * E + c;
+      ra[r] = a;
+      rb[r] = NU + b;
+      rc[r] = 2 * NU + c;
+    }
+  }
+  // the 64 cell rows of the tile
+  int cnt[2], beg[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int rr = lane + 32 * h, x = rr / kAT, y = rr % kAT;
+    cnt[h] = 0;
+    beg[h] = 0;
+    if (x < nx && y < ny) {
+      const long c0 = ((long)(X0 + x) * M1 + (Y0 + y)) * M2 + Z0;
+      beg[h] = start[c0];
+      cnt[h] = start[c0 + nz] - beg[h];
+    }
+  }
+  int incl0 = cnt[0], incl1 = cnt[1];
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int y0 = __shfl_up_sync(0xffffffffu, incl0, d);
+    const int y1 = __shfl_up_sync(0xffffffffu, incl1, d);
+    if (lane >= d) {
+      incl0 += y0;
+      incl1 += y1;
+    }
+  }
+  const int tot0 = __shfl_sync(0xffffffffu, incl0, 31);
+  const int total = tot0 + __shfl_sync(0xffffffffu, incl1, 31);
+  rowbeg[lane] = beg[0];
+  rowbeg[lane + 32] = beg[1];
+  rowoff[lane] = incl0 - cnt[0];
+  rowoff[lane + 32] = tot0 + incl1 - cnt[1];
+  __syncwarp();
+
+  for (int k0 = 0; k0 < total; k0 += 32) {
+    const int k = k0 + lane;
+    const int n = min(32, total - k0);
+    if (k < total) {
+      int r = 0;  // last row starting at or before k
+#pragma unroll
+      for (int step = 32; step; step >>= 1)
+        if (r + step < 64 && rowoff[r + step] <= k) r += step;
+      const int g = rowbeg[r] + (k - rowoff[r]);
+      const V4<T> at = atoms[g];
+      const int x = r / kAT, y = r % kAT;
+      const long c0 = ((long)(X0 + x) * M1 + (Y0 + y)) * M2 + Z0;
+      const int z = (int)(cell[g] - c0);  // the row's cells are c0 .. c0 + nz - 1
+      base[lane] = (x + NU - 1) * E * E + (y + NU - 1) * E + (z + NU - 1);
+      T *wl = w + lane * NW;
+#pragma unroll
+      for (int i = 0; i < NU; ++i) {
+        wl[i] = at.w * bspline<T, NU>(sc, i, at.x);
+        wl[NU + i] = bspline<T, NU>(sc, i, at.y);
+        wl[2 * NU + i] = bspline<T, NU>(sc, i, at.z);
+      }
+    }
+    __syncwarp();
+    for (int j = 0; j < n; ++j) {
+      const int bj = base[j];
+      const T *wj = w + j * NW;
+      T wa[NU];
+#pragma unroll
+      for (int a = 0; a < NU; a += 2) {
+        if constexpr (sizeof(T) == 4) {
+          const float2 v = *reinterpret_cast<const float2 *>(wj + a);
+          wa[a] = v.x;
+          wa[a + 1] = v.y;
+        } else {
+          const double2 v = *reinterpret_cast<const double2 *>(wj + a);
+          wa[a] = v.x;
+          wa[a + 1] = v.y;
+        }
+      }
+#pragma unroll
+      for (int f = 0; f < G::FP; ++f) {
+        const T wyz = wj[pwb[f]] * wj[pwc[f]];
+        T *ap = acc + (bj - poff[f]);
+#pragma unroll
+        for (int a = 0; a < NU; ++a) ap[-a * E * E] = fma(wyz, wa[a], ap[-a * E * E]);
+      }
+#pragma unroll
+      for (int r = 0; r < G::RR; ++r) {
+        if (roff[r] >= 0) {
+          T *ap = acc + (bj - roff[r]);
+          *ap = fma(wj[rb[r]] * wj[rc[r]], wj[ra[r]], *ap);
+        }
+      }
+      __syncwarp();
+    }
+  }
+  __syncwarp();
+  T *out = scratch + (long)tile * G::E3;
+  for (int i = lane; i < G::E3; i += 32) out[i] = acc[i];
+}
+
+// grid[p] = sum over the tiles covering p of their block value at p, in a
+// fixed order. tab (host-built, anterp_fold_table): per axis and point, the
+// count (<= 4) and the (tile, local index) covers packed as tile << 8 | local.
+template <typename T, int NU>
+__global__ void __launch_bounds__(kThreads)
+k_anterp_fold(int M0, int M1, int M2, int nt1, int nt2, const int *__restrict__ tab,
+              const T *__restrict__ scratch, T *__restrict__ grid) {
+  using G = TileGeom<NU>;
+  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long)M0 * M1 * M2) return;
+  const int p2 = idx % M2, p1 = (idx / M2) % M1, p0 = idx / ((long)M1 * M2);
+  const int *t0 = tab + 5 * p0, *t1 = tab + 5 * (M0 + p1), *t2 = tab + 5 * (M0 + M1 + p2);
+  const int n0 = t0[0], n1 = t1[0], n2 = t2[0];
+  T s = T(0);
+  for (int a = 0; a < n0; ++a) {
+    const int e0 = t0[1 + a];
+    for (int b = 0; b < n1; ++b) {
+      const int e1 = t1[1 + b];
+      const long tl = (long)(e0 >> 8) * nt1 + (e1 >> 8);
+      const int l01 = ((e0 & 255) * G::E + (e1 & 255)) * G::E;
+      for (int c = 0; c < n2; ++c) {
+        const int e2 = t2[1 + c];
+        s += scratch[(tl * nt2 + (e2 >> 8)) * G::E3 + l01 + (e2 & 255)];
+      }
+    }
+  }
+  grid[idx] = s;
+}
+
 // Field and potential at each atom (code/forcefield1.c:570-607), separable:
 // z sums first, then y, then x. Output E in Cartesian components
 // (E = A^-T (M * grad_u)) and phi_long.
@@ -423,10 +614,57 @@ AnterpTile anterp_tile(const int M[3], int nu, long natoms) {
 
 }  // namespace
 
+size_t anterp_scratch_elems(const int M[3], int nu) {
+  const size_t nt = (size_t)((M[0] + kAT - 1) / kAT) * ((M[1] + kAT - 1) / kAT) *
+                    ((M[2] + kAT - 1) / kAT);
+  const size_t e = kAT + nu - 1;
+  return nt * e * e * e;
+}
+
+bool anterp_tiles_supported(const int M[3], int nu) {
+  return M[0] >= nu && M[1] >= nu && M[2] >= nu;
+}
+
+// Tile j of an axis covers the points j kAT - nu/2 + 1 + l (mod M), l in
+// [0, n_j + nu - 1), n_j = min(kAT, M - j kAT). With M >= nu a point has at
+// most 4 covers per axis.
+std::vector<int> anterp_fold_table(const int M[3], int nu) {
+  std::vector<int> tab(5 * (size_t)(M[0] + M[1] + M[2]), 0);
+  size_t o = 0;
+  for (int ax = 0; ax < 3; ++ax) {
+    const int nt = (M[ax] + kAT - 1) / kAT;
+    for (int p = 0; p < M[ax]; ++p, o += 5) {
+      int n = 0;
+      for (int j = 0; j < nt; ++j) {
+        const int nj = std::min(kAT, M[ax] - j * kAT);
+        const int lo = j * kAT - nu / 2 + 1;
+        for (int l = ((p - lo) % M[ax] + M[ax]) % M[ax]; l < nj + nu - 1; l += M[ax])
+          if (n < 4) tab[o + 1 + n++] = (j << 8) | l;
+      }
+      tab[o] = n;
+    }
+  }
+  return tab;
+}
+
 template <typename T>
 void launch_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
-                        const int *cell_start, const SplineConsts<T> &sc,
-                        T *grid, int variant, int *err, long natoms) {
+                        const int *cell_sorted, const int *cell_start,
+                        const SplineConsts<T> &sc, T *grid, int variant, int *err,
+                        long natoms, T *scratch, const int *fold_tab) {
+  if (variant == 0 && scratch && fold_tab && anterp_tiles_supported(M, sc.nu)) {
+    const int nt0 = (M[0] + kAT - 1) / kAT, nt1 = (M[1] + kAT - 1) / kAT,
+              nt2 = (M[2] + kAT - 1) / kAT;
+    const int ntiles = nt0 * nt1 * nt2;
+    const long n = (long)M[0] * M[1] * M[2];
+    MSM_NU_SWITCH(sc.nu, (k_anterp_tiles<T, NU><<<ntiles, 32,
+                                                  TileGeom<NU>::E3 * sizeof(T), s>>>(
+                             M[0], M[1], M[2], nt1, nt2, atoms, cell_sorted, cell_start,
+                             sc, scratch)));
+    MSM_NU_SWITCH(sc.nu, (k_anterp_fold<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
+                             M[0], M[1], M[2], nt1, nt2, fold_tab, scratch, grid)));
+    return;
+  }
   if (variant == 1) {  // one grid point per thread, runtime loops
     long n = (long)M[0] * M[1] * M[2];
     MSM_NU_SWITCH(sc.nu, (k_anterpolate<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
@@ -448,6 +686,9 @@ void anterpolate_prepare() {
   MSM_NU_SWITCH_ALL(cudaFuncSetAttribute(k_anterpolate_slab<T, NU, kAnterpBX>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          kAnterpSmemBudget));
+  MSM_NU_SWITCH_ALL(cudaFuncSetAttribute(k_anterp_tiles<T, NU>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(TileGeom<NU>::E3 * sizeof(T))));
   done = true;
 }
 
@@ -492,9 +733,9 @@ void launch_grid_dot(cudaStream_t s, size_t n, const T *a, const T *b,
 
 #define MSM_INST_GRID(T)                                                       \
   template void launch_anterpolate<T>(cudaStream_t, const int *,              \
-                                      const V4<T> *, const int *,             \
+                                      const V4<T> *, const int *, const int *,\
                                       const SplineConsts<T> &, T *, int,      \
-                                      int *, long);                           \
+                                      int *, long, T *, const int *);         \
   template void anterpolate_prepare<T>();                                     \
   template void launch_interpolate<T>(cudaStream_t, int, const int *,         \
                                       const V4<T> *, const int *, const T *,  \

@@ -177,11 +177,18 @@ void launch_pair_clusters(cudaStream_t s, const PairClusterArgs<T> &a,
                           const PairConsts<T> &pc);
 
 // ---- grid transfers (k_grid.cu) ----
-// variant 0: slab-staged gather; 1: one grid point per thread (reference form)
+// variant 0: tile scatter with a fold (scratch: anterp_scratch_elems
+// values; grids smaller than nu along an axis use the slab gather);
+// 1: one grid point per thread (reference form); 2: slab-staged gather
+size_t anterp_scratch_elems(const int M[3], int nu);
+bool anterp_tiles_supported(const int M[3], int nu);
+// per-axis cover table of the fold (5 ints per grid index and axis)
+std::vector<int> anterp_fold_table(const int M[3], int nu);
 template <typename T>
 void launch_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
-                        const int *cell_start, const SplineConsts<T> &sc,
-                        T *grid, int variant, int *err, long natoms);
+                        const int *cell_sorted, const int *cell_start,
+                        const SplineConsts<T> &sc, T *grid, int variant, int *err,
+                        long natoms, T *scratch, const int *fold_tab);
 template <typename T>
 void anterpolate_prepare();
 template <typename T>
