@@ -132,6 +132,12 @@ class Plan : public FFDevice {
     if (v && v[0] == 't') return 1;
     return 2;
   }();
+  // Level stencils of symmetric kernels use the folded sweep unless
+  // MSMPB_STENCIL=full
+  bool fold_enabled_ = [] {
+    const char *v = std::getenv("MSMPB_STENCIL");
+    return !(v && v[0] == 'f');
+  }();
   // Anterpolation: tile scatter (default); MSMPB_ANTERP=simple selects one
   // grid point per thread, MSMPB_ANTERP=gather the slab-staged gather
   int anterp_variant_ = [] {
@@ -177,6 +183,10 @@ class Plan : public FFDevice {
   static constexpr bool kMixed = sizeof(T) == 4;
   T *qg_[kMaxLevels + 2] = {}, *eg_[kMaxLevels + 2] = {};
   T *padded_ = nullptr, *part_ = nullptr, *kh_[kMaxLevels + 2] = {};
+  T *khf_[kMaxLevels + 2] = {};  // folded taps (symmetric stencils)
+  // level stencil taps for the sweep variant in use
+  const T *level_taps(int l) const { return sh_[l].sym ? khf_[l] : kh_[l]; }
+  void plan_level(int l);
   T *anterp_scratch_ = nullptr;
   int *fold_tab_ = nullptr;
   double *khat_top_ = nullptr;
@@ -247,7 +257,8 @@ int Plan<T>::init(const Tables &t, int device) {
   anterpolate_prepare<T>();
   int err = set_tables(t);
   if (err) return err;
-  // stencil shapes
+  // stencil shapes; scratch for both sweep variants (a rebuild with a new
+  // box can make a stencil lose or gain its mirror symmetry)
   size_t pad_max = 1, part_max = 1;
   for (int l = 1; l < L_; ++l) {
     StencilShape &s = sh_[l];
@@ -256,18 +267,18 @@ int Plan<T>::init(const Tables &t, int device) {
       s.S[k] = t.sten[l][k];
     }
     const bool fp64 = sizeof(T) == 8;
-    tile_[l] = stencil_default_tile(s, fp64);
-    if (!stencil_templated(s) || stencil_prepare<T>(s, tile_[l]) < 0) {
-      tile_[l] = StencilTile();  // reference-form sweep
-      s.P[0] = s.M[0] + s.S[0] - 1;
-      s.P[1] = s.M[1] + s.S[1] - 1;
-      s.P[2] = s.M[2] + s.S[2] - 1;
-    } else {
-      stencil_padded_dims(s, tile_[l], fp64, s.P);
+    std::vector<double> kf;
+    for (int v = 0; v < 2; ++v) {
+      s.sym = v;
+      if (v && (s.S[0] % 2 == 0 || s.S[1] % 2 == 0)) continue;
+      plan_level(l);
+      pad_max = std::max(pad_max, (size_t)s.P[0] * s.P[1] * s.P[2]);
+      if (tile_[l].nsplit > 1)
+        part_max = std::max(part_max, (size_t)tile_[l].nsplit * s.M[0] * s.M[1] * s.M[2]);
     }
-    pad_max = std::max(pad_max, (size_t)s.P[0] * s.P[1] * s.P[2]);
-    if (tile_[l].nsplit > 1)
-      part_max = std::max(part_max, (size_t)tile_[l].nsplit * s.M[0] * s.M[1] * s.M[2]);
+    s.sym = fold_enabled_ && stencil_templated(s) &&
+            stencil_fold_taps(t.khat[l].data(), s.S, fp64, kf);
+    plan_level(l);
     // levels worth tuning: size the scratch for every candidate tile
     const double gflop = 2e-9 * s.M[0] * s.M[1] * s.M[2] * (double)s.S[0] * s.S[1] * s.S[2];
     tune_[l] = tile_[l].nz > 0 && gflop >= 1.0 && stencil_tuning_enabled();
@@ -308,9 +319,12 @@ int Plan<T>::init(const Tables &t, int device) {
     size_t g = (size_t)grid_[l][0] * grid_[l][1] * grid_[l][2];
     a.want(&qg_[l], g * sizeof(T));
     a.want(&eg_[l], g * sizeof(T));
-    if (l < L_)
+    if (l < L_) {
       a.want(&kh_[l], (size_t)sh_[l].S[0] * sh_[l].S[1] *
                           stencil_tap_pitch(sh_[l].S[2], !kMixed) * sizeof(T));
+      a.want(&khf_[l], (size_t)(sh_[l].S[0] / 2 + 1) * (sh_[l].S[1] / 2 + 1) *
+                           stencil_tap_pitch(sh_[l].S[2], !kMixed) * sizeof(T));
+    }
   }
   a.want(&padded_, pad_max * sizeof(T));
   std::vector<int> fold_tab;
@@ -355,7 +369,7 @@ int Plan<T>::tune_levels(size_t pad_cap, size_t part_cap) {
     if (!tune_[l]) continue;
     double ms = 0;
     StencilTile best = stencil_autotune<T>(
-        stream_, device_, sh_[l], tile_[l], padded_, pad_cap, kh_[l],
+        stream_, device_, sh_[l], tile_[l], padded_, pad_cap, level_taps(l),
         stencil_tap_pitch(sh_[l].S[2], khz_fp64), eg_[l], part_, part_cap, &ms);
     if (stencil_prepare<T>(sh_[l], best) < 0) continue;
     tile_[l] = best;
@@ -364,6 +378,24 @@ int Plan<T>::tune_levels(size_t pad_cap, size_t part_cap) {
   MSM_CUDA_TRY(cudaStreamSynchronize(stream_));
   cudaGetLastError();
   return MSMPB_OK;
+}
+
+// Default tile, shared-memory attribute and padded dims of level l for the
+// sweep variant sh_[l].sym
+template <typename T>
+void Plan<T>::plan_level(int l) {
+  StencilShape &s = sh_[l];
+  const bool fp64 = sizeof(T) == 8;
+  tile_[l] = stencil_default_tile(s, fp64);
+  if (!stencil_templated(s) || stencil_prepare<T>(s, tile_[l]) < 0) {
+    tile_[l] = StencilTile();  // reference-form sweep
+    s.sym = 0;
+    s.P[0] = s.M[0] + s.S[0] - 1;
+    s.P[1] = s.M[1] + s.S[1] - 1;
+    s.P[2] = s.M[2] + s.S[2] - 1;
+  } else {
+    stencil_padded_dims(s, tile_[l], fp64, s.P);
+  }
 }
 
 // Constants that depend only on the parameter set (not on the box)
@@ -479,6 +511,20 @@ int Plan<T>::update(const Tables &t) {
           kh[((size_t)i * S1 + j) * sp + k] = (T)t.khat[l][((size_t)i * S1 + j) * S2 + k];
     MSM_CUDA_TRY(cudaMemcpy(kh_[l], kh.data(), kh.size() * sizeof(T),
                             cudaMemcpyHostToDevice));
+    // folded taps when the stencil is mirror-symmetric in x and y
+    std::vector<double> kf;
+    const int sym = fold_enabled_ && stencil_templated(sh_[l]) &&
+                    stencil_fold_taps(t.khat[l].data(), sh_[l].S, !kMixed, kf);
+    if (sym != sh_[l].sym) {
+      sh_[l].sym = sym;
+      plan_level(l);
+    }
+    if (sh_[l].sym) {
+      std::vector<T> kft(kf.size());
+      for (size_t n = 0; n < kf.size(); ++n) kft[n] = (T)kf[n];
+      MSM_CUDA_TRY(cudaMemcpy(khf_[l], kft.data(), kft.size() * sizeof(T),
+                              cudaMemcpyHostToDevice));
+    }
   }
   MSM_CUDA_TRY(cudaMemcpy(khat_top_, t.khat[L_].data(),
                           t.khat[L_].size() * sizeof(double),
@@ -580,7 +626,7 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
     mark(s, kPhaseStencil, tm && l == L_ - 1);
     launch_pad<T>(s, sh_[l], qg_[l], padded_);
     if (tm) cudaEventRecord(lev_ev_[l][0], s);
-    launch_stencil<T>(s, sh_[l], tile_[l], padded_, kh_[l],
+    launch_stencil<T>(s, sh_[l], tile_[l], padded_, level_taps(l),
                       stencil_tap_pitch(sh_[l].S[2], !kMixed), (T)w[l], eg_[l],
                       part_);
     if (tm) cudaEventRecord(lev_ev_[l][1], s);

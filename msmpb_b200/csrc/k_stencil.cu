@@ -19,6 +19,7 @@
 //    broadcast). The z extent S2 is a template parameter so the R x S2
 //    FMA block is fully unrolled with register-resident operands.
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 
 #include "kernels.h"
@@ -31,6 +32,17 @@ constexpr int kMaxTemplatedS = 33;
 
 inline int blocks_for(long n) {
   return (int)std::max<long>(1, (n + kThreads - 1) / kThreads);
+}
+
+// Row pitch of a shared slice: the nz R + S - 1 values a row needs, in whole
+// 16-byte units, and an odd number of them. Lanes of one row read 16-byte
+// units R values apart; an odd pitch puts the next row's lanes on the
+// banks in between, so 16-byte row reads by up to 4 lanes per row are free
+// of bank conflicts.
+__host__ __device__ inline int slice_pitch(int nz, int R, int S, int V) {
+  int units = (nz * R + S - 1 + V - 1) / V;
+  if (units % 2 == 0) ++units;
+  return units * V;
 }
 
 template <typename T>
@@ -142,7 +154,7 @@ k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
   const int i_lo = kc * chunk, i_hi = min(S0, i_lo + chunk);
   const int z0 = blockIdx.x * NZ * R, y0 = blockIdx.y * TY, x0 = xt * TX;
   const int H = TY + S1 - 1;
-  const int W = (NZ * R + S - 1 + V - 1) / V * V;
+  const int W = slice_pitch(NZ, R, S, V);
   const int slice_elems = H * W + V;  // +V: tail reads of the last row
   const int tap_elems = S1 * SP;
   T *buf0 = smem, *buf1 = smem + slice_elems;
@@ -241,6 +253,163 @@ k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
   }
 }
 
+// Folded sweep for stencils that are mirror-symmetric in x and y (every
+// orthorhombic box; S0, S1 odd, centres c0 = S0/2, c1 = S1/2):
+//   e[x,y,z] = sum_{i<=c0, j<=c1, k} kf[i][j][k] * F_ij[y][z+k],
+//   F_i = P[x+c0+i] + P[x+c0-i] (i > 0; P[x+c0] for i = 0),
+//   F_ij[y] = F_i[y+j] + F_i[y+S1-1-j] (j < c1; F_i[y+c1] for j = c1),
+// with kf[i][j] the tap shared by the (up to) four mirror images. That is
+// (c0+1)(c1+1)S2 multiply-adds per output instead of S0 S1 S2, plus the
+// plane and row sums. A CTA owns one output plane x and a TY x (NZ R) tile
+// of it; for each i the two input planes stream into a double-buffered pair
+// of shared slices (cp.async), are summed in shared memory, and every thread
+// forms its folded rows in registers. Split over i: chunk k takes
+// i in [k chunk, min(c0+1, (k+1) chunk)), partial sums as in k_stencil_tiled.
+// kf: (c0+1) x (c1+1) rows of SP taps (zero padded).
+template <typename T, int S, int R>
+__global__ void __launch_bounds__(kThreads)
+k_stencil_fold(StencilShape sh, const T *__restrict__ P, const T *__restrict__ kf,
+               T w, T *__restrict__ e, int chunk, T *__restrict__ part) {
+  constexpr int V = 16 / sizeof(T);
+  constexpr int SP = (S + V - 1) / V * V;
+  constexpr int RL = R + S - 1;
+  constexpr int RLV = (RL + V - 1) / V * V;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *smem = reinterpret_cast<T *>(smem_raw);
+  const int NZ = blockDim.x, TY = blockDim.y;
+  const int tz = threadIdx.x, ty = threadIdx.y;
+  const int nth = NZ * TY, tid = ty * NZ + tz;
+  const int S1 = sh.S[1], c0 = sh.S[0] / 2, c1 = S1 / 2;
+  const int x = blockIdx.z % sh.M[0], kc = blockIdx.z / sh.M[0];
+  const int i_lo = kc * chunk, i_hi = min(c0 + 1, i_lo + chunk);
+  const int z0 = blockIdx.x * NZ * R, y0 = blockIdx.y * TY;
+  const int H = TY + S1 - 1;
+  const int W = slice_pitch(NZ, R, S, V);
+  const int slice = H * W + V;
+  const int tap_elems = (c1 + 1) * SP;
+  // stage s: slices A = smem + 2 s slice, B = A + slice, taps after all four
+
+  T acc[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) acc[r] = T(0);
+  auto stage = [&](int i, int s) {
+    T *a = smem + 2 * s * slice;
+    stage_plane(P, sh, x + c0 + i, y0, z0, H, W, a);
+    if (i > 0) stage_plane(P, sh, x + c0 - i, y0, z0, H, W, a + slice);
+    stage_taps(kf + (long)i * tap_elems, 0, tap_elems, smem + 4 * slice + s * tap_elems);
+  };
+  if (i_lo < i_hi) {
+    stage(i_lo, 0);
+    cp_async_commit();
+  }
+  for (int i = i_lo; i < i_hi; ++i) {
+    const int s = (i - i_lo) & 1;
+    if (i + 1 < i_hi) {
+      stage(i + 1, s ^ 1);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    T *As = smem + 2 * s * slice;
+    const T *Ks = smem + 4 * slice + s * tap_elems;
+    if (i > 0) {  // F_i = A + B, in place
+      for (int t = tid; t < H * W / V; t += nth) {
+        if constexpr (sizeof(T) == 4) {
+          float4 a = reinterpret_cast<float4 *>(As)[t];
+          const float4 b = reinterpret_cast<const float4 *>(As + slice)[t];
+          a.x += b.x;
+          a.y += b.y;
+          a.z += b.z;
+          a.w += b.w;
+          reinterpret_cast<float4 *>(As)[t] = a;
+        } else {
+          double2 a = reinterpret_cast<double2 *>(As)[t];
+          const double2 b = reinterpret_cast<const double2 *>(As + slice)[t];
+          a.x += b.x;
+          a.y += b.y;
+          reinterpret_cast<double2 *>(As)[t] = a;
+        }
+      }
+      __syncthreads();
+    }
+    const T *F = As;
+    for (int j = 0; j <= c1; ++j) {
+      const T *r1 = F + (ty + j) * W + tz * R;
+      const T *r2 = F + (ty + S1 - 1 - j) * W + tz * R;
+      T row[RLV];
+#pragma unroll
+      for (int v = 0; v < RLV; v += V) {
+        if constexpr (sizeof(T) == 4) {
+          const float4 a = *reinterpret_cast<const float4 *>(r1 + v);
+          row[v] = a.x;
+          row[v + 1] = a.y;
+          row[v + 2] = a.z;
+          row[v + 3] = a.w;
+        } else {
+          const double2 a = *reinterpret_cast<const double2 *>(r1 + v);
+          row[v] = a.x;
+          row[v + 1] = a.y;
+        }
+      }
+      if (j < c1) {
+#pragma unroll
+        for (int v = 0; v < RLV; v += V) {
+          if constexpr (sizeof(T) == 4) {
+            const float4 b = *reinterpret_cast<const float4 *>(r2 + v);
+            row[v] += b.x;
+            row[v + 1] += b.y;
+            row[v + 2] += b.z;
+            row[v + 3] += b.w;
+          } else {
+            const double2 b = *reinterpret_cast<const double2 *>(r2 + v);
+            row[v] += b.x;
+            row[v + 1] += b.y;
+          }
+        }
+      }
+      const T *kp = Ks + j * SP;
+#pragma unroll
+      for (int kk = 0; kk < SP; kk += V) {
+        T t[V];
+        if constexpr (sizeof(T) == 4) {
+          const float4 t4 = *reinterpret_cast<const float4 *>(kp + kk);
+          t[0] = t4.x;
+          t[1] = t4.y;
+          t[2] = t4.z;
+          t[3] = t4.w;
+        } else {
+          const double2 t2 = *reinterpret_cast<const double2 *>(kp + kk);
+          t[0] = t2.x;
+          t[1] = t2.y;
+        }
+#pragma unroll
+        for (int u = 0; u < V; ++u) {
+          if (kk + u < S) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) acc[r] = fma(t[u], row[r + kk + u], acc[r]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  const int y = y0 + ty;
+  if (y >= sh.M[1]) return;
+  const long mtot = (long)sh.M[0] * sh.M[1] * sh.M[2];
+  const long row0 = ((long)x * sh.M[1] + y) * sh.M[2];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int z = z0 + tz * R + r;
+    if (z >= sh.M[2]) continue;
+    if (part)
+      part[kc * mtot + row0 + z] = acc[r];
+    else
+      e[row0 + z] += w * acc[r];
+  }
+}
+
 // e += w * sum_k part[k], chunks added in index order
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
@@ -257,13 +426,24 @@ template <typename T> struct TileDefaults;
 template <> struct TileDefaults<float> { static constexpr int R = 8, TX = 4; };
 template <> struct TileDefaults<double> { static constexpr int R = 4, TX = 4; };
 
+// shared memory of the folded sweep: two stages of two slices and a tap block
+template <typename T>
+size_t fold_smem_bytes(const StencilShape &sh, const StencilTile &tl) {
+  constexpr int R = TileDefaults<T>::R;
+  constexpr int V = 16 / sizeof(T);
+  const int H = tl.ty + sh.S[1] - 1;
+  const int W = slice_pitch(tl.nz, R, sh.S[2], V);
+  const int SP = stencil_tap_pitch(sh.S[2], sizeof(T) == 8);
+  return (4 * (size_t)(H * W + V) + 2 * (size_t)(sh.S[1] / 2 + 1) * SP) * sizeof(T);
+}
+
 template <typename T, int S>
 void launch_tiled(cudaStream_t s, const StencilShape &sh, const StencilTile &tl,
                   const T *p, const T *kh, int khz, T w, T *e, T *part) {
   constexpr int R = TileDefaults<T>::R, TX = TileDefaults<T>::TX;
   constexpr int V = 16 / sizeof(T);
   const int H = tl.ty + sh.S[1] - 1;
-  const int W = (tl.nz * R + S - 1 + V - 1) / V * V;
+  const int W = slice_pitch(tl.nz, R, S, V);
   const size_t smem = (2 * (size_t)(H * W + V) +
                        (size_t)(TX + 1) * sh.S[1] * stencil_tap_pitch(S, sizeof(T) == 8)) *
                       sizeof(T);
@@ -282,19 +462,39 @@ void launch_tiled(cudaStream_t s, const StencilShape &sh, const StencilTile &tl,
   }
 }
 
+template <typename T, int S>
+void launch_fold(cudaStream_t s, const StencilShape &sh, const StencilTile &tl,
+                 const T *p, const T *kf, T w, T *e, T *part) {
+  constexpr int R = TileDefaults<T>::R;
+  const int nI = sh.S[0] / 2 + 1;
+  const int nsplit = std::max(1, tl.nsplit);
+  const int chunk = (nI + nsplit - 1) / nsplit;
+  dim3 block(tl.nz, tl.ty);
+  dim3 grid((sh.M[2] + tl.nz * R - 1) / (tl.nz * R), (sh.M[1] + tl.ty - 1) / tl.ty,
+            sh.M[0] * nsplit);
+  k_stencil_fold<T, S, R><<<grid, block, fold_smem_bytes<T>(sh, tl), s>>>(
+      sh, p, kf, w, e, chunk, nsplit > 1 ? part : nullptr);
+  if (nsplit > 1) {
+    const long n = (long)sh.M[0] * sh.M[1] * sh.M[2];
+    k_split_reduce<T><<<blocks_for(n), kThreads, 0, s>>>(n, nsplit, part, w, e);
+  }
+}
+
 // Levels (and plans) that share an instantiation need the largest request:
 // the attribute is per kernel function, so it is only ever raised.
 template <typename T, int S>
-void set_smem_attr(int bytes) {
+void set_smem_attr(int bytes, bool fold) {
   constexpr int R = TileDefaults<T>::R, TX = TileDefaults<T>::TX;
   static std::mutex mu;
-  static int current = 48 * 1024;
+  static int current[2] = {48 * 1024, 48 * 1024};
   std::lock_guard<std::mutex> lock(mu);
-  if (bytes <= current) return;
-  if (cudaFuncSetAttribute(k_stencil_tiled<T, S, R, TX>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           bytes) == cudaSuccess)
-    current = bytes;
+  if (bytes <= current[fold]) return;
+  const cudaError_t err =
+      fold ? cudaFuncSetAttribute(k_stencil_fold<T, S, R>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)
+           : cudaFuncSetAttribute(k_stencil_tiled<T, S, R, TX>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (err == cudaSuccess) current[fold] = bytes;
 }
 
 #define MSM_S_CASES(X) \
@@ -306,7 +506,7 @@ void set_smem_attr(int bytes) {
 
 StencilTile stencil_default_tile(const StencilShape &sh, bool fp64) {
   const int R = fp64 ? TileDefaults<double>::R : TileDefaults<float>::R;
-  const int TX = fp64 ? TileDefaults<double>::TX : TileDefaults<float>::TX;
+  const int TX = sh.sym ? 1 : (fp64 ? TileDefaults<double>::TX : TileDefaults<float>::TX);
   StencilTile t;
   t.tx = TX;
   // Tile shape: least padding waste, then least shared-memory traffic per
@@ -332,9 +532,10 @@ StencilTile stencil_default_tile(const StencilShape &sh, bool fp64) {
   // CTAs per SM); every chunk keeps at least one plane.
   const long tiles = (long)((sh.M[2] + t.nz * R - 1) / (t.nz * R)) *
                      ((sh.M[1] + t.ty - 1) / t.ty) * ((sh.M[0] + TX - 1) / TX);
-  int ns = (int)std::min<long>(sh.S[0], std::max<long>(1, (148L * 4 + tiles - 1) / tiles));
-  const int chunk = (sh.S[0] + ns - 1) / ns;
-  t.nsplit = (sh.S[0] + chunk - 1) / chunk;
+  const int nI = sh.sym ? sh.S[0] / 2 + 1 : sh.S[0];  // tap planes to split
+  int ns = (int)std::min<long>(nI, std::max<long>(1, (148L * 4 + tiles - 1) / tiles));
+  const int chunk = (nI + ns - 1) / ns;
+  t.nsplit = (nI + chunk - 1) / chunk;
   return t;
 }
 
@@ -357,7 +558,8 @@ void stencil_padded_dims(const StencilShape &sh, const StencilTile &tl,
   const int mx = (sh.M[0] + tl.tx - 1) / tl.tx * tl.tx;
   P[0] = mx + sh.S[0] - 1;
   P[1] = my + sh.S[1] - 1;
-  P[2] = ((mz + sh.S[2] - 1 + V - 1) / V) * V + V;
+  // rows of the last z tile reach z0 + W (+V: 16-byte tail reads)
+  P[2] = ((mz + sh.S[2] - 1 + V - 1) / V) * V + 2 * V;
 }
 
 template <typename T>
@@ -366,18 +568,48 @@ int stencil_prepare(const StencilShape &sh, const StencilTile &tl) {
   constexpr int R = TileDefaults<T>::R;
   constexpr int V = 16 / sizeof(T);
   const int H = tl.ty + sh.S[1] - 1;
-  const int W = (tl.nz * R + sh.S[2] - 1 + V - 1) / V * V;
-  const int bytes = (2 * (H * W + V) +
-                     (tl.tx + 1) * sh.S[1] * stencil_tap_pitch(sh.S[2], sizeof(T) == 8)) *
-                    (int)sizeof(T);
+  const int W = slice_pitch(tl.nz, R, sh.S[2], V);
+  const int bytes =
+      sh.sym ? (int)fold_smem_bytes<T>(sh, tl)
+             : (2 * (H * W + V) +
+                (tl.tx + 1) * sh.S[1] * stencil_tap_pitch(sh.S[2], sizeof(T) == 8)) *
+                   (int)sizeof(T);
   if (bytes > 200 * 1024) return -1;
   switch (sh.S[2]) {
 #define X(SS) \
-  case SS: set_smem_attr<T, SS>(bytes); break;
+  case SS: set_smem_attr<T, SS>(bytes, sh.sym != 0); break;
     MSM_S_CASES(X)
 #undef X
   }
   return 0;
+}
+
+bool stencil_fold_taps(const double *kh, const int S[3], bool fp64,
+                       std::vector<double> &kf) {
+  kf.clear();
+  if (S[0] % 2 == 0 || S[1] % 2 == 0) return false;
+  const int S0 = S[0], S1 = S[1], S2 = S[2], c0 = S0 / 2, c1 = S1 / 2;
+  auto at = [&](int i, int j, int k) { return kh[((size_t)i * S1 + j) * S2 + k]; };
+  double amax = 0;
+  for (size_t n = 0; n < (size_t)S0 * S1 * S2; ++n) amax = std::max(amax, std::fabs(kh[n]));
+  const double tol = 1e-12 * amax;
+  for (int i = 0; i < S0; ++i)
+    for (int j = 0; j < S1; ++j)
+      for (int k = 0; k < S2; ++k)
+        if (std::fabs(at(i, j, k) - at(S0 - 1 - i, j, k)) > tol ||
+            std::fabs(at(i, j, k) - at(i, S1 - 1 - j, k)) > tol)
+          return false;
+  const int SP = stencil_tap_pitch(S2, fp64);
+  kf.assign((size_t)(c0 + 1) * (c1 + 1) * SP, 0.0);
+  for (int i = 0; i <= c0; ++i)
+    for (int j = 0; j <= c1; ++j)
+      for (int k = 0; k < S2; ++k) {
+        const double v = at(c0 + i, c1 + j, k) + at(c0 - i, c1 + j, k) +
+                         at(c0 + i, c1 - j, k) + at(c0 - i, c1 - j, k);
+        // row j of the folded block pairs rows j and S1-1-j: tap index c1 - j'
+        kf[((size_t)i * (c1 + 1) + (c1 - j)) * SP + k] = 0.25 * v;
+      }
+  return true;
 }
 
 template <typename T>
@@ -395,8 +627,13 @@ void launch_stencil(cudaStream_t s, const StencilShape &sh, const StencilTile &t
     return;
   }
   switch (sh.S[2]) {
-#define X(SS) \
-  case SS: launch_tiled<T, SS>(s, sh, tl, p, kh, khz, w, e, part); break;
+#define X(SS)                                                      \
+  case SS:                                                         \
+    if (sh.sym)                                                    \
+      launch_fold<T, SS>(s, sh, tl, p, kh, w, e, part);            \
+    else                                                           \
+      launch_tiled<T, SS>(s, sh, tl, p, kh, khz, w, e, part);      \
+    break;
     MSM_S_CASES(X)
 #undef X
   }

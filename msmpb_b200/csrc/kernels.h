@@ -212,6 +212,8 @@ struct StencilShape {
   int M[3];   // grid dims
   int S[3];   // stencil dims
   int P[3];   // padded input dims (P[2] rounded up for 16-byte rows)
+  int sym;    // 1: taps mirror-symmetric in x and y, S0 and S1 odd (folded
+              // sweep, taps given as the folded (S0/2+1) x (S1/2+1) rows)
 };
 // CTA tile of the stencil sweep: nz x ty threads, each with tx x R outputs
 struct StencilTile {
@@ -222,6 +224,13 @@ StencilTile stencil_default_tile(const StencilShape &sh, bool fp64);
 bool stencil_templated(const StencilShape &sh);
 // row pitch of the tap array: S2 rounded up to 16 bytes (rows zero padded)
 int stencil_tap_pitch(int S2, bool fp64);
+// folded taps for a symmetric stencil: kf[i][j][k], i <= S0/2, j <= S1/2,
+// the mean of the (up to four) mirror images kh[S0/2 +- i][S1/2 +- j][k],
+// rows padded to the tap pitch. Returns false (and leaves kf empty) when
+// kh is not mirror-symmetric in x and y to 1e-12 of its largest tap or
+// S0, S1 are even.
+bool stencil_fold_taps(const double *kh, const int S[3], bool fp64,
+                       std::vector<double> &kf);
 // padded input dims that keep every tile load of `tile` inside the buffer
 void stencil_padded_dims(const StencilShape &sh, const StencilTile &tile,
                          bool fp64, int P[3]);

@@ -5,7 +5,7 @@
 // own buffers and keeps the fastest; smaller levels use the model-based
 // default (stencil_default_tile). Results are cached in a text file, one
 // line per (device, precision, grid, stencil):
-//   <device name>|<fp32|fp64>|M0,M1,M2|S0,S1,S2 nz ty nsplit ms
+//   <device name>|<fp32|fp64>|M0,M1,M2|S0,S1,S2|<folded|full> nz ty nsplit ms
 // at $MSMPB_TUNE_CACHE, else $HOME/.cache/msmpb_b200/stencil_tiles.txt.
 // MSMPB_TUNE=0 disables tuning (default tiles only).
 #include <sys/stat.h>
@@ -41,9 +41,9 @@ std::string cache_key(const StencilShape &sh, bool fp64, int device) {
   cudaDeviceProp prop{};
   cudaGetDeviceProperties(&prop, device);
   char buf[512];
-  std::snprintf(buf, sizeof buf, "%s|%s|%d,%d,%d|%d,%d,%d", prop.name,
+  std::snprintf(buf, sizeof buf, "%s|%s|%d,%d,%d|%d,%d,%d|%s", prop.name,
                 fp64 ? "fp64" : "fp32", sh.M[0], sh.M[1], sh.M[2], sh.S[0],
-                sh.S[1], sh.S[2]);
+                sh.S[1], sh.S[2], sh.sym ? "folded" : "full");
   for (char *c = buf; *c; ++c)
     if (*c == ' ') *c = '_';
   return buf;
@@ -102,8 +102,9 @@ std::vector<StencilTile> stencil_candidates(const StencilShape &sh, bool fp64) {
         t.ty = ty;
         if (nz * ty > 256 || nz * ty < 32 || ty > sh.M[1]) continue;
         if (nz * R > sh.M[2] + R - 1 && nz > 1) continue;
-        const int chunk = (sh.S[0] + std::max(1, ns) - 1) / std::max(1, ns);
-        t.nsplit = (sh.S[0] + chunk - 1) / chunk;
+        const int nI = sh.sym ? sh.S[0] / 2 + 1 : sh.S[0];
+        const int chunk = (nI + std::max(1, ns) - 1) / std::max(1, ns);
+        t.nsplit = (nI + chunk - 1) / chunk;
         bool dup = false;
         for (auto &u : out)
           dup |= (u.nz == t.nz && u.ty == t.ty && u.nsplit == t.nsplit);

@@ -152,14 +152,15 @@ def test_level_weights(precision):
 
 
 @pytest.mark.parametrize("variant", [("MSMPB_PAIR", "cells"), ("MSMPB_PAIR", "thread"),
-                                     ("MSMPB_ANTERP", "simple"), ("MSMPB_ANTERP", "gather")])
+                                     ("MSMPB_ANTERP", "simple"), ("MSMPB_ANTERP", "gather"),
+                                     ("MSMPB_STENCIL", "full")])
 @pytest.mark.parametrize("case", ["spceN900_L3_M6_a8_nu8", "changaN512_L2_M8_a0.25_nu6",
                                   "CsClN16_auto"])
 def test_alternative_kernels(case, variant, monkeypatch):
     """The alternative kernels (cell-staged pair sum with compacted hits, one
     thread per atom for the pair sum; one thread per grid point, or the
-    slab-staged gather, for anterpolation) give the same results as the
-    default ones."""
+    slab-staged gather, for anterpolation; the unfolded level stencil) give
+    the same results as the default ones."""
     monkeypatch.setenv(*variant)
     d = load(case)
     for precision in ("fp64", "mixed"):
