@@ -714,11 +714,15 @@ int Plan<T>::evaluate(const EvalRequest &r, double *energy) {
     if (r.phi)
       MSM_CUDA_TRY(cudaMemcpyAsync(r.phi, phi_s_, (size_t)N_ * sizeof(double),
                                    cudaMemcpyDeviceToHost, s));
-    double e = 0;
+    double e = 0, qs[2] = {0, 0};
     MSM_CUDA_TRY(cudaMemcpyAsync(&e, energy_, sizeof(double),
                                  cudaMemcpyDeviceToHost, s));
+    if (r.q2)
+      MSM_CUDA_TRY(cudaMemcpyAsync(qs, qstats_, 2 * sizeof(double),
+                                   cudaMemcpyDeviceToHost, s));
     int st = sync();
     if (energy) *energy = e;
+    if (r.q2) *r.q2 = qs[1];
     return st;
   }
   return MSMPB_OK;

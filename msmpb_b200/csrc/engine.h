@@ -41,6 +41,8 @@ struct EvalRequest {
   double *energy_dev;    // device scalar or nullptr (device mode)
   cudaStream_t stream;   // device mode: caller stream (0 = own stream)
   bool timing;           // record per-phase events
+  double *q2;            // host mode, may be null: receives sum q_i^2 (FP64,
+                         // reduced on the device)
 };
 
 // Runs one evaluation. Host mode synchronises and returns the energy in

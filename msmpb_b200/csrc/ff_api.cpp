@@ -276,14 +276,17 @@ double FF_energy_potentials(FF *ff, double (*force)[3], double (*position)[3],
   r.force = force ? &force[0][0] : nullptr;
   r.phi = potential;
   r.timing = ff->timing != 0;
-  double e = NAN;
+  double e = NAN, q2 = 0;
+  r.q2 = &q2;
   int st = msm::engine_evaluate(ff->dev, r, &e);
   if (st != MSMPB_OK) {
     set_error(ff, st);
     return NAN;
   }
   if (r.timing) fill_times(ff);
-  ff->errEst = msm::err_model(h->params, ff->q, ff->orderAcc) /
+  // the reference refreshes the estimate after every evaluation
+  // (code/forcefield1.c:233); sum q^2 comes from the device reduction
+  ff->errEst = msm::err_model_q2(h->params, q2, ff->orderAcc) /
                std::pow(ff->cutoff, ff->orderAcc);
   return e;
 }

@@ -47,6 +47,8 @@ bool select_params(Params &p, int N, const double *q, const double edges[3][3],
 
 // Error model (code/forcefield0.c:521-587)
 double err_model(const Params &p, const double *q, int nu);
+// the same from a precomputed sum of q_i^2
+double err_model_q2(const Params &p, double Q2, int nu);
 double delta_f(const Params &p, const double *q);
 
 // Quasi-interpolation weights omega'_l and c_L only (code/forcefield0.c:726-767);

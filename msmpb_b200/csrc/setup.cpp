@@ -76,11 +76,15 @@ double invert3(const double a[3][3], double ai[3][3]) {
 }
 
 double err_model(const Params &p, const double *q, int nu) {
+  double Q2 = 0;
+  for (int i = 0; i < p.N; ++i) Q2 += q[i] * q[i];
+  return err_model_q2(p, Q2, nu);
+}
+
+double err_model_q2(const Params &p, double Q2, int nu) {
   int M1[3] = {p.top[0], p.top[1], p.top[2]};
   for (int l = 1; l < p.L; ++l)
     for (int &m : M1) m *= 2;
-  double Q2 = 0;
-  for (int i = 0; i < p.N; ++i) Q2 += q[i] * q[i];
   double Fref = (Q2 / (double)p.N) / std::pow(p.detA / (double)p.N, 5. / 6.);
   double h1 = std::max({norm_row(p.A, 0) / M1[0], norm_row(p.A, 1) / M1[1],
                         norm_row(p.A, 2) / M1[2]});

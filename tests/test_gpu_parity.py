@@ -217,3 +217,14 @@ def test_triclinic_box_vs_oracle(precision):
     assert abs(e - eo) / abs(eo) < te
     assert force_err(f, fo, q, edges) < tf
     assert rel_rms(phi, po) < tp
+
+
+def test_error_estimate_after_evaluation():
+    """FF_energy refreshes errEst (code/forcefield1.c:233); the library takes
+    sum q^2 from its device reduction, so it agrees with the host formula to
+    rounding."""
+    q, pos, edges, kw = _oracle_case("water300")
+    o = Oracle(q, edges, cutoff=kw.get("cutoff", -1), nu=kw.get("order", -1))
+    ff = ForceField(q, pos, edges, **kw, precision="mixed")
+    ff.energy(pos)
+    assert ff.err_est() == pytest.approx(o.err_est(), rel=1e-12)
