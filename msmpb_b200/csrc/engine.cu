@@ -564,14 +564,17 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   if (kMixed) launch_permute64(s, N_, pperm_, prel64_, psorted64_);
   launch_gather<T>(s, N_, gperm_, gfrac_, gcell_, gsorted_, gcs_, ginv_);
   nl += 3 + 6 + 2 + 2 + 2;
-  mark(s, kPhasePair, tm);
-  if (pair_variant_ == 2 && clusters_ok_) {
+  const bool clusters = pair_variant_ == 2 && clusters_ok_;
+  if (clusters) {  // cluster build (part of the binning phase)
     const V4<double> *src64 =
         kMixed ? psorted64_ : reinterpret_cast<const V4<double> *>(psorted_);
     launch_column_clusters(s, ncol_, geom_.nc[2], pstart_, clcount_);
     launch_scan(s, clcount_, clstart_, ncol_, scan_tmp_);
     launch_cluster_fill<T>(s, maxcl_, ncol_, geom_.nc[2], pstart_, clstart_, pcs_,
                            src64, cz_, cpos_, cpos64_, cinfo_, cubox_);
+  }
+  mark(s, kPhasePair, tm);
+  if (clusters) {
     PairClusterArgs<T> ca{};
     ca.maxcl = maxcl_;
     ca.ncol = ncol_;

@@ -94,8 +94,8 @@ std::vector<StencilTile> stencil_candidates(const StencilShape &sh, bool fp64) {
   const StencilTile d = stencil_default_tile(sh, fp64);
   out.push_back(d);
   const int R = fp64 ? 4 : 8;
-  for (int nz : {d.nz, 4, 6, 8, 9, 12})
-    for (int ty : {4, 8, 12, 16})
+  for (int nz : {d.nz, 2, 3, 4, 6, 8, 9, 12})
+    for (int ty : {4, 8, 12, 16, 24, 32})
       for (int ns : {1, 2, d.nsplit, 2 * d.nsplit}) {
         StencilTile t = d;
         t.nz = nz;
