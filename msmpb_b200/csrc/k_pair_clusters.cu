@@ -185,25 +185,23 @@ __device__ __forceinline__ void close_pair64(const PairConsts<float> &pc,
   fz += cf * ez;
 }
 
-template <typename T> struct QueueEntry;
-template <> struct alignas(16) QueueEntry<float> { int unit; float sx, sy, sz; };
-template <> struct alignas(16) QueueEntry<double> { int unit, pad; double sx, sy, sz, pad2; };
-
 // One 8 x 4 tile: lane (ii, jq) takes pair (i-atom ii, j-atom jq of the
-// unit). Close pairs (mixed form) are recorded for the FP64 pass while the
-// lane's record has room, else summed here in FP32.
+// queued unit, already shifted into the i-cluster's frame). Close pairs
+// (mixed form) are recorded for the FP64 pass while the lane's record has
+// room, else summed here in FP32.
 template <typename T, int NU, bool MIXED>
 __device__ __forceinline__ void tile(const PairConsts<T> &pc, const V4<T> &ai,
-                                     const V4<T> &aj, T sx, T sy, T sz, int jslot,
-                                     int islot, int code, int2 *closeq, int &nclose,
-                                     T &px, T &py, T &pz, T &pp) {
-  const T dx = aj.x + (sx - ai.x), dy = aj.y + (sy - ai.y), dz = aj.z + (sz - ai.z);
+                                     const V4<T> &aj, const int *qunit, int e, int jq,
+                                     int islot, const int *qcode, int2 *closeq,
+                                     int &nclose, T &px, T &py, T &pz, T &pp) {
+  const T dx = aj.x - ai.x, dy = aj.y - ai.y, dz = aj.z - ai.z;
   const T r2 = dx * dx + dy * dy + dz * dz;
-  // the atom itself (same slot, zero shift) is the only pair at r2 == 0
-  if (r2 < pc.a02 && (jslot != islot || r2 != T(0))) {
+  if (r2 < pc.a02) {
+    // the atom itself (same slot, zero shift) is the only pair at r2 == 0
+    if (r2 == T(0) && qunit[e] * 4 + jq == islot) return;
     if constexpr (MIXED) {
       if (r2 < pc.close2 && nclose < kCloseCap) {
-        closeq[nclose++] = make_int2(jslot, code);
+        closeq[nclose++] = make_int2(qunit[e] * 4 + jq, qcode[e]);
         return;
       }
     }
@@ -219,8 +217,10 @@ __device__ __forceinline__ void tile(const PairConsts<T> &pc, const V4<T> &ai,
 template <typename T, int NU, bool MIXED>
 __global__ void __launch_bounds__(kWarps * 32)
 k_pair_clusters(PairClusterArgs<T> a, PairConsts<T> pc) {
-  __shared__ QueueEntry<T> queue[kWarps][32];
-  __shared__ int qcode[kWarps][32];
+  // passing units of the current batch: their 4 atoms shifted into the
+  // i-cluster's frame, the unit index and the (column, image) code
+  __shared__ V4<T> qatoms[kWarps][32][4];
+  __shared__ int qunit[kWarps][32], qcode[kWarps][32];
   __shared__ int item_off[kWarps][32], item_u0[kWarps][32], item_code[kWarps][32];
   __shared__ int2 closeq[MIXED ? kWarps : 1][MIXED ? 32 * kCloseCap : 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -289,8 +289,8 @@ k_pair_clusters(PairClusterArgs<T> a, PairConsts<T> pc) {
     for (int b0 = 0; b0 < total; b0 += 32) {
       const int c = b0 + lane;
       bool pass = false;
-      QueueEntry<T> ent;
-      int ecode = 0;
+      int ecode = 0, eunit = 0;
+      T esx = 0, esy = 0, esz = 0;
       if (c < total) {
         int j = 0;  // last item starting at or before c
 #pragma unroll
@@ -306,36 +306,40 @@ k_pair_clusters(PairClusterArgs<T> a, PairConsts<T> pc) {
         const double sy = co.base[1] + dzc * a.cz[1];
         const double sz = co.base[2] + dzc * a.cz[2];
         pass = box_near(ci.c, ci.h, ub.c, ub.h, (float)sx, (float)sy, (float)sz, a.rbox2);
-        ent.unit = unit;
-        ent.sx = (T)sx;
-        ent.sy = (T)sy;
-        ent.sz = (T)sz;
+        eunit = unit;
+        esx = (T)sx;
+        esy = (T)sy;
+        esz = (T)sz;
       }
       const unsigned m = __ballot_sync(0xffffffffu, pass);
       if (pass) {
         const int slot = __popc(m & lt);
-        queue[warp][slot] = ent;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          V4<T> v = a.cpos[eunit * 4 + q];
+          v.x += esx;
+          v.y += esy;
+          v.z += esz;
+          qatoms[warp][slot][q] = v;
+        }
+        qunit[warp][slot] = eunit;
         qcode[warp][slot] = ecode;
       }
       __syncwarp();
       const int nq = __popc(m);
       T px = 0, py = 0, pz = 0, pp = 0;
+      const int *qu = qunit[warp], *qc = qcode[warp];
       int e = 0;
       for (; e + 2 <= nq; e += 2) {
-        const QueueEntry<T> q0 = queue[warp][e], q1 = queue[warp][e + 1];
-        const int j0 = q0.unit * 4 + jq, j1 = q1.unit * 4 + jq;
-        const V4<T> a0 = a.cpos[j0], a1 = a.cpos[j1];
-        tile<T, NU, MIXED>(pc, ai, a0, q0.sx, q0.sy, q0.sz, j0, islot, qcode[warp][e],
-                           myclose, nclose, px, py, pz, pp);
-        tile<T, NU, MIXED>(pc, ai, a1, q1.sx, q1.sy, q1.sz, j1, islot,
-                           qcode[warp][e + 1], myclose, nclose, px, py, pz, pp);
+        const V4<T> a0 = qatoms[warp][e][jq], a1 = qatoms[warp][e + 1][jq];
+        tile<T, NU, MIXED>(pc, ai, a0, qu, e, jq, islot, qc, myclose, nclose, px, py, pz,
+                           pp);
+        tile<T, NU, MIXED>(pc, ai, a1, qu, e + 1, jq, islot, qc, myclose, nclose, px, py,
+                           pz, pp);
       }
-      if (e < nq) {
-        const QueueEntry<T> q0 = queue[warp][e];
-        const int j0 = q0.unit * 4 + jq;
-        tile<T, NU, MIXED>(pc, ai, a.cpos[j0], q0.sx, q0.sy, q0.sz, j0, islot,
-                           qcode[warp][e], myclose, nclose, px, py, pz, pp);
-      }
+      if (e < nq)
+        tile<T, NU, MIXED>(pc, ai, qatoms[warp][e][jq], qu, e, jq, islot, qc, myclose,
+                           nclose, px, py, pz, pp);
       __syncwarp();
       if (MIXED) {
         fx.add(px);
