@@ -261,9 +261,9 @@ k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
 // with kf[i][j] the tap shared by the (up to) four mirror images. That is
 // (c0+1)(c1+1)S2 multiply-adds per output instead of S0 S1 S2, plus the
 // plane and row sums. A CTA owns one output plane x and a TY x (NZ R) tile
-// of it; for each i the two input planes stream into a double-buffered pair
-// of shared slices (cp.async), are summed in shared memory, and every thread
-// forms its folded rows in registers. Split over i: chunk k takes
+// of it; for each i the two input planes stream into shared slices
+// (cp.async; the next pair's copies overlap this pair's sweep), are summed in
+// shared memory, and every thread forms its folded rows in registers. Split over i: chunk k takes
 // i in [k chunk, min(c0+1, (k+1) chunk)), partial sums as in k_stencil_tiled.
 // kf: (c0+1) x (c1+1) rows of SP taps (zero padded).
 template <typename T, int S, int R>
@@ -287,16 +287,18 @@ k_stencil_fold(StencilShape sh, const T *__restrict__ P, const T *__restrict__ k
   const int W = slice_pitch(NZ, R, S, V);
   const int slice = H * W + V;
   const int tap_elems = (c1 + 1) * SP;
-  // stage s: slices A = smem + 2 s slice, B = A + slice, taps after all four
+  // shared layout: A slices of stages 0 and 1, one B slice, tap blocks of
+  // stages 0 and 1. Step i: wait for its planes, add B into A (B is then
+  // free), start the copies of step i+1, and sweep while they land.
+  T *Bsl = smem + 2 * slice;
 
   T acc[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) acc[r] = T(0);
   auto stage = [&](int i, int s) {
-    T *a = smem + 2 * s * slice;
-    stage_plane(P, sh, x + c0 + i, y0, z0, H, W, a);
-    if (i > 0) stage_plane(P, sh, x + c0 - i, y0, z0, H, W, a + slice);
-    stage_taps(kf + (long)i * tap_elems, 0, tap_elems, smem + 4 * slice + s * tap_elems);
+    stage_plane(P, sh, x + c0 + i, y0, z0, H, W, smem + s * slice);
+    if (i > 0) stage_plane(P, sh, x + c0 - i, y0, z0, H, W, Bsl);
+    stage_taps(kf + (long)i * tap_elems, 0, tap_elems, smem + 3 * slice + s * tap_elems);
   };
   if (i_lo < i_hi) {
     stage(i_lo, 0);
@@ -304,21 +306,15 @@ k_stencil_fold(StencilShape sh, const T *__restrict__ P, const T *__restrict__ k
   }
   for (int i = i_lo; i < i_hi; ++i) {
     const int s = (i - i_lo) & 1;
-    if (i + 1 < i_hi) {
-      stage(i + 1, s ^ 1);
-      cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
+    cp_async_wait<0>();
     __syncthreads();
-    T *As = smem + 2 * s * slice;
-    const T *Ks = smem + 4 * slice + s * tap_elems;
+    T *As = smem + s * slice;
+    const T *Ks = smem + 3 * slice + s * tap_elems;
     if (i > 0) {  // F_i = A + B, in place
       for (int t = tid; t < H * W / V; t += nth) {
         if constexpr (sizeof(T) == 4) {
           float4 a = reinterpret_cast<float4 *>(As)[t];
-          const float4 b = reinterpret_cast<const float4 *>(As + slice)[t];
+          const float4 b = reinterpret_cast<const float4 *>(Bsl)[t];
           a.x += b.x;
           a.y += b.y;
           a.z += b.z;
@@ -326,13 +322,17 @@ k_stencil_fold(StencilShape sh, const T *__restrict__ P, const T *__restrict__ k
           reinterpret_cast<float4 *>(As)[t] = a;
         } else {
           double2 a = reinterpret_cast<double2 *>(As)[t];
-          const double2 b = reinterpret_cast<const double2 *>(As + slice)[t];
+          const double2 b = reinterpret_cast<const double2 *>(Bsl)[t];
           a.x += b.x;
           a.y += b.y;
           reinterpret_cast<double2 *>(As)[t] = a;
         }
       }
-      __syncthreads();
+    }
+    __syncthreads();  // B consumed; the other stage's buffers are free
+    if (i + 1 < i_hi) {
+      stage(i + 1, s ^ 1);
+      cp_async_commit();
     }
     const T *F = As;
     for (int j = 0; j <= c1; ++j) {
@@ -393,7 +393,6 @@ k_stencil_fold(StencilShape sh, const T *__restrict__ P, const T *__restrict__ k
         }
       }
     }
-    __syncthreads();
   }
   const int y = y0 + ty;
   if (y >= sh.M[1]) return;
@@ -426,7 +425,7 @@ template <typename T> struct TileDefaults;
 template <> struct TileDefaults<float> { static constexpr int R = 8, TX = 4; };
 template <> struct TileDefaults<double> { static constexpr int R = 4, TX = 4; };
 
-// shared memory of the folded sweep: two stages of two slices and a tap block
+// shared memory of the folded sweep: two A slices, one B slice, two tap blocks
 template <typename T>
 size_t fold_smem_bytes(const StencilShape &sh, const StencilTile &tl) {
   constexpr int R = TileDefaults<T>::R;
@@ -434,7 +433,7 @@ size_t fold_smem_bytes(const StencilShape &sh, const StencilTile &tl) {
   const int H = tl.ty + sh.S[1] - 1;
   const int W = slice_pitch(tl.nz, R, sh.S[2], V);
   const int SP = stencil_tap_pitch(sh.S[2], sizeof(T) == 8);
-  return (4 * (size_t)(H * W + V) + 2 * (size_t)(sh.S[1] / 2 + 1) * SP) * sizeof(T);
+  return (3 * (size_t)(H * W + V) + 2 * (size_t)(sh.S[1] / 2 + 1) * SP) * sizeof(T);
 }
 
 template <typename T, int S>
