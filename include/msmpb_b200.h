@@ -63,6 +63,17 @@ int FF_energy_device(FF *ff, const double *position_d, const double *charge_d,
 /* Waits for the library's stream and reports device-side check failures. */
 int FF_sync(FF *ff);
 
+/* FF_rebuild (code/forcefield0.c:598-680: new box, every build-time choice
+ * kept) with the level stencils computed on the GPU, ordered on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream) with no host
+ * synchronisation: for box changes every step (constant-pressure MD). The
+ * box-dependent constants and the top-level multiplier are recomputed on
+ * the host (microseconds). The host copies of the level stencils
+ * (ff->khat[1..maxLevel-1]) keep the previous box's values; FF_rebuild
+ * refreshes them. Pair lists are rebuilt at every evaluation, so no
+ * positions are needed. Returns MSMPB_OK or an error code. */
+int FF_rebuild_device(FF *ff, double edges[3][3], void *stream);
+
 /* Milliseconds of each phase of the last evaluation, measured with CUDA
  * events on the evaluation stream (also copied into the reference's time_*
  * fields in seconds). Order: bin, pair, anterpolation, restriction,

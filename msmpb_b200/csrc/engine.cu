@@ -26,6 +26,9 @@
 struct FFDevice {
   virtual ~FFDevice() {}
   virtual int update(const msm::Tables &t) = 0;
+  // new box with the level stencils computed on the device, in the order of
+  // `stream` (no host synchronisation); t holds everything else
+  virtual int update_device(const msm::Tables &t, cudaStream_t stream) = 0;
   virtual int evaluate(const msm::EvalRequest &r, double *energy) = 0;
   virtual int sync() = 0;
   virtual int phase_times(double *ms, int n) = 0;
@@ -85,6 +88,7 @@ class Plan : public FFDevice {
   int init(const Tables &t, int device);
   ~Plan() override;
   int update(const Tables &t) override;
+  int update_device(const Tables &t, cudaStream_t stream) override;
   int evaluate(const EvalRequest &r, double *energy) override;
   int sync() override;
   int phase_times(double *ms, int n) override;
@@ -105,6 +109,7 @@ class Plan : public FFDevice {
 
  private:
   int set_tables(const Tables &t);
+  int update_box(const Tables &t, cudaStream_t s, bool stencils_on_device);
   int tune_levels(size_t pad_cap, size_t part_cap);
   int launch_graph(const EvalRequest &r, cudaStream_t s, const double *pos,
                    const double *q, double *force, double *phi, double *edev);
@@ -206,6 +211,15 @@ class Plan : public FFDevice {
   cudaGraphExec_t exec_ = nullptr;
   GraphKey key_{};
   bool have_graph_ = false;
+  bool graph_stale_ = false;  // kernel parameters changed (new box)
+  // recorded after a device-side rebuild; every later evaluation's stream
+  // waits for it (the rebuild may run on another stream)
+  cudaEvent_t rebuild_ev_ = nullptr;
+  bool rebuild_recorded_ = false;
+  // omega' rows (x, y, z of each level, stride oms_) and work space of the
+  // device stencil computation
+  double *om_d_ = nullptr, *stwork_ = nullptr;
+  int oms_ = 1;
   cudaEvent_t ev_[kNumPhases + 1] = {};
   cudaEvent_t lev_ev_[kMaxLevels + 2][2] = {};
   bool timed_ = false;
@@ -216,6 +230,7 @@ template <typename T>
 Plan<T>::~Plan() {
   if (stream_) cudaStreamSynchronize(stream_);
   if (exec_) cudaGraphExecDestroy(exec_);
+  if (rebuild_ev_) cudaEventDestroy(rebuild_ev_);
   for (auto &e : ev_)
     if (e) cudaEventDestroy(e);
   for (auto &pr : lev_ev_)
@@ -344,6 +359,14 @@ int Plan<T>::init(const Tables &t, int device) {
   a.want(&energy_, sizeof(double));
   a.want(&off_d_, kMaxNeighbourOffsets * sizeof(CellOffset<T>));
   a.want(&coloff_d_, kMaxColumnOffsets * sizeof(ColumnOffset));
+  oms_ = 1;
+  size_t stn = 1;
+  for (int l = 1; l < L_; ++l) {
+    stn = std::max(stn, (size_t)sh_[l].S[0] * sh_[l].S[1] * sh_[l].S[2]);
+    for (int k = 0; k < 3; ++k) oms_ = std::max(oms_, (int)t.omegap[l][k].size());
+  }
+  a.want(&om_d_, (size_t)(L_ + 1) * 3 * oms_ * sizeof(double));
+  a.want(&stwork_, 3 * stn * sizeof(double));
   a.want(&clcount_, (ncol_ + 1) * sizeof(int));
   a.want(&clstart_, (ncol_ + 1) * sizeof(int));
   a.want(&cpos_, (size_t)maxcl_ * 8 * sizeof(V4<T>));
@@ -356,6 +379,15 @@ int Plan<T>::init(const Tables &t, int device) {
   if (fold_tab_)
     MSM_CUDA_TRY(cudaMemcpy(fold_tab_, fold_tab.data(), fold_tab.size() * sizeof(int),
                             cudaMemcpyHostToDevice));
+  {  // omega' rows depend on the grid sizes only
+    std::vector<double> om((size_t)(L_ + 1) * 3 * oms_, 0.);
+    for (int l = 1; l < L_; ++l)
+      for (int k = 0; k < 3; ++k)
+        std::copy(t.omegap[l][k].begin(), t.omegap[l][k].end(),
+                  om.begin() + ((size_t)l * 3 + k) * oms_);
+    MSM_CUDA_TRY(cudaMemcpy(om_d_, om.data(), om.size() * sizeof(double),
+                            cudaMemcpyHostToDevice));
+  }
   if ((err = update(t))) return err;
   return tune_levels(pad_max, part_max);
 }
@@ -424,6 +456,33 @@ int Plan<T>::set_tables(const Tables &t) {
 // Box-dependent state: geometry, neighbour offsets, stencils, constants
 template <typename T>
 int Plan<T>::update(const Tables &t) {
+  // the previous evaluation may still read the tables being replaced
+  MSM_CUDA_TRY(cudaSetDevice(device_));
+  MSM_CUDA_TRY(cudaStreamSynchronize(stream_));
+  if (last_stream_ && last_stream_ != stream_)
+    MSM_CUDA_TRY(cudaStreamSynchronize(last_stream_));
+  const int st = update_box(t, stream_, false);
+  MSM_CUDA_TRY(cudaStreamSynchronize(stream_));
+  return st;
+}
+
+template <typename T>
+int Plan<T>::update_device(const Tables &t, cudaStream_t stream) {
+  MSM_CUDA_TRY(cudaSetDevice(device_));
+  if (!rebuild_ev_)
+    MSM_CUDA_TRY(cudaEventCreateWithFlags(&rebuild_ev_, cudaEventDisableTiming));
+  const int st = update_box(t, stream, true);
+  if (st != MSMPB_OK) return st;
+  MSM_CUDA_TRY(cudaEventRecord(rebuild_ev_, stream));
+  rebuild_recorded_ = true;
+  return MSMPB_OK;
+}
+
+// Box-dependent state: geometry, neighbour lists, constants, top multiplier
+// and level stencils (from t, or computed on the device), uploaded in the
+// order of s.
+template <typename T>
+int Plan<T>::update_box(const Tables &t, cudaStream_t s, bool stencils_on_device) {
   const Params &p = t.p;
   for (int r = 0; r < 3; ++r)
     for (int c = 0; c < 3; ++c) {
@@ -495,12 +554,37 @@ int Plan<T>::update(const Tables &t) {
   // index along the column in 8
   clusters_ok_ = ncoloff_ <= kMaxColumnOffsets && K2_ / geom_.nc[2] + 2 < 120;
   if (clusters_ok_)
-    MSM_CUDA_TRY(cudaMemcpy(coloff_d_, coloffs_.data(), ncoloff_ * sizeof(ColumnOffset),
-                            cudaMemcpyHostToDevice));
-  MSM_CUDA_TRY(cudaSetDevice(device_));
-  MSM_CUDA_TRY(cudaMemcpy(off_d_, offsets_.data(), noff_ * sizeof(CellOffset<T>),
-                          cudaMemcpyHostToDevice));
-  for (int l = 1; l < L_; ++l) {
+    MSM_CUDA_TRY(cudaMemcpyAsync(coloff_d_, coloffs_.data(), ncoloff_ * sizeof(ColumnOffset),
+                                 cudaMemcpyHostToDevice, s));
+  MSM_CUDA_TRY(cudaMemcpyAsync(off_d_, offsets_.data(), noff_ * sizeof(CellOffset<T>),
+                               cudaMemcpyHostToDevice, s));
+  if (stencils_on_device) {
+    // mirror symmetry in x and y holds for every orthorhombic box
+    for (int l = 1; l < L_; ++l) {
+      const int sym = fold_enabled_ && ortho && stencil_templated(sh_[l]) &&
+                      sh_[l].S[0] % 2 == 1 && sh_[l].S[1] % 2 == 1;
+      if (sym != sh_[l].sym) {
+        sh_[l].sym = sym;
+        plan_level(l);
+      }
+      LevelStencilArgs la{};
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) la.A[3 * r + c] = p.A[r][c];
+      for (int k = 0; k < 3; ++k) {
+        la.as[k] = std::sqrt(p.Ai[0][k] * p.Ai[0][k] + p.Ai[1][k] * p.Ai[1][k] +
+                             p.Ai[2][k] * p.Ai[2][k]);
+        la.g[k] = grid_[l][k];
+        la.sd[k] = sh_[l].S[k];
+      }
+      la.al = p.aCut[l];
+      for (int k = 0; k < nu_ && k < 16; ++k) la.tau[k] = t.tau[k];
+      la.nu = nu_;
+      la.oms = oms_;
+      launch_level_stencil<T>(s, la, om_d_ + (size_t)l * 3 * oms_, stwork_, kh_[l],
+                              sh_[l].sym ? khf_[l] : nullptr, !kMixed);
+    }
+  }
+  for (int l = 1; l < L_ && !stencils_on_device; ++l) {
     // rows of S2 taps padded to a 16-byte pitch (zeros), z fastest
     const int S0 = sh_[l].S[0], S1 = sh_[l].S[1], S2 = sh_[l].S[2];
     const int sp = stencil_tap_pitch(S2, !kMixed);
@@ -509,8 +593,9 @@ int Plan<T>::update(const Tables &t) {
       for (int j = 0; j < S1; ++j)
         for (int k = 0; k < S2; ++k)
           kh[((size_t)i * S1 + j) * sp + k] = (T)t.khat[l][((size_t)i * S1 + j) * S2 + k];
-    MSM_CUDA_TRY(cudaMemcpy(kh_[l], kh.data(), kh.size() * sizeof(T),
-                            cudaMemcpyHostToDevice));
+    MSM_CUDA_TRY(cudaMemcpyAsync(kh_[l], kh.data(), kh.size() * sizeof(T),
+                                 cudaMemcpyHostToDevice, s));
+    MSM_CUDA_TRY(cudaStreamSynchronize(s));  // kh is a local
     // folded taps when the stencil is mirror-symmetric in x and y
     std::vector<double> kf;
     const int sym = fold_enabled_ && stencil_templated(sh_[l]) &&
@@ -522,18 +607,17 @@ int Plan<T>::update(const Tables &t) {
     if (sh_[l].sym) {
       std::vector<T> kft(kf.size());
       for (size_t n = 0; n < kf.size(); ++n) kft[n] = (T)kf[n];
-      MSM_CUDA_TRY(cudaMemcpy(khf_[l], kft.data(), kft.size() * sizeof(T),
-                              cudaMemcpyHostToDevice));
+      MSM_CUDA_TRY(cudaMemcpyAsync(khf_[l], kft.data(), kft.size() * sizeof(T),
+                                   cudaMemcpyHostToDevice, s));
+      MSM_CUDA_TRY(cudaStreamSynchronize(s));  // kft is a local
     }
   }
-  MSM_CUDA_TRY(cudaMemcpy(khat_top_, t.khat[L_].data(),
-                          t.khat[L_].size() * sizeof(double),
-                          cudaMemcpyHostToDevice));
-  if (exec_) {
-    cudaGraphExecDestroy(exec_);
-    exec_ = nullptr;
-  }
-  have_graph_ = false;  // geometry is baked into kernel parameters
+  MSM_CUDA_TRY(cudaMemcpyAsync(khat_top_, t.khat[L_].data(),
+                               t.khat[L_].size() * sizeof(double),
+                               cudaMemcpyHostToDevice, s));
+  // geometry and constants are kernel parameters: the next graph launch
+  // re-captures and updates the instantiated graph in place
+  graph_stale_ = true;
   return MSMPB_OK;
 }
 
@@ -686,6 +770,7 @@ int Plan<T>::evaluate(const EvalRequest &r, double *energy) {
   // caller's stream (0 = the legacy default stream).
   cudaStream_t s = r.host ? stream_ : r.stream;
   last_stream_ = s;
+  if (rebuild_recorded_) MSM_CUDA_TRY(cudaStreamWaitEvent(s, rebuild_ev_, 0));
   const double *pos = r.pos, *q = r.q;
   double *force = r.force, *phi = r.phi;
   if (r.host) {
@@ -743,8 +828,10 @@ int Plan<T>::launch_graph(const EvalRequest &r, cudaStream_t s,
   key.energy = edev;
   for (int l = 0; l <= L_; ++l) key.w[l] = r.weight ? r.weight[l] : 1.0;
   key.timing = false;
-  if (!have_graph_ || !(key == key_)) {
-    if (exec_) {
+  if (!have_graph_ || !(key == key_) || graph_stale_) {
+    // same buffers, new parameters: update the instantiated graph in place
+    const bool refresh = have_graph_ && exec_ && key == key_;
+    if (exec_ && !refresh) {
       cudaGraphExecDestroy(exec_);
       exec_ = nullptr;
     }
@@ -763,7 +850,17 @@ int Plan<T>::launch_graph(const EvalRequest &r, cudaStream_t s,
       cudaGetLastError();
       return st != MSMPB_OK ? st : MSMPB_ERR_CUDA;
     }
-    cudaError_t ie = cudaGraphInstantiate(&exec_, g, 0);
+    cudaError_t ie = cudaErrorUnknown;
+    if (refresh) {
+      cudaGraphExecUpdateResultInfo info{};
+      ie = cudaGraphExecUpdate(exec_, g, &info);
+      if (ie != cudaSuccess) {  // the launch sequence changed shape
+        cudaGetLastError();
+        cudaGraphExecDestroy(exec_);
+        exec_ = nullptr;
+      }
+    }
+    if (!exec_) ie = cudaGraphInstantiate(&exec_, g, 0);
     cudaGraphDestroy(g);
     if (ie != cudaSuccess) {
       exec_ = nullptr;
@@ -771,6 +868,7 @@ int Plan<T>::launch_graph(const EvalRequest &r, cudaStream_t s,
     }
     key_ = key;
     have_graph_ = true;
+    graph_stale_ = false;
   }
   MSM_CUDA_TRY(cudaGraphLaunch(exec_, s));
   return MSMPB_OK;
@@ -860,6 +958,9 @@ FFDevice *engine_create(const Tables &t, int precision, int device, int *err) {
 void engine_destroy(FFDevice *d) { delete d; }
 
 int engine_update_tables(FFDevice *d, const Tables &t) { return d->update(t); }
+int engine_update_tables_device(FFDevice *d, const Tables &t, cudaStream_t stream) {
+  return d->update_device(t, stream);
+}
 
 int engine_evaluate(FFDevice *d, const EvalRequest &r, double *energy) {
   return d->evaluate(r, energy);

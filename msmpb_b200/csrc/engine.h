@@ -30,6 +30,9 @@ void engine_destroy(FFDevice *d);
 
 // Re-uploads box-dependent tables after FF_rebuild (same sizes).
 int engine_update_tables(FFDevice *d, const Tables &t);
+// The same with the level stencils computed on the device, ordered on
+// `stream` (t's level stencils are not read).
+int engine_update_tables_device(FFDevice *d, const Tables &t, cudaStream_t stream);
 
 struct EvalRequest {
   const double *pos;     // host or device N*3

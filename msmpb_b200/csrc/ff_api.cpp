@@ -253,6 +253,25 @@ void FF_rebuild(FF *ff, double edges[3][3], double (*position)[3],
   }
 }
 
+int FF_rebuild_device(FF *ff, double edges[3][3], void *stream) {
+  HostState *h = host(ff);
+  if (!h || !h->built) return ff->last_error = MSMPB_ERR_STATE;
+  if (!ff->dev) return ff->last_error = MSMPB_ERR_NODEVICE;
+  msm::Params p = h->params;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) p.A[i][j] = edges[i][j];
+  p.detA = msm::invert3(p.A, p.Ai);
+  if (!(p.detA > 0)) return ff->last_error = MSMPB_ERR_ARGUMENT;
+  h->params = p;
+  export_params(ff, p);
+  msm::rebuild_box_tables(h->tables, p);
+  export_tables(ff, h->tables);
+  int st = msm::engine_update_tables_device(ff->dev, h->tables,
+                                            static_cast<cudaStream_t>(stream));
+  if (st != MSMPB_OK) ff->last_error = st;
+  return st;
+}
+
 double FF_energy_potentials(FF *ff, double (*force)[3], double (*position)[3],
                             double *weight, double *potential) {
   HostState *h = host(ff);

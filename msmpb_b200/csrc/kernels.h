@@ -254,6 +254,23 @@ void launch_stencil(cudaStream_t s, const StencilShape &sh,
                     const StencilTile &tile, const T *padded, const T *kh,
                     int khz, T weight, T *e, T *part);
 
+// ---- level stencils on the device for a new box (k_setup.cu) ----
+struct LevelStencilArgs {
+  double A[9];      // row-major; columns are the box edge vectors
+  double as[3];     // column norms of A^-1
+  double al;        // cutoff of the level, a_l
+  double tau[16];   // softening polynomial coefficients
+  int nu;
+  int g[3];         // level grid dims
+  int sd[3];        // stencil dims
+  int oms;          // row stride of the omega' table (x, y, z rows)
+};
+// kp: sd0 x sd1 rows of the tap pitch; kf (may be null): folded rows;
+// om: omega'_x, omega'_y, omega'_z rows of a.oms; work: 3 sd^3 doubles
+template <typename T>
+void launch_level_stencil(cudaStream_t s, const LevelStencilArgs &a, const double *om,
+                          double *work, T *kp, T *kf, bool fp64);
+
 // ---- top-level FFT solve (k_fft.cu) ----
 bool top_solve_supported(const int M[3]);
 void top_solve_prepare();

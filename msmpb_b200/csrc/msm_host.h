@@ -57,5 +57,9 @@ void build_omegap_tables(Tables &t);
 
 // All tables for a parameter set (code/forcefield0.c:369-467, :598-675).
 void build_tables(Tables &t, const Params &p);
+// New box, same grid sizes and order: refreshes the box-dependent constants
+// and the top-level multiplier; the level stencils t.khat[1..L-1] are left
+// as they are (the device computes its own).
+void rebuild_box_tables(Tables &t, const Params &p);
 
 }  // namespace msm

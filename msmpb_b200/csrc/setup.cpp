@@ -440,4 +440,11 @@ void build_tables(Tables &t, const Params &p) {
   for (int l = p.L - 1; l >= 1; --l) make_level_stencil(t, l, as);
 }
 
+void rebuild_box_tables(Tables &t, const Params &p) {
+  t.p = p;
+  const double as[3] = {norm_col(p.Ai, 0), norm_col(p.Ai, 1), norm_col(p.Ai, 2)};
+  make_constants(t, as);
+  make_top(t);
+}
+
 }  // namespace msm

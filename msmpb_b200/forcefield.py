@@ -202,6 +202,15 @@ class ForceField:
         if err not in (L.OK, L.ERR_NODEVICE):
             raise MSMError(err, "FF_rebuild")
 
+    def rebuild_device(self, edges, stream=0):
+        """FF_rebuild_device: new box, level stencils computed on the GPU in
+        the order of `stream` (a CUDA stream handle; 0 = legacy default)."""
+        self.edges = _f64(np.asarray(edges).reshape(3, 3)).copy()
+        st = self._lib.FF_rebuild_device(self.ff, _ptr(self.edges),
+                                         C.c_void_p(stream) if stream else None)
+        if st != L.OK:
+            raise MSMError(st, "FF_rebuild_device")
+
     def close(self):
         if getattr(self, "ff", None):
             self._lib.FF_delete(self.ff)

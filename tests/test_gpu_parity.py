@@ -228,3 +228,41 @@ def test_error_estimate_after_evaluation():
     ff = ForceField(q, pos, edges, **kw, precision="mixed")
     ff.energy(pos)
     assert ff.err_est() == pytest.approx(o.err_est(), rel=1e-12)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_rebuild_device_box_change(precision):
+    """FF_rebuild_device (level stencils computed on the GPU) against the FP64
+    FF_rebuild of the same box on the host, for a larger, a smaller and a
+    triclinic box (where the stencils lose their mirror symmetry), and against
+    the oracle where the new box keeps the build-time nLim (a rebuild keeps
+    every build-time choice, code/forcefield0.c:598-680)."""
+    q, pos, edges = systems.water(8000, 62.0, 11)
+    kw = dict(cutoff=9.0, order=6, levels=3, top_grid=6)
+    te, tf, tp = TOL[precision]
+    ff = ForceField(q, pos, edges, **kw, precision=precision)
+    ff.set_timing(False)
+    ff.energy(pos)  # a captured graph exists before the box changes
+    tri = np.array([[62.0, 0.0, 0.0], [5.0, 62.0, 0.0], [-3.0, 2.0, 62.0]])
+    for e2, p2 in ((edges * 1.03, pos * 1.03), (edges * 0.98, pos * 0.98), (tri, pos)):
+        ff.rebuild_device(e2)
+        e, f, phi = ff.energy(p2, potentials=True)
+        host = ForceField(q, pos, edges, **kw, precision="fp64")
+        host.rebuild(e2, p2)
+        eh, fh, ph = host.energy(p2, potentials=True)
+        host.close()
+        scale = 1e-1 if precision == "fp64" else 1.0  # FP64: 1e-12 / 1e-11
+        assert abs(e - eh) / abs(eh) < te * scale
+        assert force_err(f, fh, q, e2) < tf * scale
+        assert rel_rms(phi, ph) < tp * scale
+    # the larger box keeps nLim: the oracle built there is the same operator
+    e2, p2 = edges * 1.03, pos * 1.03
+    ff.rebuild_device(e2)
+    e, f, phi = ff.energy(p2, potentials=True)
+    o = Oracle(q, e2, cutoff=9.0, nu=6, levels=3, top_grid=6)
+    assert o.nlim == ff.nlim
+    eo, fo, po = o.energy(p2)
+    assert abs(e - eo) / abs(eo) < te
+    assert force_err(f, fo, q, e2) < tf
+    assert rel_rms(phi, po) < tp
+    ff.close()
