@@ -25,6 +25,9 @@ Outputs (all under oracle/_ref/):
   libmsmpb_ref.so            patched library (+ ``struct O o`` definition)
   libmsmpb_ref_unpatched.so  unpatched library
   msmpb_ref                  the reference CLI driver over the patched sources
+  msmpb_dropin               the same driver source, unmodified, compiled against
+                             this project's include/forcefield.h and linked to
+                             msmpb_b200/libmsmpb.so (the drop-in check of the CLI)
 
 Usage: python oracle/build_ref.py [--reference DIR]
 """
@@ -99,6 +102,16 @@ def build(reference_root="/root/reference", quiet=False):
          "-o", os.path.join(OUT, "libmsmpb_ref_unpatched.so")])
     run([cc, *CFLAGS, *inc, drv, ff0, ff1p, fft, "-lm",
          "-o", os.path.join(OUT, "msmpb_ref")])
+    # the unmodified driver against this project's header and library; a
+    # scratch copy, so that its quoted include finds include/forcefield.h
+    root = os.path.dirname(HERE)
+    our_lib_dir = os.path.join(root, "msmpb_b200")
+    if os.path.exists(os.path.join(our_lib_dir, "libmsmpb.so")):
+        drv_copy = os.path.join(src_dir, "msmpb_dropin.c")
+        shutil.copy(drv, drv_copy)
+        run([cc, "-O2", "-std=gnu11", "-w", "-I", os.path.join(root, "include"), drv_copy,
+             "-L", our_lib_dir, "-lmsmpb", "-lm", "-Wl,-rpath,$ORIGIN/../../msmpb_b200",
+             "-o", os.path.join(OUT, "msmpb_dropin")])
     if not quiet:
         print("build_ref: built", OUT)
     return True
