@@ -214,12 +214,75 @@ __device__ __forceinline__ void tile(const PairConsts<T> &pc, const V4<T> &ai,
   }
 }
 
+// Two tiles at once in the mixed form (queue entries e, e+1 on the two
+// halves of packed FP32 registers: fma.rn.f32x2 and friends do two FP32
+// operations per instruction, each rounded as the scalar one). X = (x_e,
+// x_e+1, y_e, y_e+1), Y = (z_e, z_e+1, q_e, q_e+1). Pairs beyond the cutoff
+// contribute exactly zero (their charge is masked, their r^2 replaced by a
+// safe value); close pairs and the atom itself go the scalar way.
+template <int NU>
+__device__ __forceinline__ void tile2(const PairConsts<float> &pc, const V4<float> &ai,
+                                      const float4 &X, const float4 &Y, const int *qunit,
+                                      int e, int jq, int islot, const int *qcode,
+                                      int2 *closeq, int &nclose, float2 &px, float2 &py,
+                                      float2 &pz, float2 &pp) {
+  const float2 nx = make_float2(-ai.x, -ai.x), ny = make_float2(-ai.y, -ai.y),
+               nz = make_float2(-ai.z, -ai.z);
+  const float2 dx = __fadd2_rn(make_float2(X.x, X.y), nx);
+  const float2 dy = __fadd2_rn(make_float2(X.z, X.w), ny);
+  const float2 dz = __fadd2_rn(make_float2(Y.x, Y.y), nz);
+  float2 r2 = __fmul2_rn(dx, dx);
+  r2 = __ffma2_rn(dy, dy, r2);
+  r2 = __ffma2_rn(dz, dz, r2);
+  bool h0 = r2.x < pc.a02, h1 = r2.y < pc.a02;
+  if (!(h0 || h1)) return;
+  // the atom itself is skipped; close pairs are recorded for the FP64 pass
+  // while there is room (else they stay here, in FP32)
+  auto consumed = [&](int ee, float r) {
+    const int jslot = qunit[ee] * 4 + jq;
+    if (r == 0.f && jslot == islot) return true;
+    if (nclose < kCloseCap) {
+      closeq[nclose++] = make_int2(jslot, qcode[ee]);
+      return true;
+    }
+    return false;
+  };
+  if (h0 && r2.x < pc.close2 && consumed(e, r2.x)) h0 = false;
+  if (h1 && r2.y < pc.close2 && consumed(e + 1, r2.y)) h1 = false;
+  if (!(h0 || h1)) return;
+  const float2 rr = make_float2(h0 ? r2.x : pc.a02, h1 ? r2.y : pc.a02);
+  const float2 qj = make_float2(h0 ? Y.z : 0.f, h1 ? Y.w : 0.f);
+  const float2 s = __ffma2_rn(rr, make_float2(pc.inv_a02, pc.inv_a02), make_float2(-1.f, -1.f));
+  float2 ts = make_float2(pc.tau[NU - 1], pc.tau[NU - 1]), t1 = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int m = NU - 2; m >= 0; --m) {
+    t1 = __ffma2_rn(s, t1, ts);
+    ts = __ffma2_rn(s, ts, make_float2(pc.tau[m], pc.tau[m]));
+  }
+  const float2 rinv = make_float2(rsqrtf(rr.x), rsqrtf(rr.y));
+  const float2 pot =
+      __fmul2_rn(qj, __ffma2_rn(ts, make_float2(-pc.inv_a0, -pc.inv_a0), rinv));
+  const float2 rinv3 = __fmul2_rn(__fmul2_rn(rinv, rinv), rinv);
+  const float2 fs = __fmul2_rn(
+      make_float2(-qj.x, -qj.y),
+      __ffma2_rn(t1, make_float2(pc.two_inv_a03, pc.two_inv_a03), rinv3));
+  pp = __fadd2_rn(pp, pot);
+  px = __ffma2_rn(fs, dx, px);
+  py = __ffma2_rn(fs, dy, py);
+  pz = __ffma2_rn(fs, dz, pz);
+}
+
 template <typename T, int NU, bool MIXED>
 __global__ void __launch_bounds__(kWarps * 32)
 k_pair_clusters(PairClusterArgs<T> a, PairConsts<T> pc) {
   // passing units of the current batch: their 4 atoms shifted into the
   // i-cluster's frame, the unit index and the (column, image) code
-  __shared__ V4<T> qatoms[kWarps][32][4];
+  // (mixed form: entries interleaved in pairs, at qpk[w][e/2][8 jq ..] =
+  // x_e, x_e+1, y_e, y_e+1, z_e, z_e+1, q_e, q_e+1; each pair's block padded to
+  // 36 words so that the per-slot writes of one warp spread over the banks)
+  constexpr int kPk = 36;
+  __shared__ V4<T> qatoms[MIXED ? 1 : kWarps][MIXED ? 1 : 32][4];
+  __shared__ __align__(16) float qpk[MIXED ? kWarps : 1][16][kPk];
   __shared__ int qunit[kWarps][32], qcode[kWarps][32];
   __shared__ int item_off[kWarps][32], item_u0[kWarps][32], item_code[kWarps][32];
   __shared__ int2 closeq[MIXED ? kWarps : 1][MIXED ? 32 * kCloseCap : 1];
@@ -320,7 +383,15 @@ k_pair_clusters(PairClusterArgs<T> a, PairConsts<T> pc) {
           v.x += esx;
           v.y += esy;
           v.z += esz;
-          qatoms[warp][slot][q] = v;
+          if constexpr (MIXED) {
+            float *d = &qpk[warp][slot >> 1][8 * q + (slot & 1)];
+            d[0] = v.x;
+            d[2] = v.y;
+            d[4] = v.z;
+            d[6] = v.w;
+          } else {
+            qatoms[warp][slot][q] = v;
+          }
         }
         qunit[warp][slot] = eunit;
         qcode[warp][slot] = ecode;
@@ -330,16 +401,39 @@ k_pair_clusters(PairClusterArgs<T> a, PairConsts<T> pc) {
       T px = 0, py = 0, pz = 0, pp = 0;
       const int *qu = qunit[warp], *qc = qcode[warp];
       int e = 0;
-      for (; e + 2 <= nq; e += 2) {
-        const V4<T> a0 = qatoms[warp][e][jq], a1 = qatoms[warp][e + 1][jq];
-        tile<T, NU, MIXED>(pc, ai, a0, qu, e, jq, islot, qc, myclose, nclose, px, py, pz,
-                           pp);
-        tile<T, NU, MIXED>(pc, ai, a1, qu, e + 1, jq, islot, qc, myclose, nclose, px, py,
-                           pz, pp);
+      if constexpr (MIXED) {
+        float2 px2 = make_float2(0.f, 0.f), py2 = px2, pz2 = px2, pp2 = px2;
+        for (; e + 2 <= nq; e += 2) {
+          const float4 X = *reinterpret_cast<const float4 *>(&qpk[warp][e >> 1][8 * jq]);
+          const float4 Y = *reinterpret_cast<const float4 *>(&qpk[warp][e >> 1][8 * jq + 4]);
+          tile2<NU>(pc, ai, X, Y, qu, e, jq, islot, qc, myclose, nclose, px2, py2, pz2, pp2);
+        }
+        px = px2.x + px2.y;
+        py = py2.x + py2.y;
+        pz = pz2.x + pz2.y;
+        pp = pp2.x + pp2.y;
+        if (e < nq) {  // the last, unpaired entry (even index: first half)
+          const float *d = &qpk[warp][e >> 1][8 * jq];
+          V4<T> aj;
+          aj.x = d[0];
+          aj.y = d[2];
+          aj.z = d[4];
+          aj.w = d[6];
+          tile<T, NU, MIXED>(pc, ai, aj, qu, e, jq, islot, qc, myclose, nclose, px, py, pz,
+                             pp);
+        }
+      } else {
+        for (; e + 2 <= nq; e += 2) {
+          const V4<T> a0 = qatoms[warp][e][jq], a1 = qatoms[warp][e + 1][jq];
+          tile<T, NU, MIXED>(pc, ai, a0, qu, e, jq, islot, qc, myclose, nclose, px, py, pz,
+                             pp);
+          tile<T, NU, MIXED>(pc, ai, a1, qu, e + 1, jq, islot, qc, myclose, nclose, px, py,
+                             pz, pp);
+        }
+        if (e < nq)
+          tile<T, NU, MIXED>(pc, ai, qatoms[warp][e][jq], qu, e, jq, islot, qc, myclose,
+                             nclose, px, py, pz, pp);
       }
-      if (e < nq)
-        tile<T, NU, MIXED>(pc, ai, qatoms[warp][e][jq], qu, e, jq, islot, qc, myclose,
-                           nclose, px, py, pz, pp);
       __syncwarp();
       if (MIXED) {
         fx.add(px);
