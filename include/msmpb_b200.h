@@ -63,6 +63,29 @@ int FF_energy_device(FF *ff, const double *position_d, const double *charge_d,
 /* Waits for the library's stream and reports device-side check failures. */
 int FF_sync(FF *ff);
 
+/* Adjoint of an evaluation (no counterpart in the reference, which computes
+ * no derivatives beyond forces): for a force cotangent Fbar (device, N*3)
+ * and an energy cotangent Ubar, the gradients of
+ *   L = Ubar U + sum_i Fbar_i . F_i
+ * with respect to the charges (charge_grad_d, N) and the positions
+ * (position_grad_d, N*3), device outputs in input order, either may be
+ * NULL; same inputs, weights and stream conventions as FF_energy_device.
+ * The transposed operator chain runs on the GPU: the short-range pair
+ * Hessian, anterpolation of the dipoles q_i Fbar_i with derivative
+ * B-splines, the same grid operator, interpolation with first and second
+ * derivative B-splines. reuse_forward != 0 promises that the last
+ * evaluation of this handle (FF_evaluation_count) had these inputs and
+ * weights and reuses its grids and per-atom results; otherwise a forward
+ * pass runs first. Finest grids smaller than the B-spline order along an
+ * axis return MSMPB_ERR_UNSUPPORTED. */
+int FF_adjoint_device(FF *ff, const double *position_d, const double *charge_d,
+                      const double *weight, const double *force_bar_d, double energy_bar,
+                      double *charge_grad_d, double *position_grad_d, int reuse_forward,
+                      void *stream);
+
+/* Forward evaluations run by this handle so far (any entry point). */
+long FF_evaluation_count(const FF *ff);
+
 /* FF_rebuild (code/forcefield0.c:598-680: new box, every build-time choice
  * kept) with the level stencils computed on the GPU, ordered on `stream`
  * (a cudaStream_t; NULL = the legacy default stream) with no host

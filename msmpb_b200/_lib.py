@@ -39,7 +39,8 @@ EXPORTED = [
     "FF_get_precision", "FF_set_device", "FF_energy_potentials",
     "FF_energy_device", "FF_sync", "FF_phase_times", "FF_kernel_launches",
     "FF_stencil_times", "FF_set_timing", "msmpb_measure_fp32_tflops",
-    "msmpb_level_stencil_noalloc", "FF_rebuild_device",
+    "msmpb_level_stencil_noalloc", "FF_rebuild_device", "FF_adjoint_device",
+    "FF_evaluation_count",
 ]
 
 _lib = None
@@ -97,6 +98,10 @@ def load():
         "FF_build": (None, [P, C.c_int, _dp, _dp, C.c_double]),
         "FF_rebuild": (None, [P, _dp, _dp, C.c_double]),
         "FF_rebuild_device": (C.c_int, [P, _dp, C.c_void_p]),
+        "FF_adjoint_device": (C.c_int, [P, C.c_void_p, C.c_void_p, _dp, C.c_void_p,
+                                        C.c_double, C.c_void_p, C.c_void_p, C.c_int,
+                                        C.c_void_p]),
+        "FF_evaluation_count": (C.c_long, [P]),
         "FF_energy": (C.c_double, [P, _dp, _dp, _dp]),
         "FF_energy_potentials": (C.c_double, [P, _dp, _dp, _dp, _dp]),
         "FF_energy_device": (C.c_int, [P, C.c_void_p, C.c_void_p, _dp,

@@ -30,6 +30,8 @@ struct FFDevice {
   // `stream` (no host synchronisation); t holds everything else
   virtual int update_device(const msm::Tables &t, cudaStream_t stream) = 0;
   virtual int evaluate(const msm::EvalRequest &r, double *energy) = 0;
+  virtual int adjoint(const msm::AdjointRequest &r) = 0;
+  virtual long evaluations() const = 0;
   virtual int sync() = 0;
   virtual int phase_times(double *ms, int n) = 0;
   virtual int launches() = 0;
@@ -90,6 +92,8 @@ class Plan : public FFDevice {
   int update(const Tables &t) override;
   int update_device(const Tables &t, cudaStream_t stream) override;
   int evaluate(const EvalRequest &r, double *energy) override;
+  int adjoint(const AdjointRequest &r) override;
+  long evaluations() const override { return nevals_; }
   int sync() override;
   int phase_times(double *ms, int n) override;
   int launches() override { return nlaunch_; }
@@ -110,6 +114,7 @@ class Plan : public FFDevice {
  private:
   int set_tables(const Tables &t);
   int update_box(const Tables &t, cudaStream_t s, bool stencils_on_device);
+  int enqueue_chain(cudaStream_t s, T *const *qg, T *const *eg, const double *w, bool tm);
   int tune_levels(size_t pad_cap, size_t part_cap);
   int launch_graph(const EvalRequest &r, cudaStream_t s, const double *pos,
                    const double *q, double *force, double *phi, double *edev);
@@ -212,6 +217,12 @@ class Plan : public FFDevice {
   GraphKey key_{};
   bool have_graph_ = false;
   bool graph_stale_ = false;  // kernel parameters changed (new box)
+  long nevals_ = 0;           // forward evaluations so far
+  // adjoint buffers (allocated on first use)
+  void *adj_mem_ = nullptr;
+  V4<T> *fbs_ = nullptr, *dip_ = nullptr, *adj_a_ = nullptr, *adj_b_ = nullptr,
+        *adj_g_ = nullptr, *adj_h_ = nullptr;
+  T *qg2_[kMaxLevels + 2] = {}, *eg2_[kMaxLevels + 2] = {};
   // recorded after a device-side rebuild; every later evaluation's stream
   // waits for it (the rebuild may run on another stream)
   cudaEvent_t rebuild_ev_ = nullptr;
@@ -231,6 +242,7 @@ Plan<T>::~Plan() {
   if (stream_) cudaStreamSynchronize(stream_);
   if (exec_) cudaGraphExecDestroy(exec_);
   if (rebuild_ev_) cudaEventDestroy(rebuild_ev_);
+  if (adj_mem_) cudaFree(adj_mem_);
   for (auto &e : ev_)
     if (e) cudaEventDestroy(e);
   for (auto &pr : lev_ev_)
@@ -621,6 +633,36 @@ int Plan<T>::update_box(const Tables &t, cudaStream_t s, bool stencils_on_device
   return MSMPB_OK;
 }
 
+// The grid operator K: q[1] -> e[1] (restriction, top solve, then from the
+// coarsest level down, prolongation plus the level stencil). Returns the
+// number of kernel launches.
+template <typename T>
+int Plan<T>::enqueue_chain(cudaStream_t s, T *const *qg, T *const *eg, const double *w,
+                           bool tm) {
+  int nl = 0;
+  mark(s, kPhaseRestrict, tm);
+  for (int l = 1; l < L_; ++l) {
+    launch_restrict<T>(s, grid_[l], qg[l], qg[l + 1], J_, nu_);
+    nl += 1;
+  }
+  mark(s, kPhaseTop, tm);
+  launch_top_solve<T>(s, grid_[L_], qg[L_], khat_top_, w[L_], fft_, nullptr, eg[L_]);
+  nl += 5;
+  for (int l = L_ - 1; l >= 1; --l) {
+    mark(s, kPhaseProlong, tm && l == L_ - 1);
+    cudaMemsetAsync(eg[l], 0, (size_t)grid_[l][0] * grid_[l][1] * grid_[l][2] * sizeof(T), s);
+    launch_prolong_add<T>(s, grid_[l], eg[l + 1], eg[l], J_, nu_);
+    mark(s, kPhaseStencil, tm && l == L_ - 1);
+    launch_pad<T>(s, sh_[l], qg[l], padded_);
+    if (tm) cudaEventRecord(lev_ev_[l][0], s);
+    launch_stencil<T>(s, sh_[l], tile_[l], padded_, level_taps(l),
+                      stencil_tap_pitch(sh_[l].S[2], !kMixed), (T)w[l], eg[l], part_);
+    if (tm) cudaEventRecord(lev_ev_[l][1], s);
+    nl += 3;
+  }
+  return nl;
+}
+
 template <typename T>
 int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
                      const double *q, double *force, double *phi,
@@ -693,32 +735,7 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   launch_anterpolate<T>(s, grid_[1], gsorted_, gcs_, gstart_, sc_, qg_[1],
                         anterp_variant_, err_d_, N_, anterp_scratch_, fold_tab_);
   nl += (anterp_variant_ == 0 && anterp_scratch_) ? 2 : 1;
-  mark(s, kPhaseRestrict, tm);
-  for (int l = 1; l < L_; ++l) {
-    launch_restrict<T>(s, grid_[l], qg_[l], qg_[l + 1], J_, nu_);
-    nl += 1;
-  }
-  mark(s, kPhaseTop, tm);
-  launch_top_solve<T>(s, grid_[L_], qg_[L_], khat_top_, w[L_], fft_, nullptr,
-                      eg_[L_]);
-  nl += 5;
-  // levels L-1..1: prolongation then the level stencil
-  float pro_ms = 0;
-  (void)pro_ms;
-  for (int l = L_ - 1; l >= 1; --l) {
-    mark(s, kPhaseProlong, tm && l == L_ - 1);
-    cudaMemsetAsync(eg_[l], 0,
-                    (size_t)grid_[l][0] * grid_[l][1] * grid_[l][2] * sizeof(T), s);
-    launch_prolong_add<T>(s, grid_[l], eg_[l + 1], eg_[l], J_, nu_);
-    mark(s, kPhaseStencil, tm && l == L_ - 1);
-    launch_pad<T>(s, sh_[l], qg_[l], padded_);
-    if (tm) cudaEventRecord(lev_ev_[l][0], s);
-    launch_stencil<T>(s, sh_[l], tile_[l], padded_, level_taps(l),
-                      stencil_tap_pitch(sh_[l].S[2], !kMixed), (T)w[l], eg_[l],
-                      part_);
-    if (tm) cudaEventRecord(lev_ev_[l][1], s);
-    nl += 3;
-  }
+  nl += enqueue_chain(s, qg_, eg_, w, tm);
   mark(s, kPhaseInterp, tm);
   launch_grid_dot<T>(s, (size_t)ncg_, qg_[1], eg_[1], grid_parts_, ngrid_);
   launch_interpolate<T>(s, N_, grid_[1], gsorted_, gcs_, eg_[1], sc_, geom_, gout_);
@@ -771,6 +788,7 @@ int Plan<T>::evaluate(const EvalRequest &r, double *energy) {
   cudaStream_t s = r.host ? stream_ : r.stream;
   last_stream_ = s;
   if (rebuild_recorded_) MSM_CUDA_TRY(cudaStreamWaitEvent(s, rebuild_ev_, 0));
+  ++nevals_;
   const double *pos = r.pos, *q = r.q;
   double *force = r.force, *phi = r.phi;
   if (r.host) {
@@ -812,6 +830,80 @@ int Plan<T>::evaluate(const EvalRequest &r, double *energy) {
     if (energy) *energy = e;
     if (r.q2) *r.q2 = qs[1];
     return st;
+  }
+  return MSMPB_OK;
+}
+
+template <typename T>
+int Plan<T>::adjoint(const AdjointRequest &r) {
+  MSM_CUDA_TRY(cudaSetDevice(device_));
+  if (!anterp_scratch_ || !fold_tab_) return MSMPB_ERR_UNSUPPORTED;
+  if (!r.pos || !r.q || !r.fbar) return MSMPB_ERR_ARGUMENT;
+  if (!adj_mem_) {
+    // six per-atom records and a second set of level grids
+    size_t bytes = 6 * (size_t)N_ * sizeof(V4<T>) + 256 * 6;
+    for (int l = 1; l <= L_; ++l)
+      bytes += 2 * ((size_t)grid_[l][0] * grid_[l][1] * grid_[l][2] * sizeof(T) + 256);
+    if (cudaMalloc(&adj_mem_, bytes) != cudaSuccess) {
+      adj_mem_ = nullptr;
+      cudaGetLastError();
+      return MSMPB_ERR_NOMEM;
+    }
+    char *p = static_cast<char *>(adj_mem_);
+    auto take = [&](size_t b) {
+      char *q = p;
+      p += (b + 255) / 256 * 256;
+      return q;
+    };
+    for (V4<T> **b : {&fbs_, &dip_, &adj_a_, &adj_b_, &adj_g_, &adj_h_})
+      *b = reinterpret_cast<V4<T> *>(take((size_t)N_ * sizeof(V4<T>)));
+    for (int l = 1; l <= L_; ++l) {
+      const size_t g = (size_t)grid_[l][0] * grid_[l][1] * grid_[l][2] * sizeof(T);
+      qg2_[l] = reinterpret_cast<T *>(take(g));
+      eg2_[l] = reinterpret_cast<T *>(take(g));
+    }
+  }
+  cudaStream_t s = r.stream;
+  last_stream_ = s;
+  if (rebuild_recorded_) MSM_CUDA_TRY(cudaStreamWaitEvent(s, rebuild_ev_, 0));
+  double w[kMaxLevels + 1];
+  for (int l = 0; l <= L_; ++l) w[l] = r.weight ? r.weight[l] : 1.0;
+  cudaGetLastError();
+  if (!r.reuse) {  // the forward state this adjoint linearises about
+    EvalRequest fr{};
+    fr.pos = r.pos;
+    fr.q = r.q;
+    fr.weight = r.weight;
+    const int st = enqueue(fr, s, r.pos, r.q, nullptr, nullptr, energy_);
+    if (st != MSMPB_OK) return st;
+    ++nevals_;
+  }
+  launch_adj_gather<T>(s, N_, pperm_, r.fbar, fbs_);
+  launch_adj_pair<T>(s, N_, psorted_, fbs_, pcs_, pstart_, geom_, off_d_, noff_, pc_, adj_a_,
+                     adj_b_);
+  launch_adj_dipoles<T>(s, N_, gperm_, r.q, r.fbar, geom_, dip_);
+  launch_adj_anterpolate<T>(s, grid_[1], gsorted_, gcs_, gstart_, sc_, dip_, qg2_[1],
+                            anterp_scratch_, fold_tab_);
+  enqueue_chain(s, qg2_, eg2_, w, false);
+  launch_adj_interpolate<T>(s, N_, grid_[1], gsorted_, gcs_, gperm_, r.fbar, eg2_[1],
+                            eg_[1], sc_, geom_, adj_g_, adj_h_);
+  AdjointCombineArgs ca{};
+  ca.N = N_;
+  ca.w0 = w[0];
+  ca.coeff1 = coeff1_;
+  ca.coeff2 = coeff2_;
+  ca.gamma0_over_a0 = gamma0_a0_;
+  ca.q = r.q;
+  ca.qstats = qstats_;
+  ca.fbar = r.fbar;
+  ca.ubar = r.ubar;
+  ca.dq = r.dq;
+  ca.dr = r.dr;
+  launch_adj_combine<T>(s, ca, pinv_, ginv_, pout_, gout_, adj_a_, adj_b_, adj_g_, adj_h_);
+  const cudaError_t ce = cudaGetLastError();
+  if (ce != cudaSuccess) {
+    std::fprintf(stderr, "msmpb_b200: adjoint launch error: %s\n", cudaGetErrorString(ce));
+    return MSMPB_ERR_CUDA;
   }
   return MSMPB_OK;
 }
@@ -958,6 +1050,8 @@ FFDevice *engine_create(const Tables &t, int precision, int device, int *err) {
 void engine_destroy(FFDevice *d) { delete d; }
 
 int engine_update_tables(FFDevice *d, const Tables &t) { return d->update(t); }
+int engine_adjoint(FFDevice *d, const AdjointRequest &r) { return d->adjoint(r); }
+long engine_evaluations(FFDevice *d) { return d->evaluations(); }
 int engine_update_tables_device(FFDevice *d, const Tables &t, cudaStream_t stream) {
   return d->update_device(t, stream);
 }

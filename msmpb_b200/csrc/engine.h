@@ -52,6 +52,21 @@ struct EvalRequest {
 // *energy; device mode is asynchronous. Returns an MSMPB_* status.
 int engine_evaluate(FFDevice *d, const EvalRequest &r, double *energy);
 
+// Adjoint of one evaluation (see k_adjoint.cu): for the cotangents fbar
+// (device, N*3) and ubar, charge and position gradients of
+// ubar U + sum fbar . F (device outputs, input order, each may be null).
+// reuse: the last evaluation of this plan had these inputs and weights, so
+// its retained state is used; otherwise a forward pass runs first.
+struct AdjointRequest {
+  const double *pos, *q, *weight, *fbar;
+  double ubar;
+  double *dq, *dr;
+  bool reuse;
+  cudaStream_t stream;
+};
+int engine_adjoint(FFDevice *d, const AdjointRequest &r);
+long engine_evaluations(FFDevice *d);
+
 // Waits for outstanding work and returns device-side check flags as status.
 int engine_sync(FFDevice *d);
 

@@ -337,6 +337,33 @@ int FF_energy_device(FF *ff, const double *position_d, const double *charge_d,
   return st;
 }
 
+int FF_adjoint_device(FF *ff, const double *position_d, const double *charge_d,
+                      const double *weight, const double *force_bar_d, double energy_bar,
+                      double *charge_grad_d, double *position_grad_d, int reuse_forward,
+                      void *stream) {
+  HostState *h = host(ff);
+  if (!h || !h->built) return ff->last_error = MSMPB_ERR_STATE;
+  if (!ff->dev) return ff->last_error = MSMPB_ERR_NODEVICE;
+  if (!position_d || !charge_d || !force_bar_d) return ff->last_error = MSMPB_ERR_ARGUMENT;
+  msm::AdjointRequest r{};
+  r.pos = position_d;
+  r.q = charge_d;
+  r.weight = weight;
+  r.fbar = force_bar_d;
+  r.ubar = energy_bar;
+  r.dq = charge_grad_d;
+  r.dr = position_grad_d;
+  r.reuse = reuse_forward != 0;
+  r.stream = static_cast<cudaStream_t>(stream);
+  const int st = msm::engine_adjoint(ff->dev, r);
+  if (st != MSMPB_OK) ff->last_error = st;
+  return st;
+}
+
+long FF_evaluation_count(const FF *ff) {
+  return ff->dev ? msm::engine_evaluations(ff->dev) : 0;
+}
+
 int FF_sync(FF *ff) {
   if (!ff->dev) return MSMPB_ERR_NODEVICE;
   int st = msm::engine_sync(ff->dev);

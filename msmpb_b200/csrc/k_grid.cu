@@ -48,6 +48,28 @@ __device__ __forceinline__ T bspline_d(const SplineConsts<T> &sc, int i, T t,
   return v;
 }
 
+// value, d/dt and d^2/dt^2
+template <typename T, int NU>
+__device__ __forceinline__ T bspline_d2(const SplineConsts<T> &sc, int i, T t, T &d1, T &d2) {
+  T sign = T(1);
+  if (i >= NU / 2) {
+    i = NU - 1 - i;
+    t = T(1) - t;
+    sign = T(-1);
+  }
+  const T *c = sc.Q + i * NU;
+  T v = c[NU - 1], dv = T(0), ddv = T(0);
+#pragma unroll
+  for (int k = NU - 2; k >= 0; --k) {
+    ddv = dv + t * ddv;
+    dv = v + t * dv;
+    v = c[k] + t * v;
+  }
+  d1 = sign * dv;
+  d2 = T(2) * ddv;
+  return v;
+}
+
 // Anterpolation as an atomic-free gather: grid point g collects from the
 // atoms of cells g + n, n in [-nu/2, nu/2)^3, in cell order (atoms within a
 // cell ordered by index), so the sum order is fixed.
@@ -249,13 +271,20 @@ struct TileGeom {
   static constexpr int NW = 3 * NU + 2;   // weight row (even: vector loads)
 };
 
-template <typename T, int NU>
+// DIP: dipoles instead of charges (the adjoint's dipole grid,
+// d_g = sum_i p_i . grad B_i(g)): dip[k] holds the atom's dipole in grid
+// units, p^_a = M_a (A^-1 p)_a, and a contribution is
+// p^x Q'x Qy Qz + p^y Qx Q'y Qz + p^z Qx Qy Q'z. Weight row: P = p^x Q'x, Qx,
+// Qy, Qz, p^y Q'y, p^z Q'z (nu each).
+template <typename T, int NU, bool DIP>
 __global__ void __launch_bounds__(32)
 k_anterp_tiles(int M0, int M1, int M2, int nt1, int nt2, const V4<T> *__restrict__ atoms,
                const int *__restrict__ cell, const int *__restrict__ start,
-               SplineConsts<T> sc, T *__restrict__ scratch) {
+               SplineConsts<T> sc, T *__restrict__ scratch, const V4<T> *__restrict__ dip) {
   using G = TileGeom<NU>;
-  constexpr int E = G::E, NW = G::NW;
+  constexpr int E = G::E, NW = DIP ? 6 * NU + 2 : G::NW;
+  // offsets of the y and z weights in the row
+  constexpr int OY = DIP ? 2 * NU : NU, OZ = DIP ? 3 * NU : 2 * NU;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *acc = reinterpret_cast<T *>(smem_raw);  // G::E3 values
   __shared__ __align__(16) T w[32 * NW];
@@ -273,8 +302,8 @@ k_anterp_tiles(int M0, int M1, int M2, int nt1, int nt2, const V4<T> *__restrict
   for (int f = 0; f < G::FP; ++f) {
     const int pr = f * 32 + lane, b = pr / NU, c = pr % NU;
     poff[f] = b * E + c;
-    pwb[f] = NU + b;
-    pwc[f] = 2 * NU + c;
+    pwb[f] = OY + b;
+    pwc[f] = OZ + c;
   }
   int roff[G::RR > 0 ? G::RR : 1], ra[G::RR > 0 ? G::RR : 1], rb[G::RR > 0 ? G::RR : 1],
       rc[G::RR > 0 ? G::RR : 1];
@@ -287,8 +316,8 @@ k_anterp_tiles(int M0, int M1, int M2, int nt1, int nt2, const V4<T> *__restrict
       const int pr = G::FP * 32 + ci / NU, a = ci % NU, b = pr / NU, c = pr % NU;
       roff[r] = a * E * E + b * E + c;
       ra[r] = a;
-      rb[r] = NU + b;
-      rc[r] = 2 * NU + c;
+      rb[r] = OY + b;
+      rc[r] = OZ + c;
     }
   }
   // the 64 cell rows of the tile
@@ -337,11 +366,25 @@ k_anterp_tiles(int M0, int M1, int M2, int nt1, int nt2, const V4<T> *__restrict
       const int z = (int)(cell[g] - c0);  // the row's cells are c0 .. c0 + nz - 1
       base[lane] = (x + NU - 1) * E * E + (y + NU - 1) * E + (z + NU - 1);
       T *wl = w + lane * NW;
+      if constexpr (DIP) {
+        const V4<T> dp = dip[g];
 #pragma unroll
-      for (int i = 0; i < NU; ++i) {
-        wl[i] = at.w * bspline<T, NU>(sc, i, at.x);
-        wl[NU + i] = bspline<T, NU>(sc, i, at.y);
-        wl[2 * NU + i] = bspline<T, NU>(sc, i, at.z);
+        for (int i = 0; i < NU; ++i) {
+          T d;
+          wl[NU + i] = bspline_d<T, NU>(sc, i, at.x, d);
+          wl[i] = dp.x * d;
+          wl[OY + i] = bspline_d<T, NU>(sc, i, at.y, d);
+          wl[4 * NU + i] = dp.y * d;
+          wl[OZ + i] = bspline_d<T, NU>(sc, i, at.z, d);
+          wl[5 * NU + i] = dp.z * d;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < NU; ++i) {
+          wl[i] = at.w * bspline<T, NU>(sc, i, at.x);
+          wl[NU + i] = bspline<T, NU>(sc, i, at.y);
+          wl[2 * NU + i] = bspline<T, NU>(sc, i, at.z);
+        }
       }
     }
     __syncwarp();
@@ -361,18 +404,38 @@ k_anterp_tiles(int M0, int M1, int M2, int nt1, int nt2, const V4<T> *__restrict
           wa[a + 1] = v.y;
         }
       }
+      T wx[DIP ? NU : 1];
+      if constexpr (DIP) {
+#pragma unroll
+        for (int a = 0; a < NU; ++a) wx[a] = wj[NU + a];
+      }
 #pragma unroll
       for (int f = 0; f < G::FP; ++f) {
         const T wyz = wj[pwb[f]] * wj[pwc[f]];
         T *ap = acc + (bj - poff[f]);
+        if constexpr (DIP) {
+          // pwb - OY = b, pwc - OZ = c
+          const T u = wj[pwc[f]] * wj[4 * NU + pwb[f] - OY] +
+                      wj[pwb[f]] * wj[5 * NU + pwc[f] - OZ];
 #pragma unroll
-        for (int a = 0; a < NU; ++a) ap[-a * E * E] = fma(wyz, wa[a], ap[-a * E * E]);
+          for (int a = 0; a < NU; ++a)
+            ap[-a * E * E] = fma(wyz, wa[a], fma(u, wx[a], ap[-a * E * E]));
+        } else {
+#pragma unroll
+          for (int a = 0; a < NU; ++a) ap[-a * E * E] = fma(wyz, wa[a], ap[-a * E * E]);
+        }
       }
 #pragma unroll
       for (int r = 0; r < G::RR; ++r) {
         if (roff[r] >= 0) {
           T *ap = acc + (bj - roff[r]);
-          *ap = fma(wj[rb[r]] * wj[rc[r]], wj[ra[r]], *ap);
+          if constexpr (DIP) {
+            const T wyz = wj[rb[r]] * wj[rc[r]];
+            const T u = wj[rc[r]] * wj[4 * NU + rb[r] - OY] + wj[rb[r]] * wj[5 * NU + rc[r] - OZ];
+            *ap = fma(wyz, wj[ra[r]], fma(u, wj[NU + ra[r]], *ap));
+          } else {
+            *ap = fma(wj[rb[r]] * wj[rc[r]], wj[ra[r]], *ap);
+          }
         }
       }
       __syncwarp();
@@ -471,6 +534,101 @@ k_interpolate(int N, int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
   r.z = (T)(g.Ai[2] * gxv + g.Ai[5] * gyv + g.Ai[8] * gzv);
   r.w = phi + ec;
   out[k] = r;
+}
+
+// Adjoint interpolation, per atom (grid-sorted order): the value psi and
+// the Cartesian gradient G of the interpolated dipole potential ed, and the
+// Hessian of the interpolated charge potential e1 applied to the force
+// cotangent: Hess F^ = A^-T D H_u D A^-1 F^ (D = diag(M), H_u the second
+// derivatives in grid units, from second-derivative B-splines). All sums run
+// about the home grid value (derivative weights sum to zero).
+// out_g = (G, psi), out_h = (Hess F^, 0).
+template <typename T, int NU>
+__global__ void __launch_bounds__(kThreads)
+k_adj_interp(int N, int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
+             const int *__restrict__ cell, const int *__restrict__ gperm,
+             const double *__restrict__ fbar, const T *__restrict__ ed,
+             const T *__restrict__ e1, SplineConsts<T> sc, Geometry g,
+             V4<T> *__restrict__ out_g, V4<T> *__restrict__ out_h) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  const V4<T> at = atoms[k];
+  const int c = cell[k];
+  const int mz = c % M2, my = (c / M2) % M1, mx = c / (M1 * M2);
+  T wx[NU], dx[NU], hx[NU], wy[NU], dy[NU], hy[NU], wz[NU], dz[NU], hz[NU];
+#pragma unroll
+  for (int i = 0; i < NU; ++i) {
+    wx[i] = bspline_d2<T, NU>(sc, i, at.x, dx[i], hx[i]);
+    wy[i] = bspline_d2<T, NU>(sc, i, at.y, dy[i], hy[i]);
+    wz[i] = bspline_d2<T, NU>(sc, i, at.z, dz[i], hz[i]);
+  }
+  int zi[NU];
+#pragma unroll
+  for (int i = 0; i < NU; ++i) zi[i] = pwrap(mz - (i - NU / 2), M2);
+  const long home = ((long)mx * M1 + my) * M2 + mz;
+  const T cd = ed[home], c1 = e1[home];
+  T p = 0, gx = 0, gy = 0, gz = 0;                       // ed: value, grad_u
+  T hxx = 0, hyy = 0, hzz = 0, hxy = 0, hxz = 0, hyz = 0;  // e1: H_u
+  for (int a = 0; a < NU; ++a) {
+    const int ix = pwrap(mx - (a - NU / 2), M0);
+    T t00 = 0, t10 = 0, t01 = 0;                 // ed
+    T u00 = 0, u10 = 0, u01 = 0, u20 = 0, u11 = 0, u02 = 0;  // e1
+    for (int b = 0; b < NU; ++b) {
+      const int iy = pwrap(my - (b - NU / 2), M1);
+      const long row = ((long)ix * M1 + iy) * M2;
+      T s0 = 0, s1 = 0, r0 = 0, r1 = 0, r2 = 0;
+#pragma unroll
+      for (int i = 0; i < NU; ++i) {
+        const T vd = ed[row + zi[i]] - cd, v1 = e1[row + zi[i]] - c1;
+        s0 += wz[i] * vd;
+        s1 += dz[i] * vd;
+        r0 += wz[i] * v1;
+        r1 += dz[i] * v1;
+        r2 += hz[i] * v1;
+      }
+      t00 += wy[b] * s0;
+      t10 += dy[b] * s0;
+      t01 += wy[b] * s1;
+      u00 += wy[b] * r0;
+      u10 += dy[b] * r0;
+      u01 += wy[b] * r1;
+      u20 += hy[b] * r0;
+      u11 += dy[b] * r1;
+      u02 += wy[b] * r2;
+    }
+    p += wx[a] * t00;
+    gx += dx[a] * t00;
+    gy += wx[a] * t10;
+    gz += wx[a] * t01;
+    hxx += hx[a] * u00;
+    hyy += wx[a] * u20;
+    hzz += wx[a] * u02;
+    hxy += dx[a] * u10;
+    hxz += dx[a] * u01;
+    hyz += wx[a] * u11;
+  }
+  // grid-unit derivatives to Cartesian
+  const double Mv[3] = {(double)M0, (double)M1, (double)M2};
+  const double gu[3] = {(double)gx * Mv[0], (double)gy * Mv[1], (double)gz * Mv[2]};
+  const int i = gperm[k];
+  const double fb[3] = {fbar[3 * i], fbar[3 * i + 1], fbar[3 * i + 2]};
+  double v[3];  // D A^-1 F^
+  for (int q = 0; q < 3; ++q)
+    v[q] = Mv[q] * (g.Ai[3 * q] * fb[0] + g.Ai[3 * q + 1] * fb[1] + g.Ai[3 * q + 2] * fb[2]);
+  const double H[3][3] = {{hxx, hxy, hxz}, {hxy, hyy, hyz}, {hxz, hyz, hzz}};
+  double hv[3];  // D H_u v
+  for (int q = 0; q < 3; ++q) hv[q] = Mv[q] * (H[q][0] * v[0] + H[q][1] * v[1] + H[q][2] * v[2]);
+  V4<T> og, oh;
+  og.x = (T)(g.Ai[0] * gu[0] + g.Ai[3] * gu[1] + g.Ai[6] * gu[2]);
+  og.y = (T)(g.Ai[1] * gu[0] + g.Ai[4] * gu[1] + g.Ai[7] * gu[2]);
+  og.z = (T)(g.Ai[2] * gu[0] + g.Ai[5] * gu[1] + g.Ai[8] * gu[2]);
+  og.w = p + cd;
+  oh.x = (T)(g.Ai[0] * hv[0] + g.Ai[3] * hv[1] + g.Ai[6] * hv[2]);
+  oh.y = (T)(g.Ai[1] * hv[0] + g.Ai[4] * hv[1] + g.Ai[7] * hv[2]);
+  oh.z = (T)(g.Ai[2] * hv[0] + g.Ai[5] * hv[1] + g.Ai[8] * hv[2]);
+  oh.w = T(0);
+  out_g[k] = og;
+  out_h[k] = oh;
 }
 
 struct TwoScale {
@@ -657,10 +815,10 @@ void launch_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
               nt2 = (M[2] + kAT - 1) / kAT;
     const int ntiles = nt0 * nt1 * nt2;
     const long n = (long)M[0] * M[1] * M[2];
-    MSM_NU_SWITCH(sc.nu, (k_anterp_tiles<T, NU><<<ntiles, 32,
-                                                  TileGeom<NU>::E3 * sizeof(T), s>>>(
+    MSM_NU_SWITCH(sc.nu, (k_anterp_tiles<T, NU, false><<<ntiles, 32,
+                                                         TileGeom<NU>::E3 * sizeof(T), s>>>(
                              M[0], M[1], M[2], nt1, nt2, atoms, cell_sorted, cell_start,
-                             sc, scratch)));
+                             sc, scratch, nullptr)));
     MSM_NU_SWITCH(sc.nu, (k_anterp_fold<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
                              M[0], M[1], M[2], nt1, nt2, fold_tab, scratch, grid)));
     return;
@@ -686,10 +844,39 @@ void anterpolate_prepare() {
   MSM_NU_SWITCH_ALL(cudaFuncSetAttribute(k_anterpolate_slab<T, NU, kAnterpBX>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          kAnterpSmemBudget));
-  MSM_NU_SWITCH_ALL(cudaFuncSetAttribute(k_anterp_tiles<T, NU>,
+  MSM_NU_SWITCH_ALL(cudaFuncSetAttribute(k_anterp_tiles<T, NU, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(TileGeom<NU>::E3 * sizeof(T))));
+  MSM_NU_SWITCH_ALL(cudaFuncSetAttribute(k_anterp_tiles<T, NU, true>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(TileGeom<NU>::E3 * sizeof(T))));
   done = true;
+}
+
+template <typename T>
+void launch_adj_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
+                            const int *cell_sorted, const int *cell_start,
+                            const SplineConsts<T> &sc, const V4<T> *dip, T *grid,
+                            T *scratch, const int *fold_tab) {
+  const int nt0 = (M[0] + kAT - 1) / kAT, nt1 = (M[1] + kAT - 1) / kAT,
+            nt2 = (M[2] + kAT - 1) / kAT;
+  const long n = (long)M[0] * M[1] * M[2];
+  MSM_NU_SWITCH(sc.nu, (k_anterp_tiles<T, NU, true><<<nt0 * nt1 * nt2, 32,
+                                                      TileGeom<NU>::E3 * sizeof(T), s>>>(
+                           M[0], M[1], M[2], nt1, nt2, atoms, cell_sorted, cell_start, sc,
+                           scratch, dip)));
+  MSM_NU_SWITCH(sc.nu, (k_anterp_fold<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
+                           M[0], M[1], M[2], nt1, nt2, fold_tab, scratch, grid)));
+}
+
+template <typename T>
+void launch_adj_interpolate(cudaStream_t s, int N, const int M[3], const V4<T> *atoms,
+                            const int *cell_sorted, const int *gperm, const double *fbar,
+                            const T *ed, const T *e1, const SplineConsts<T> &sc,
+                            const Geometry &g, V4<T> *out_g, V4<T> *out_h) {
+  MSM_NU_SWITCH(sc.nu, (k_adj_interp<T, NU><<<blocks_for(N), kThreads, 0, s>>>(
+                           N, M[0], M[1], M[2], atoms, cell_sorted, gperm, fbar, ed, e1, sc,
+                           g, out_g, out_h)));
 }
 
 template <typename T>
@@ -737,6 +924,15 @@ void launch_grid_dot(cudaStream_t s, size_t n, const T *a, const T *b,
                                       const SplineConsts<T> &, T *, int,      \
                                       int *, long, T *, const int *);         \
   template void anterpolate_prepare<T>();                                     \
+  template void launch_adj_anterpolate<T>(cudaStream_t, const int *, const V4<T> *,  \
+                                          const int *, const int *,                 \
+                                          const SplineConsts<T> &, const V4<T> *, T *, \
+                                          T *, const int *);                        \
+  template void launch_adj_interpolate<T>(cudaStream_t, int, const int *,           \
+                                          const V4<T> *, const int *, const int *,  \
+                                          const double *, const T *, const T *,     \
+                                          const SplineConsts<T> &, const Geometry &, \
+                                          V4<T> *, V4<T> *);                        \
   template void launch_interpolate<T>(cudaStream_t, int, const int *,         \
                                       const V4<T> *, const int *, const T *,  \
                                       const SplineConsts<T> &,                \

@@ -254,6 +254,44 @@ void launch_stencil(cudaStream_t s, const StencilShape &sh,
                     const StencilTile &tile, const T *padded, const T *kh,
                     int khz, T weight, T *e, T *part);
 
+// ---- adjoint (k_adjoint.cu, k_grid.cu) ----
+struct AdjointCombineArgs {
+  int N;
+  double w0, coeff1, coeff2, gamma0_over_a0;
+  const double *q;       // input order
+  const double *qstats;  // [qsum, q2sum]
+  const double *fbar;    // force cotangent, N*3, input order
+  double ubar;           // energy cotangent
+  double *dq;            // N or null
+  double *dr;            // N*3 or null
+};
+template <typename T>
+void launch_adj_gather(cudaStream_t s, int N, const int *perm, const double *fbar, V4<T> *out);
+template <typename T>
+void launch_adj_dipoles(cudaStream_t s, int N, const int *perm, const double *q,
+                        const double *fbar, const Geometry &g, V4<T> *out);
+template <typename T>
+void launch_adj_pair(cudaStream_t s, int N, const V4<T> *ps, const V4<T> *fbs, const int *pcs,
+                     const int *start, const Geometry &g, const CellOffset<T> *off, int noff,
+                     const PairConsts<T> &pc, V4<T> *out_a, V4<T> *out_b);
+template <typename T>
+void launch_adj_combine(cudaStream_t s, const AdjointCombineArgs &a, const int *pinv,
+                        const int *ginv, const V4<T> *pout, const V4<T> *gout,
+                        const V4<T> *adj_a, const V4<T> *adj_b, const V4<T> *adj_g,
+                        const V4<T> *adj_h);
+// dipole anterpolation (tile scatter; grids >= nu per axis) and the adjoint
+// interpolation (value and gradient of ed, Hessian of e1 times Fbar)
+template <typename T>
+void launch_adj_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
+                            const int *cell_sorted, const int *cell_start,
+                            const SplineConsts<T> &sc, const V4<T> *dip, T *grid,
+                            T *scratch, const int *fold_tab);
+template <typename T>
+void launch_adj_interpolate(cudaStream_t s, int N, const int M[3], const V4<T> *atoms,
+                            const int *cell_sorted, const int *gperm, const double *fbar,
+                            const T *ed, const T *e1, const SplineConsts<T> &sc,
+                            const Geometry &g, V4<T> *out_g, V4<T> *out_h);
+
 // ---- level stencils on the device for a new box (k_setup.cu) ----
 struct LevelStencilArgs {
   double A[9];      // row-major; columns are the box edge vectors

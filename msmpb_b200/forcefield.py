@@ -164,6 +164,23 @@ class ForceField:
         if st != L.OK:
             raise MSMError(st, "FF_energy_device")
 
+    def adjoint_device(self, pos_ptr, q_ptr, fbar_ptr, ubar=0.0, dq_ptr=0, dr_ptr=0,
+                       reuse=False, stream=0, weights=None):
+        """FF_adjoint_device: charge and position gradients of
+        ubar U + sum Fbar . F (device pointers as ints; outputs in input
+        order). reuse: the last evaluation had these inputs and weights."""
+        w = None if weights is None else _f64(weights)
+        st = self._lib.FF_adjoint_device(
+            self.ff, C.c_void_p(pos_ptr), C.c_void_p(q_ptr), _ptr(w) if w is not None else None,
+            C.c_void_p(fbar_ptr), float(ubar), C.c_void_p(dq_ptr) if dq_ptr else None,
+            C.c_void_p(dr_ptr) if dr_ptr else None, 1 if reuse else 0,
+            C.c_void_p(stream) if stream else None)
+        if st != L.OK:
+            raise MSMError(st, "FF_adjoint_device")
+
+    def evaluation_count(self):
+        return int(self._lib.FF_evaluation_count(self.ff))
+
     def sync(self):
         st = self._lib.FF_sync(self.ff)
         if st != L.OK:
