@@ -269,6 +269,42 @@ def pair_roofline(ff, phases, lev, peak):
     }
 
 
+def adjoint_timing(ff, pos_d, q_d, f_d, phi_d, e_d, torch, flush, forward_ms, reps=10):
+    """FF_adjoint_device after the forward it linearises about (its state
+    reused), CUDA events on the stream, L2 flushed before each launch; and
+    the same with the forward recomputed inside the call."""
+    sh = torch.cuda.current_stream().cuda_stream
+    n = len(q_d)
+    fbar = torch.randn((n, 3), dtype=torch.float64, device=pos_d.device)
+    dq = torch.empty(n, dtype=torch.float64, device=pos_d.device)
+    dr = torch.empty((n, 3), dtype=torch.float64, device=pos_d.device)
+    ff.energy_device(pos_d.data_ptr(), q_d.data_ptr(), f_d.data_ptr(), phi_d.data_ptr(),
+                     e_d.data_ptr(), sh)
+    out = {}
+    for reuse in (True, False):
+        for _ in range(2):
+            ff.adjoint_device(pos_d.data_ptr(), q_d.data_ptr(), fbar.data_ptr(), 0.5,
+                              dq.data_ptr(), dr.data_ptr(), reuse=reuse, stream=sh)
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            ff.adjoint_device(pos_d.data_ptr(), q_d.data_ptr(), fbar.data_ptr(), 0.5,
+                              dq.data_ptr(), dr.data_ptr(), reuse=reuse, stream=sh)
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        key = "reusing_forward" if reuse else "with_forward"
+        out[key + "_ms"] = round(float(np.median(ts)), 4)
+    out["forward_ms"] = round(forward_ms, 4)
+    out["ratio_to_forward"] = round(out["reusing_forward_ms"] / forward_ms, 3)
+    out["note"] = ("gradients of ubar U + sum fbar . F w.r.t. charges and positions; "
+                   "the forward's grids and per-atom results reused")
+    ff.sync()
+    return out
+
+
 def box_change_timing(ff, edges, pos, pos_d, q_d, f_d, phi_d, e_d, torch, reps=5):
     """One MD step with a new box: FF_rebuild (tables on the host) or
     FF_rebuild_device (level stencils on the GPU), then one evaluation; wall
@@ -437,6 +473,9 @@ def run_ours(args):
            "ms_per_step": e2e_s * 1e3,
            "timing": "wall clock around the synchronous host call (pinned arrays)"}
 
+    # ---- adjoint (force and energy cotangents -> charge and position gradients) ----
+    adjoint = adjoint_timing(ff, pos_d, q_d, f_d, phi_d, e_d, torch, flush, ms)
+
     # ---- box change every step (constant-pressure MD) ----
     rebuild = box_change_timing(ff, edges, pos, pos_d, q_d, f_d, phi_d, e_d, torch)
 
@@ -458,6 +497,7 @@ def run_ours(args):
         "energy": {"mixed": e_mixed, "fp64": e_fp64},
         "accuracy": acc, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
         "box_change": rebuild,
+        "adjoint": adjoint,
         "gpu_launches": launches, "clocks": clocks,
     }
     if rank == 0:
