@@ -97,6 +97,48 @@ long FF_evaluation_count(const FF *ff);
  * positions are needed. Returns MSMPB_OK or an error code. */
 int FF_rebuild_device(FF *ff, double edges[3][3], void *stream);
 
+/* Batches: many independent systems evaluated by one CUDA graph launch. No
+ * counterpart in the reference (one system per FF_energy call,
+ * code/forcefield0.c:684-780).
+ *
+ * Each member is an FF handle after FF_build, on one device, each handle at
+ * most once; the handles may differ in N, box, order, levels and precision.
+ * The batch captures every member's evaluation (the launch sequence of
+ * FF_energy_device) into one graph over `branches` parallel branches, so
+ * kernels of different systems run side by side on the GPU; members are
+ * placed longest-first on the least-loaded branch. branches = 0 lets the
+ * first FF_batch_energy_device call pick the count by timing replays of
+ * candidate graphs (4, 8, 16, 32, 64 and min(n, 64)); that call synchronises
+ * `stream`. At most 64 branches. Returns NULL with *status set (may be
+ * NULL) on an invalid list (NULL or repeated handle, mixed devices:
+ * MSMPB_ERR_ARGUMENT; a handle not built: MSMPB_ERR_STATE) or a CUDA
+ * failure. The handles must outlive the batch and must not be evaluated
+ * while a batch replay that holds them runs. */
+typedef struct FFBatch FFBatch;
+FFBatch *FF_batch_new(FF *const *members, int n, int branches, int *status);
+
+/* Evaluates every member, asynchronously on `stream` (a cudaStream_t; NULL
+ * = the legacy default stream). Arrays of n device pointers, in member
+ * order, with FF_energy_device's per-system meaning: position_d[i] (N_i*3
+ * doubles), charge_d[i] (N_i); weight (host, may be NULL, as may an entry:
+ * maxLevel_i+1 doubles each), force_d and potential_d (may be NULL, as may an
+ * entry); energy_d: n doubles on the device (may be NULL). The graph is
+ * captured on the first call and again when a pointer, a weight or a
+ * member's box (FF_rebuild, FF_rebuild_device) changes; otherwise a call is
+ * one graph launch. Device-side checks are reported by FF_sync of a member.
+ * Returns MSMPB_OK or an error code (also kept for FF_batch_last_error). */
+int FF_batch_energy_device(FFBatch *batch, const double *const *position_d,
+                           const double *const *charge_d, const double *const *weight,
+                           double *const *force_d, double *const *potential_d,
+                           double *energy_d, void *stream);
+
+/* Branches of the current graph (after tuning: the chosen count), kernels
+ * it launches, the first error of the batch's calls; and release. */
+int FF_batch_branches(const FFBatch *batch);
+int FF_batch_kernel_launches(const FFBatch *batch);
+int FF_batch_last_error(const FFBatch *batch);
+void FF_batch_delete(FFBatch *batch);
+
 /* Milliseconds of each phase of the last evaluation, measured with CUDA
  * events on the evaluation stream (also copied into the reference's time_*
  * fields in seconds). Order: bin, pair, anterpolation, restriction,

@@ -40,7 +40,9 @@ EXPORTED = [
     "FF_energy_device", "FF_sync", "FF_phase_times", "FF_kernel_launches",
     "FF_stencil_times", "FF_set_timing", "msmpb_measure_fp32_tflops",
     "msmpb_level_stencil_noalloc", "FF_rebuild_device", "FF_adjoint_device",
-    "FF_evaluation_count",
+    "FF_evaluation_count", "FF_batch_new", "FF_batch_energy_device",
+    "FF_batch_branches", "FF_batch_kernel_launches", "FF_batch_last_error",
+    "FF_batch_delete",
 ]
 
 _lib = None
@@ -128,6 +130,14 @@ def load():
         "FF_stencil_times": (C.c_int, [P, _dp, C.c_int]),
         "FF_set_timing": (None, [P, C.c_int]),
         "msmpb_measure_fp32_tflops": (C.c_double, [C.c_int, C.c_int]),
+        "FF_batch_new": (C.c_void_p, [C.POINTER(P), C.c_int, C.c_int, _ip]),
+        "FF_batch_energy_device": (C.c_int, [C.c_void_p] + [C.POINTER(C.c_void_p)] * 2 +
+                                   [C.POINTER(_dp)] + [C.POINTER(C.c_void_p)] * 2 +
+                                   [C.c_void_p, C.c_void_p]),
+        "FF_batch_branches": (C.c_int, [C.c_void_p]),
+        "FF_batch_kernel_launches": (C.c_int, [C.c_void_p]),
+        "FF_batch_last_error": (C.c_int, [C.c_void_p]),
+        "FF_batch_delete": (None, [C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -32,6 +32,14 @@ struct FFDevice {
   virtual int evaluate(const msm::EvalRequest &r, double *energy) = 0;
   virtual int adjoint(const msm::AdjointRequest &r) = 0;
   virtual long evaluations() const = 0;
+  // the launch sequence of one device-pointer evaluation on s, nothing else
+  // (no waits, no host work): for capture into a caller's graph
+  virtual int enqueue_into(const msm::EvalRequest &r, cudaStream_t s) = 0;
+  // an evaluation issued outside this plan (a batch replay) is about to run
+  // on s: order it after a pending device rebuild and count it
+  virtual int begin(cudaStream_t s) = 0;
+  virtual long version() const = 0;  // bumped by every box update
+  virtual int device_index() const = 0;
   virtual int sync() = 0;
   virtual int phase_times(double *ms, int n) = 0;
   virtual int launches() = 0;
@@ -94,6 +102,18 @@ class Plan : public FFDevice {
   int evaluate(const EvalRequest &r, double *energy) override;
   int adjoint(const AdjointRequest &r) override;
   long evaluations() const override { return nevals_; }
+  int enqueue_into(const EvalRequest &r, cudaStream_t s) override {
+    return enqueue(r, s, r.pos, r.q, r.force, r.phi, r.energy_dev ? r.energy_dev : energy_);
+  }
+  int begin(cudaStream_t s) override {
+    MSM_CUDA_TRY(cudaSetDevice(device_));
+    last_stream_ = s;
+    if (rebuild_recorded_) MSM_CUDA_TRY(cudaStreamWaitEvent(s, rebuild_ev_, 0));
+    ++nevals_;
+    return MSMPB_OK;
+  }
+  long version() const override { return version_; }
+  int device_index() const override { return device_; }
   int sync() override;
   int phase_times(double *ms, int n) override;
   int launches() override { return nlaunch_; }
@@ -218,6 +238,7 @@ class Plan : public FFDevice {
   bool have_graph_ = false;
   bool graph_stale_ = false;  // kernel parameters changed (new box)
   long nevals_ = 0;           // forward evaluations so far
+  long version_ = 0;          // box updates so far
   // adjoint buffers (allocated on first use)
   void *adj_mem_ = nullptr;
   V4<T> *fbs_ = nullptr, *dip_ = nullptr, *adj_a_ = nullptr, *adj_b_ = nullptr,
@@ -630,6 +651,7 @@ int Plan<T>::update_box(const Tables &t, cudaStream_t s, bool stencils_on_device
   // geometry and constants are kernel parameters: the next graph launch
   // re-captures and updates the instantiated graph in place
   graph_stale_ = true;
+  ++version_;
   return MSMPB_OK;
 }
 
@@ -647,7 +669,7 @@ int Plan<T>::enqueue_chain(cudaStream_t s, T *const *qg, T *const *eg, const dou
   }
   mark(s, kPhaseTop, tm);
   launch_top_solve<T>(s, grid_[L_], qg[L_], khat_top_, w[L_], fft_, nullptr, eg[L_]);
-  nl += 5;
+  nl += top_solve_launches(grid_[L_]);
   for (int l = L_ - 1; l >= 1; --l) {
     mark(s, kPhaseProlong, tm && l == L_ - 1);
     cudaMemsetAsync(eg[l], 0, (size_t)grid_[l][0] * grid_[l][1] * grid_[l][2] * sizeof(T), s);
@@ -689,7 +711,7 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   launch_gather<T>(s, N_, pperm_, prel_, pcell_, psorted_, pcs_, pinv_);
   if (kMixed) launch_permute64(s, N_, pperm_, prel64_, psorted64_);
   launch_gather<T>(s, N_, gperm_, gfrac_, gcell_, gsorted_, gcs_, ginv_);
-  nl += 3 + 6 + 2 + 2 + 2;
+  nl += 3 + 6 + 2 + 2 + 2 + (kMixed ? 1 : 0);
   const bool clusters = pair_variant_ == 2 && clusters_ok_;
   if (clusters) {  // cluster build (part of the binning phase)
     const V4<double> *src64 =
@@ -1051,6 +1073,12 @@ void engine_destroy(FFDevice *d) { delete d; }
 
 int engine_update_tables(FFDevice *d, const Tables &t) { return d->update(t); }
 int engine_adjoint(FFDevice *d, const AdjointRequest &r) { return d->adjoint(r); }
+int engine_enqueue(FFDevice *d, const EvalRequest &r, cudaStream_t s) {
+  return d->enqueue_into(r, s);
+}
+int engine_begin(FFDevice *d, cudaStream_t s) { return d->begin(s); }
+long engine_version(FFDevice *d) { return d->version(); }
+int engine_device(FFDevice *d) { return d->device_index(); }
 long engine_evaluations(FFDevice *d) { return d->evaluations(); }
 int engine_update_tables_device(FFDevice *d, const Tables &t, cudaStream_t stream) {
   return d->update_device(t, stream);

@@ -65,6 +65,15 @@ struct AdjointRequest {
   cudaStream_t stream;
 };
 int engine_adjoint(FFDevice *d, const AdjointRequest &r);
+// Enqueues one device-pointer evaluation (r.pos, r.q, r.force, r.phi,
+// r.energy_dev; r.host false) on s with no waits or host work, for capture
+// into a caller's graph; engine_version changes with every box update.
+// engine_begin, outside any capture, orders such an evaluation about to run
+// on s after a pending device rebuild and counts it.
+int engine_enqueue(FFDevice *d, const EvalRequest &r, cudaStream_t s);
+int engine_begin(FFDevice *d, cudaStream_t s);
+long engine_version(FFDevice *d);
+int engine_device(FFDevice *d);
 long engine_evaluations(FFDevice *d);
 
 // Waits for outstanding work and returns device-side check flags as status.

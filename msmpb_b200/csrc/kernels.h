@@ -311,6 +311,7 @@ void launch_level_stencil(cudaStream_t s, const LevelStencilArgs &a, const doubl
 
 // ---- top-level FFT solve (k_fft.cu) ----
 bool top_solve_supported(const int M[3]);
+int top_solve_launches(const int M[3]);  // kernels one launch_top_solve issues
 void top_solve_prepare();
 template <typename T>
 void launch_top_solve(cudaStream_t s, const int M[3], const T *q,

@@ -238,3 +238,60 @@ class ForceField:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Many built ForceField handles evaluated by one CUDA graph launch
+    (FF_batch_new / FF_batch_energy_device). ``branches``: parallel branches
+    of the graph, 0 = tuned on the first evaluation."""
+
+    def __init__(self, members, branches=0):
+        self._lib = L.load()
+        self.members = list(members)
+        n = len(self.members)
+        arr = (C.POINTER(L.FFStruct) * n)(*[m.ff for m in self.members])
+        st = C.c_int(0)
+        self.b = self._lib.FF_batch_new(arr, n, int(branches), C.byref(st))
+        if not self.b:
+            raise MSMError(st.value, "FF_batch_new")
+
+    def energy_device(self, pos_ptrs, q_ptrs, force_ptrs=None, phi_ptrs=None,
+                      energy_ptr=0, stream=0, weights=None):
+        """Device pointers (ints) per member, in member order; energy_ptr:
+        one device buffer of len(members) doubles."""
+        n = len(self.members)
+        vp = lambda ps: (C.c_void_p * n)(*[p or None for p in ps]) if ps is not None else None
+        keep = []
+        w = None
+        if weights is not None:
+            w = (_dp * n)()
+            for i, wi in enumerate(weights):
+                if wi is not None:
+                    a = _f64(wi)
+                    keep.append(a)
+                    w[i] = _ptr(a)
+        st = self._lib.FF_batch_energy_device(
+            self.b, vp(pos_ptrs), vp(q_ptrs), w, vp(force_ptrs), vp(phi_ptrs),
+            C.c_void_p(energy_ptr or None), C.c_void_p(stream or None))
+        if st != L.OK:
+            raise MSMError(st, "FF_batch_energy_device")
+
+    def branches(self):
+        return self._lib.FF_batch_branches(self.b)
+
+    def kernel_launches(self):
+        return self._lib.FF_batch_kernel_launches(self.b)
+
+    def last_error(self):
+        return self._lib.FF_batch_last_error(self.b)
+
+    def close(self):
+        if getattr(self, "b", None):
+            self._lib.FF_batch_delete(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
