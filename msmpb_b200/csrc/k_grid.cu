@@ -635,65 +635,195 @@ struct TwoScale {
   double J[11];
 };
 
+// Restriction and prolongation as separable per-axis two-scale sums: a CTA
+// stages its tile plus the B-spline halo in shared memory (periodic wrap
+// applied once, at the load) and contracts z, then y, then x there, so a
+// point costs 3 (nu + 1) multiply-adds instead of (nu + 1)^3 (restriction)
+// or about (nu / 2 + 1)^3 (prolongation) wrapped loads.
+constexpr int kSepThreads = 256;
+
+// Restriction tile: CX x CY x CZ coarse points (z fastest)
+template <typename T>
+struct RestrictTile {
+  static constexpr int CX = 4, CY = 8, CZ = sizeof(T) == 4 ? 16 : 8;
+};
+template <typename T, int NU>
+struct RestrictGeom {
+  using Tl = RestrictTile<T>;
+  static constexpr int RX = 2 * Tl::CX + NU - 1, RY = 2 * Tl::CY + NU - 1,
+                       RZ = 2 * Tl::CZ + NU - 1;
+  // fine region, then the z-contracted region (RX x RY x CZ); the y pass
+  // writes RX x CY x CZ over the start of the fine region
+  static constexpr int SMEM = (RX * RY * RZ + RX * RY * Tl::CZ) * (int)sizeof(T);
+};
+
 // q^{l+1}_m = sum_n J_n q^l_{2m+n}, n in [-nu/2, nu/2]^3
 // (code/forcefield1.c:401-477)
 template <typename T, int NU>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kSepThreads)
 k_restrict(int F0, int F1, int F2, const T *__restrict__ fine,
            T *__restrict__ coarse, TwoScale js) {
+  using Tl = RestrictTile<T>;
+  using G = RestrictGeom<T, NU>;
+  constexpr int CX = Tl::CX, CY = Tl::CY, CZ = Tl::CZ, RX = G::RX, RY = G::RY, RZ = G::RZ;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *reg = reinterpret_cast<T *>(smem_raw);
+  T *t1 = reg + RX * RY * RZ;
+  T *t2 = reg;
   const int C0 = F0 / 2, C1 = F1 / 2, C2 = F2 / 2;
-  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long)C0 * C1 * C2) return;
-  const int z = idx % C2, y = (idx / C2) % C1, x = idx / ((long)C1 * C2);
+  const int nbz = (C2 + CZ - 1) / CZ, nby = (C1 + CY - 1) / CY;
+  const int bz = blockIdx.x % nbz, by = (blockIdx.x / nbz) % nby, bx = blockIdx.x / (nbz * nby);
+  const int x0 = bx * CX, y0 = by * CY, z0 = bz * CZ;
+  __shared__ int wrap[RX + RY + RZ];  // periodic indices of the region's planes, rows, columns
   T J[NU + 1];
 #pragma unroll
   for (int i = 0; i <= NU; ++i) J[i] = (T)js.J[i];
-  T acc = 0;
-  for (int a = 0; a <= NU; ++a) {
-    const int fx = pwrap(2 * x + a - NU / 2, F0);
-    T ay = 0;
-    for (int b = 0; b <= NU; ++b) {
-      const int fy = pwrap(2 * y + b - NU / 2, F1);
-      const T *row = fine + ((long)fx * F1 + fy) * F2;
-      T az = 0;
-#pragma unroll
-      for (int c = 0; c <= NU; ++c) az += J[c] * row[pwrap(2 * z + c - NU / 2, F2)];
-      ay += J[b] * az;
-    }
-    acc += J[a] * ay;
+  for (int i = threadIdx.x; i < RX + RY + RZ; i += kSepThreads)
+    wrap[i] = i < RX        ? pwrap(2 * x0 - NU / 2 + i, F0) * F1
+              : i < RX + RY ? pwrap(2 * y0 - NU / 2 + i - RX, F1)
+                            : pwrap(2 * z0 - NU / 2 + i - RX - RY, F2);
+  __syncthreads();
+#pragma unroll 4
+  for (int t = threadIdx.x; t < RX * RY * RZ; t += kSepThreads) {
+    const int rz = t % RZ, ry = (t / RZ) % RY, rx = t / (RZ * RY);
+    reg[t] = fine[(long)(wrap[rx] + wrap[RX + ry]) * F2 + wrap[RX + RY + rz]];
   }
-  coarse[idx] = acc;
+  __syncthreads();
+  for (int t = threadIdx.x; t < RX * RY * CZ; t += kSepThreads) {
+    const int cz = t % CZ, r = t / CZ;  // r = rx * RY + ry
+    const T *row = reg + r * RZ + 2 * cz;
+    T acc = 0;
+#pragma unroll
+    for (int c = 0; c <= NU; ++c) acc += J[c] * row[c];
+    t1[t] = acc;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < RX * CY * CZ; t += kSepThreads) {
+    const int cz = t % CZ, cy = (t / CZ) % CY, rx = t / (CZ * CY);
+    const T *col = t1 + (rx * RY + 2 * cy) * CZ + cz;
+    T acc = 0;
+#pragma unroll
+    for (int b = 0; b <= NU; ++b) acc += J[b] * col[b * CZ];
+    t2[t] = acc;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < CX * CY * CZ; t += kSepThreads) {
+    const int cz = t % CZ, cy = (t / CZ) % CY, cx = t / (CZ * CY);
+    const int x = x0 + cx, y = y0 + cy, z = z0 + cz;
+    if (x >= C0 || y >= C1 || z >= C2) continue;
+    const T *col = t2 + ((2 * cx) * CY + cy) * CZ + cz;
+    T acc = 0;
+#pragma unroll
+    for (int a = 0; a <= NU; ++a) acc += J[a] * col[a * CY * CZ];
+    coarse[((long)x * C1 + y) * C2 + z] = acc;
+  }
+}
+
+// Prolongation tile: FX x FY x FZ fine points; the coarse region along an
+// axis covers every m with |x - 2m| <= nu/2 for x in the tile
+constexpr int kPX = 8, kPY = 8, kPZ = 32;
+template <int NU>
+struct ProlongGeom {
+  // tile starts are even, so m runs over [x0/2 - ceil(nu/4), (x0 + F - 1 + nu/2)/2]
+  static constexpr int lo = (NU / 2 + 1) / 2;
+  static constexpr int RX = (kPX - 1 + NU / 2) / 2 + lo + 1, RY = (kPY - 1 + NU / 2) / 2 + lo + 1,
+                       RZ = (kPZ - 1 + NU / 2) / 2 + lo + 1;
+  static constexpr int N_REG = RX * RY * RZ, N_T1 = RX * RY * kPZ, N_T2 = RX * kPY * kPZ;
+};
+
+// Taps of fine index x: n = x - 2m in [-nu/2, nu/2] with the parity of
+// x + nu/2, i.e. n = -nu/2 + p + 2k, p = (x + nu/2) & 1, k = 0.. (nu/2 - p);
+// weights picked by compile-time k so J stays in registers.
+template <int NU>
+__device__ __forceinline__ bool tap_live(int x, int k) {
+  return k < NU / 2 || ((x + NU / 2) & 1) == 0;
+}
+template <typename T, int NU>
+__device__ __forceinline__ T tap_weight(const T (&J)[NU + 1], int x, int k) {
+  const int p = (x + NU / 2) & 1;
+  return (p && 2 * k + 1 <= NU) ? J[2 * k + 1 <= NU ? 2 * k + 1 : NU] : J[2 * k];
+}
+// coarse index m = (x - n) / 2 (x - n is even)
+template <int NU>
+__device__ __forceinline__ int tap_coarse(int x, int k) {
+  return (x + NU / 2 - ((x + NU / 2) & 1) - 2 * k) >> 1;
 }
 
 // e^l_x += sum over (m, n) with 2m + n = x (mod M) of J_n e^{l+1}_m
 // (transpose of the restriction; code/forcefield1.c:530-567)
 template <typename T, int NU>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kSepThreads)
 k_prolong(int F0, int F1, int F2, const T *__restrict__ coarse,
           T *__restrict__ fine, TwoScale js) {
+  using G = ProlongGeom<NU>;
+  constexpr int RX = G::RX, RY = G::RY, RZ = G::RZ, lo = G::lo;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *reg = reinterpret_cast<T *>(smem_raw);
+  T *t1 = reg + G::N_REG;
+  T *t2 = t1 + G::N_T1;
   const int C0 = F0 / 2, C1 = F1 / 2, C2 = F2 / 2;
-  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long)F0 * F1 * F2) return;
-  const int z = idx % F2, y = (idx / F2) % F1, x = idx / ((long)F1 * F2);
-  // tap n = x - 2m in [-NU/2, NU/2]: the first n with the parity of x
-  const int nx0 = -NU / 2 + ((x + NU / 2) & 1);
-  const int ny0 = -NU / 2 + ((y + NU / 2) & 1);
-  const int nz0 = -NU / 2 + ((z + NU / 2) & 1);
-  T acc = 0;
-  for (int n = nx0; n <= NU / 2; n += 2) {
-    const int cx = pwrap((x - n) >> 1, C0);
-    T ay = 0;
-    for (int nb = ny0; nb <= NU / 2; nb += 2) {
-      const int cy = pwrap((y - nb) >> 1, C1);
-      const T *row = coarse + ((long)cx * C1 + cy) * C2;
-      T az = 0;
-      for (int nc = nz0; nc <= NU / 2; nc += 2)
-        az += (T)js.J[nc + NU / 2] * row[pwrap((z - nc) >> 1, C2)];
-      ay += (T)js.J[nb + NU / 2] * az;
-    }
-    acc += (T)js.J[n + NU / 2] * ay;
+  const int nbz = (F2 + kPZ - 1) / kPZ, nby = (F1 + kPY - 1) / kPY;
+  const int bz = blockIdx.x % nbz, by = (blockIdx.x / nbz) % nby, bx = blockIdx.x / (nbz * nby);
+  const int x0 = bx * kPX, y0 = by * kPY, z0 = bz * kPZ;
+  // coarse region origin along each axis
+  const int mx0 = x0 / 2 - lo, my0 = y0 / 2 - lo, mz0 = z0 / 2 - lo;
+  __shared__ int wrap[RX + RY + RZ];
+  T J[NU + 1];
+#pragma unroll
+  for (int i = 0; i <= NU; ++i) J[i] = (T)js.J[i];
+  for (int i = threadIdx.x; i < RX + RY + RZ; i += kSepThreads)
+    wrap[i] = i < RX        ? pwrap(mx0 + i, C0) * C1
+              : i < RX + RY ? pwrap(my0 + i - RX, C1)
+                            : pwrap(mz0 + i - RX - RY, C2);
+  __syncthreads();
+#pragma unroll 4
+  for (int t = threadIdx.x; t < G::N_REG; t += kSepThreads) {
+    const int rz = t % RZ, ry = (t / RZ) % RY, rx = t / (RZ * RY);
+    reg[t] = coarse[(long)(wrap[rx] + wrap[RX + ry]) * C2 + wrap[RX + RY + rz]];
   }
-  fine[idx] += acc;
+  __syncthreads();
+  // z: t1[rx][ry][fz] = sum_n J_n reg[rx][ry][(z - n)/2 - mz0], n = z (mod 2)
+  for (int t = threadIdx.x; t < G::N_T1; t += kSepThreads) {
+    const int fz = t % kPZ, r = t / kPZ;
+    const int z = z0 + fz;
+    const T *row = reg + r * RZ - mz0;
+    T acc = 0;
+#pragma unroll
+    for (int k = 0; k <= NU / 2; ++k)
+      if (tap_live<NU>(z, k)) acc += tap_weight<T, NU>(J, z, k) * row[tap_coarse<NU>(z, k)];
+    t1[t] = acc;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < G::N_T2; t += kSepThreads) {
+    const int fz = t % kPZ, fy = (t / kPZ) % kPY, rx = t / (kPZ * kPY);
+    const int y = y0 + fy;
+    const T *col = t1 + rx * RY * kPZ + fz;
+    T acc = 0;
+#pragma unroll
+    for (int k = 0; k <= NU / 2; ++k)
+      if (tap_live<NU>(y, k))
+        acc += tap_weight<T, NU>(J, y, k) * col[(tap_coarse<NU>(y, k) - my0) * kPZ];
+    t2[t] = acc;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kPX * kPY * kPZ; t += kSepThreads) {
+    const int fz = t % kPZ, fy = (t / kPZ) % kPY, fx = t / (kPZ * kPY);
+    const int x = x0 + fx, y = y0 + fy, z = z0 + fz;
+    if (x >= F0 || y >= F1 || z >= F2) continue;
+    const T *col = t2 + fy * kPZ + fz;
+    T acc = 0;
+#pragma unroll
+    for (int k = 0; k <= NU / 2; ++k)
+      if (tap_live<NU>(x, k))
+        acc += tap_weight<T, NU>(J, x, k) * col[(tap_coarse<NU>(x, k) - mx0) * kPY * kPZ];
+    fine[((long)x * F1 + y) * F2 + z] += acc;
+  }
+}
+
+template <typename T, int NU>
+constexpr int prolong_smem() {
+  return (ProlongGeom<NU>::N_REG + ProlongGeom<NU>::N_T1 + ProlongGeom<NU>::N_T2) *
+         (int)sizeof(T);
 }
 
 template <typename T>
@@ -850,6 +980,12 @@ void anterpolate_prepare() {
   MSM_NU_SWITCH_ALL(cudaFuncSetAttribute(k_anterp_tiles<T, NU, true>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(TileGeom<NU>::E3 * sizeof(T))));
+  MSM_NU_SWITCH_ALL(cudaFuncSetAttribute(k_restrict<T, NU>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         RestrictGeom<T, NU>::SMEM));
+  MSM_NU_SWITCH_ALL(cudaFuncSetAttribute(k_prolong<T, NU>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (prolong_smem<T, NU>())));
   done = true;
 }
 
@@ -893,8 +1029,11 @@ void launch_restrict(cudaStream_t s, const int Mf[3], const T *fine,
                      T *coarse, const double *J, int nu) {
   TwoScale js;
   for (int i = 0; i <= nu; ++i) js.J[i] = J[i];
-  long n = (long)(Mf[0] / 2) * (Mf[1] / 2) * (Mf[2] / 2);
-  MSM_NU_SWITCH(nu, (k_restrict<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
+  using Tl = RestrictTile<T>;
+  const int C0 = Mf[0] / 2, C1 = Mf[1] / 2, C2 = Mf[2] / 2;
+  const int blocks = ((C0 + Tl::CX - 1) / Tl::CX) * ((C1 + Tl::CY - 1) / Tl::CY) *
+                     ((C2 + Tl::CZ - 1) / Tl::CZ);
+  MSM_NU_SWITCH(nu, (k_restrict<T, NU><<<blocks, kSepThreads, RestrictGeom<T, NU>::SMEM, s>>>(
                         Mf[0], Mf[1], Mf[2], fine, coarse, js)));
 }
 
@@ -903,8 +1042,9 @@ void launch_prolong_add(cudaStream_t s, const int Mf[3], const T *coarse,
                         T *fine, const double *J, int nu) {
   TwoScale js;
   for (int i = 0; i <= nu; ++i) js.J[i] = J[i];
-  long n = (long)Mf[0] * Mf[1] * Mf[2];
-  MSM_NU_SWITCH(nu, (k_prolong<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
+  const int blocks = ((Mf[0] + kPX - 1) / kPX) * ((Mf[1] + kPY - 1) / kPY) *
+                     ((Mf[2] + kPZ - 1) / kPZ);
+  MSM_NU_SWITCH(nu, (k_prolong<T, NU><<<blocks, kSepThreads, prolong_smem<T, NU>(), s>>>(
                         Mf[0], Mf[1], Mf[2], coarse, fine, js)));
 }
 

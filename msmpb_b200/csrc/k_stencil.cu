@@ -48,15 +48,18 @@ __host__ __device__ inline int slice_pitch(int nz, int R, int S, int V) {
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_pad(StencilShape sh, const T *__restrict__ q, T *__restrict__ p) {
-  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long n = (long)sh.P[0] * sh.P[1] * sh.P[2];
-  if (idx >= n) return;
-  const int c = idx % sh.P[2], b = (idx / sh.P[2]) % sh.P[1],
-            a = idx / ((long)sh.P[1] * sh.P[2]);
+  // one padded row (a, b) per blockIdx.(z, y); threads along it
+  const int a = blockIdx.z, b = blockIdx.y;
   const int x = pwrap(a - sh.S[0] / 2, sh.M[0]);
   const int y = pwrap(b - sh.S[1] / 2, sh.M[1]);
-  const int z = pwrap(c - sh.S[2] / 2, sh.M[2]);
-  p[idx] = q[((long)x * sh.M[1] + y) * sh.M[2] + z];
+  const T *src = q + ((long)x * sh.M[1] + y) * sh.M[2];
+  T *dst = p + ((long)a * sh.P[1] + b) * sh.P[2];
+  const int h = sh.S[2] / 2, M2 = sh.M[2];
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < sh.P[2]; c += gridDim.x * blockDim.x) {
+    int z = c - h;
+    if (z < 0 || z >= M2) z = pwrap(z, M2);
+    dst[c] = src[z];
+  }
 }
 
 // Reference-form sweep: one output per thread, all loops at run time.
@@ -613,8 +616,8 @@ bool stencil_fold_taps(const double *kh, const int S[3], bool fp64,
 
 template <typename T>
 void launch_pad(cudaStream_t s, const StencilShape &sh, const T *q, T *p) {
-  long n = (long)sh.P[0] * sh.P[1] * sh.P[2];
-  k_pad<T><<<blocks_for(n), kThreads, 0, s>>>(sh, q, p);
+  const dim3 grid((sh.P[2] + kThreads - 1) / kThreads, sh.P[1], sh.P[0]);
+  k_pad<T><<<grid, kThreads, 0, s>>>(sh, q, p);
 }
 
 template <typename T>
