@@ -193,6 +193,7 @@ class Plan : public FFDevice {
   int ncp_ = 0, ncg_ = 0, noff_ = 0;
   int ncol_ = 0, maxcl_ = 0, ncoloff_ = 0, K2_ = 0;
   bool clusters_ok_ = false;
+  bool self_images_ = false;  // a lattice vector shorter than a0
   double cz_[3] = {};
   int nq_ = 0, ncomb_ = 0, ngrid_ = 0;
   std::vector<CellOffset<T>> offsets_;
@@ -525,6 +526,26 @@ int Plan<T>::update_box(const Tables &t, cudaStream_t s, bool stencils_on_device
   coeff1_ = t.coeff1;
   coeff2_ = t.coeff2;
   gamma0_a0_ = t.gamma0 / p.a0;
+  // an atom's own periodic images within a0 (the lattice vectors the
+  // constant coeff1 sums, code/forcefield0.c:612-636)
+  self_images_ = false;
+  {
+    int lim[3];
+    for (int k = 0; k < 3; ++k)
+      lim[k] = (int)std::ceil(p.a0 * std::sqrt(p.Ai[k][0] * p.Ai[k][0] + p.Ai[k][1] * p.Ai[k][1] +
+                                               p.Ai[k][2] * p.Ai[k][2]) - 1.);
+    for (int x = -lim[0]; x <= lim[0] && !self_images_; ++x)
+      for (int y = -lim[1]; y <= lim[1] && !self_images_; ++y)
+        for (int z = -lim[2]; z <= lim[2] && !self_images_; ++z) {
+          if (x == 0 && y == 0 && z == 0) continue;
+          double r2 = 0;
+          for (int k = 0; k < 3; ++k) {
+            const double rk = p.A[k][0] * x + p.A[k][1] * y + p.A[k][2] * z;
+            r2 += rk * rk;
+          }
+          self_images_ = r2 < p.a0 * p.a0;
+        }
+  }
   // neighbour-cell instances: every offset d with |d_k| <= ceil(a0|a*_k| nc_k)
   bool ortho = true;
   for (int r = 0; r < 3; ++r)
@@ -743,6 +764,7 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
     ca.cpos64 = cpos64_;
     ca.out = pout_;
     ca.err = err_d_;
+    ca.self_images = self_images_ ? 1 : 0;
     launch_pair_clusters<T>(s, ca, pc_);
     nl += 1 + 3 + 1;
   } else if (pair_variant_ == 0 && pair_cells_supported(noff_, N_)) {

@@ -89,7 +89,7 @@ k_adj_pair(int N, const V4<T> *__restrict__ ps, const V4<T> *__restrict__ fbs,
       const V4<T> aj = ps[j];
       const T dx = aj.x + sx, dy = aj.y + sy, dz = aj.z + sz;
       const T r2 = dx * dx + dy * dy + dz * dz;
-      if (r2 < pc.a02 && (j != k || r2 != T(0))) {
+      if (r2 < pc.a02 && j != k) {  // never the atom itself, at any image
         const T s = r2 * pc.inv_a02 - T(1);
         T p0 = pc.tau[NU - 1], p1 = T(0), p2 = T(0);
 #pragma unroll

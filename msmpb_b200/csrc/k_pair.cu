@@ -62,9 +62,9 @@ k_pair(int N, const V4<T> *__restrict__ ps, const V4<double> *__restrict__ ps64,
       const V4<T> aj = ps[j];
       const T dx = aj.x + sx, dy = aj.y + sy, dz = aj.z + sz;
       const T r2 = dx * dx + dy * dy + dz * dz;
-      // the atom itself (zero shift) is the only pair at r2 == 0; its
-      // periodic images are pairs like any other
-      if (r2 < pc.a02 && (j != k || r2 != T(0))) {
+      // the atom itself is skipped at every image: the reference pairs no
+      // atom with itself and sums its own images in the constant coeff1
+      if (r2 < pc.a02 && j != k) {
         if (CLOSE && r2 < pc.close2 && nclose < kCloseList) {
           close_j[nclose] = j;
           close_o[nclose] = o;

@@ -188,8 +188,12 @@ __device__ __forceinline__ void close_pair64(const PairConsts<float> &pc,
 // One 8 x 4 tile: lane (ii, jq) takes pair (i-atom ii, j-atom jq of the
 // queued unit, already shifted into the i-cluster's frame). Close pairs
 // (mixed form) are recorded for the FP64 pass while the lane's record has
-// room, else summed here in FP32.
-template <typename T, int NU, bool MIXED>
+// room, else summed here in FP32. The atom itself is never a pair: the
+// reference sums an atom's own periodic images in the constant coeff1
+// (code/forcefield0.c:612-636). SELF: the box has a lattice vector shorter
+// than a0, so the atom's images can reach the tile and every pair checks
+// its slot; otherwise only the zero-shift atom (r2 == 0) can be itself.
+template <typename T, int NU, bool MIXED, bool SELF>
 __device__ __forceinline__ void tile(const PairConsts<T> &pc, const V4<T> &ai,
                                      const V4<T> &aj, const int *qunit, int e, int jq,
                                      int islot, const int *qcode, int2 *closeq,
@@ -197,8 +201,7 @@ __device__ __forceinline__ void tile(const PairConsts<T> &pc, const V4<T> &ai,
   const T dx = aj.x - ai.x, dy = aj.y - ai.y, dz = aj.z - ai.z;
   const T r2 = dx * dx + dy * dy + dz * dz;
   if (r2 < pc.a02) {
-    // the atom itself (same slot, zero shift) is the only pair at r2 == 0
-    if (r2 == T(0) && qunit[e] * 4 + jq == islot) return;
+    if ((SELF || r2 == T(0)) && qunit[e] * 4 + jq == islot) return;
     if constexpr (MIXED) {
       if (r2 < pc.close2 && nclose < kCloseCap) {
         closeq[nclose++] = make_int2(qunit[e] * 4 + jq, qcode[e]);
@@ -220,7 +223,7 @@ __device__ __forceinline__ void tile(const PairConsts<T> &pc, const V4<T> &ai,
 // x_e+1, y_e, y_e+1), Y = (z_e, z_e+1, q_e, q_e+1). Pairs beyond the cutoff
 // contribute exactly zero (their charge is masked, their r^2 replaced by a
 // safe value); close pairs and the atom itself go the scalar way.
-template <int NU>
+template <int NU, bool SELF>
 __device__ __forceinline__ void tile2(const PairConsts<float> &pc, const V4<float> &ai,
                                       const float4 &X, const float4 &Y, const int *qunit,
                                       int e, int jq, int islot, const int *qcode,
@@ -235,6 +238,10 @@ __device__ __forceinline__ void tile2(const PairConsts<float> &pc, const V4<floa
   r2 = __ffma2_rn(dy, dy, r2);
   r2 = __ffma2_rn(dz, dz, r2);
   bool h0 = r2.x < pc.a02, h1 = r2.y < pc.a02;
+  if constexpr (SELF) {
+    if (h0 && qunit[e] * 4 + jq == islot) h0 = false;
+    if (h1 && qunit[e + 1] * 4 + jq == islot) h1 = false;
+  }
   if (!(h0 || h1)) return;
   // the atom itself is skipped; close pairs are recorded for the FP64 pass
   // while there is room (else they stay here, in FP32)
@@ -272,7 +279,7 @@ __device__ __forceinline__ void tile2(const PairConsts<float> &pc, const V4<floa
   pz = __ffma2_rn(fs, dz, pz);
 }
 
-template <typename T, int NU, bool MIXED>
+template <typename T, int NU, bool MIXED, bool SELF>
 __global__ void __launch_bounds__(kWarps * 32)
 k_pair_clusters(PairClusterArgs<T> a, PairConsts<T> pc) {
   // passing units of the current batch: their 4 atoms shifted into the
@@ -406,7 +413,8 @@ k_pair_clusters(PairClusterArgs<T> a, PairConsts<T> pc) {
         for (; e + 2 <= nq; e += 2) {
           const float4 X = *reinterpret_cast<const float4 *>(&qpk[warp][e >> 1][8 * jq]);
           const float4 Y = *reinterpret_cast<const float4 *>(&qpk[warp][e >> 1][8 * jq + 4]);
-          tile2<NU>(pc, ai, X, Y, qu, e, jq, islot, qc, myclose, nclose, px2, py2, pz2, pp2);
+          tile2<NU, SELF>(pc, ai, X, Y, qu, e, jq, islot, qc, myclose, nclose, px2, py2, pz2,
+                          pp2);
         }
         px = px2.x + px2.y;
         py = py2.x + py2.y;
@@ -419,19 +427,19 @@ k_pair_clusters(PairClusterArgs<T> a, PairConsts<T> pc) {
           aj.y = d[2];
           aj.z = d[4];
           aj.w = d[6];
-          tile<T, NU, MIXED>(pc, ai, aj, qu, e, jq, islot, qc, myclose, nclose, px, py, pz,
+          tile<T, NU, MIXED, SELF>(pc, ai, aj, qu, e, jq, islot, qc, myclose, nclose, px, py, pz,
                              pp);
         }
       } else {
         for (; e + 2 <= nq; e += 2) {
           const V4<T> a0 = qatoms[warp][e][jq], a1 = qatoms[warp][e + 1][jq];
-          tile<T, NU, MIXED>(pc, ai, a0, qu, e, jq, islot, qc, myclose, nclose, px, py, pz,
+          tile<T, NU, MIXED, SELF>(pc, ai, a0, qu, e, jq, islot, qc, myclose, nclose, px, py, pz,
                              pp);
-          tile<T, NU, MIXED>(pc, ai, a1, qu, e + 1, jq, islot, qc, myclose, nclose, px, py,
+          tile<T, NU, MIXED, SELF>(pc, ai, a1, qu, e + 1, jq, islot, qc, myclose, nclose, px, py,
                              pz, pp);
         }
         if (e < nq)
-          tile<T, NU, MIXED>(pc, ai, qatoms[warp][e][jq], qu, e, jq, islot, qc, myclose,
+          tile<T, NU, MIXED, SELF>(pc, ai, qatoms[warp][e][jq], qu, e, jq, islot, qc, myclose,
                              nclose, px, py, pz, pp);
       }
       __syncwarp();
@@ -498,7 +506,10 @@ template <typename T, int NU>
 void launch_nu(cudaStream_t s, const PairClusterArgs<T> &a, const PairConsts<T> &pc) {
   constexpr bool kMixed = sizeof(T) == 4;
   const int blocks = std::max(1, (a.maxcl + kWarps - 1) / kWarps);
-  k_pair_clusters<T, NU, kMixed><<<blocks, kWarps * 32, 0, s>>>(a, pc);
+  if (a.self_images)
+    k_pair_clusters<T, NU, kMixed, true><<<blocks, kWarps * 32, 0, s>>>(a, pc);
+  else
+    k_pair_clusters<T, NU, kMixed, false><<<blocks, kWarps * 32, 0, s>>>(a, pc);
 }
 
 }  // namespace

@@ -162,6 +162,8 @@ struct PairClusterArgs {
   const V4<double> *cpos64;   // FP64 copy (mixed form) or null
   V4<T> *out;                 // per sorted atom: force / q_i and potential
   int *err;
+  int self_images;            // a lattice vector shorter than a0: an atom's
+                              // own images reach its tiles and are skipped
 };
 int cluster_capacity(int N, int ncol);
 void launch_column_clusters(cudaStream_t s, int ncol, int nc2, const int *start,

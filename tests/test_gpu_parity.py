@@ -172,6 +172,35 @@ def test_alternative_kernels(case, variant, monkeypatch):
         ff.close()
 
 
+@pytest.mark.parametrize("variant", ["clusters", "cells", "thread"])
+def test_box_smaller_than_cutoff(variant, monkeypatch):
+    """Boxes with a lattice vector shorter than the cutoff: an atom's own
+    periodic images lie within a0. The reference sums them once, in the
+    constant coeff1 (code/forcefield0.c:612-636), and its pair list never
+    pairs an atom with itself (code/forcefield1.c:240-321), so every pair
+    kernel must skip the atom at all its images."""
+    if variant != "clusters":
+        monkeypatch.setenv("MSMPB_PAIR", variant)
+    rng = np.random.default_rng(21)
+    n = 24
+    q = rng.choice([-1.0, 1.0], n)
+    q -= q.mean()
+    for edges in (np.diag([6.0, 7.0, 6.5]), np.array([[6.0, 1.0, 0.5], [0.0, 6.5, 1.2],
+                                                      [0.0, 0.0, 7.0]])):
+        pos = rng.uniform(0, 1, (n, 3)) @ edges.T
+        o = Oracle(q, edges, cutoff=8.0, nu=4, levels=1, top_grid=[8, 8, 8])
+        eo, fo, po = o.energy(pos)
+        for precision in ("fp64", "mixed"):
+            ff = ForceField(q, pos, edges, cutoff=8.0, order=4, levels=1, top_grid=8,
+                            precision=precision)
+            e, f, phi = ff.energy(pos, potentials=True)
+            te, tf, tp = TOL[precision]
+            assert abs(e - eo) / abs(eo) < te, (precision, e, eo)
+            assert force_err(f, fo, q, edges) < tf
+            assert rel_rms(phi, po) < tp
+            ff.close()
+
+
 def test_repeat_and_charge_update():
     """Repeated calls give identical results; charge edits between calls
     are seen (FF_new keeps the caller's pointer, code/forcefield0.c:172)."""
