@@ -145,3 +145,85 @@ def load():
         fn.argtypes = args
     _lib = lib
     return lib
+
+
+# ---------------------------------------------------------------------------
+# The smooth-PME comparator library (include/pme.h, include/pme_b200.h)
+
+PME_LIB_PATH = os.path.join(HERE, "libpme.so")
+
+PME_EXPORTED = [
+    "FF_new", "FF_set_cutoff", "FF_get_cutoff", "FF_set_orderAcc", "FF_set_topGridDim",
+    "FF_set_tolDir", "FF_build", "FF_get_orderAcc", "FF_get_topGridDim", "FF_get_tolDir",
+    "FF_get_errEst", "FF_rebuild", "FF_energy", "FF_delete", "msm4g_tictocmanager",
+    "msm4g_tic", "msm4g_toc", "prod", "prodT",
+    "FF_last_error", "FF_error_string", "FF_set_precision", "FF_get_precision",
+    "FF_set_device", "FF_set_timing", "FF_energy_potentials", "FF_energy_device",
+    "FF_sync", "FF_phase_times", "FF_kernel_launches",
+]
+
+_pme = None
+
+
+class PmeStruct(C.Structure):
+    """struct FF of include/pme.h (reference layout + appended members)."""
+    _fields_ = [
+        ("N", C.c_int), ("q", _dp), ("A", C.c_double * 9), ("Ai", C.c_double * 9),
+        ("detA", C.c_double), ("cutoff", C.c_double), ("orderAcc", C.c_int),
+        ("topGridDim", C.c_int * 3), ("nlist", _ip), ("nlist_len", C.c_int),
+        ("nlist_interaction_count", C.c_int), ("tolDir", C.c_double),
+        ("fftw_in", C.c_void_p), ("forward", C.c_void_p), ("backward", C.c_void_p),
+        ("beta", C.c_double), ("Q", _dp), ("cL", _dp * 3), ("khat", _dp),
+        ("coeff1", C.c_double), ("coeff2", C.c_double),
+        ("time_partcl2partcl", C.c_double), ("time_nlist", C.c_double),
+        ("time_grid2grid", C.c_double), ("time_stencil", C.c_double),
+        ("time_anterpolation", C.c_double), ("time_interpolation", C.c_double),
+        ("dev", C.c_void_p), ("host_state", C.c_void_p), ("last_error", C.c_int),
+        ("precision", C.c_int), ("device", C.c_int), ("timing", C.c_int),
+    ]
+
+
+def load_pme():
+    """Load and bind libpme.so (raises OSError if it is not built)."""
+    global _pme
+    if _pme is not None:
+        return _pme
+    if not os.path.exists(PME_LIB_PATH):
+        raise OSError("msmpb_b200: %s is missing; run `python -m msmpb_b200.build`"
+                      % PME_LIB_PATH)
+    lib = C.CDLL(PME_LIB_PATH)
+    P = C.POINTER(PmeStruct)
+    sig = {
+        "FF_new": (P, [C.c_int, _dp, _dp]),
+        "FF_set_cutoff": (None, [P, C.c_double]),
+        "FF_get_cutoff": (C.c_double, [P]),
+        "FF_set_orderAcc": (None, [P, C.c_int]),
+        "FF_set_topGridDim": (None, [P, _ip]),
+        "FF_set_tolDir": (None, [P, C.c_double]),
+        "FF_build": (None, [P, _dp]),
+        "FF_get_orderAcc": (C.c_int, [P]),
+        "FF_get_topGridDim": (None, [P, _ip]),
+        "FF_get_tolDir": (C.c_double, [P]),
+        "FF_get_errEst": (C.c_double, [P, C.c_int, _dp]),
+        "FF_rebuild": (None, [P, _dp, _dp]),
+        "FF_energy": (C.c_double, [P, _dp, _dp, _dp]),
+        "FF_energy_potentials": (C.c_double, [P, _dp, _dp, _dp, _dp]),
+        "FF_energy_device": (C.c_int, [P, C.c_void_p, C.c_void_p, _dp, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p]),
+        "FF_delete": (None, [P]),
+        "FF_last_error": (C.c_int, [P]),
+        "FF_error_string": (C.c_char_p, [C.c_int]),
+        "FF_set_precision": (None, [P, C.c_int]),
+        "FF_get_precision": (C.c_int, [P]),
+        "FF_set_device": (None, [P, C.c_int]),
+        "FF_set_timing": (None, [P, C.c_int]),
+        "FF_sync": (C.c_int, [P]),
+        "FF_phase_times": (C.c_int, [P, _dp, C.c_int]),
+        "FF_kernel_launches": (C.c_int, [P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _pme = lib
+    return lib

@@ -1,10 +1,14 @@
-"""Build the MSM library for sm_100a: ``msmpb_b200/libmsmpb.so``.
+"""Build the libraries for sm_100a: ``msmpb_b200/libmsmpb.so`` (MSM) and
+``msmpb_b200/libpme.so`` (the smooth-PME comparator).
 
-Every .cu/.cpp under msmpb_b200/csrc is compiled with nvcc
+Every .cu/.cpp under msmpb_b200/csrc (and csrc/pme) is compiled with nvcc
 (``-gencode arch=compute_100a,code=sm_100a -lineinfo``) into
-msmpb_b200/_build/, then linked into a shared library that exports the
-forcefield.h C ABI (see include/). CUDA runtime is linked statically so the
-library loads on any box with the driver.
+msmpb_b200/_build/. libmsmpb.so links the engine and kernels with the MSM C
+ABI (forcefield.h, msmpb_b200.h: ff_api.cpp, batch.cpp, noalloc.cu);
+libpme.so links the same engine and kernels with the PME C ABI (pme.h,
+pme_b200.h: csrc/pme/). The two export the same FF_* names for their own
+methods, as the reference's two builds do. CUDA runtime is linked
+statically so the libraries load on any box with the driver.
 
 Usage: python -m msmpb_b200.build [--force] [-j N] [--verbose]
 """
@@ -20,6 +24,10 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libmsmpb.so")
+PME_LIB = os.path.join(PKG, "libpme.so")
+PME_SRC = os.path.join(CSRC, "pme")
+# MSM C ABI, not linked into libpme.so
+MSM_ONLY = ("ff_api.cpp", "batch.cpp", "noalloc.cu")
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -37,9 +45,10 @@ def nvcc():
 
 def sources():
     out = []
-    for f in sorted(os.listdir(CSRC)):
-        if f.endswith((".cu", ".cpp")):
-            out.append(os.path.join(CSRC, f))
+    for d in (CSRC, PME_SRC):
+        for f in sorted(os.listdir(d)):
+            if f.endswith((".cu", ".cpp")):
+                out.append(os.path.join(d, f))
     return out
 
 
@@ -85,11 +94,15 @@ def build(force=False, jobs=None, verbose=False, extra=None):
             msg = f.result()
             if verbose and msg:
                 print(msg)
-    if todo or not os.path.exists(LIB) or os.path.getmtime(LIB) < _newest(objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static"]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+    msm_objs = [o for s, o in zip(srcs, objs) if os.path.dirname(s) == CSRC]
+    pme_objs = [o for s, o in zip(srcs, objs)
+                if os.path.basename(s) not in MSM_ONLY]
+    for lib, lobjs in ((LIB, msm_objs), (PME_LIB, pme_objs)):
+        if todo or not os.path.exists(lib) or os.path.getmtime(lib) < _newest(lobjs):
+            cmd = [nvcc(), *ARCH, "-shared", "-o", lib, *lobjs, "-cudart", "static"]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
     return LIB
 
 

@@ -194,6 +194,7 @@ class Plan : public FFDevice {
   int ncol_ = 0, maxcl_ = 0, ncoloff_ = 0, K2_ = 0;
   bool clusters_ok_ = false;
   bool self_images_ = false;  // a lattice vector shorter than a0
+  int kind_ = kKindMsm;       // kKindPme: one-level PME plan
   double cz_[3] = {};
   int nq_ = 0, ncomb_ = 0, ngrid_ = 0;
   std::vector<CellOffset<T>> offsets_;
@@ -468,7 +469,16 @@ void Plan<T>::plan_level(int l) {
 template <typename T>
 int Plan<T>::set_tables(const Tables &t) {
   const Params &p = t.p;
-  pc_.nu = sc_.nu = p.nu;
+  kind_ = t.kind;
+  pc_.nu = t.kind == kKindPme ? 0 : p.nu;  // 0 selects the erfc kernel
+  sc_.nu = p.nu;
+  const double c_exp = 2. * t.beta / std::sqrt(std::acos(-1.));
+  pc_.beta = (T)t.beta;
+  pc_.beta2 = (T)(t.beta * t.beta);
+  pc_.c_exp = (T)c_exp;
+  pc_.betad = t.beta;
+  pc_.beta2d = t.beta * t.beta;
+  pc_.c_expd = c_exp;
   pc_.a02 = (T)(p.a0 * p.a0);
   pc_.inv_a02 = (T)(1. / (p.a0 * p.a0));
   pc_.inv_a0 = (T)(1. / p.a0);
@@ -502,6 +512,7 @@ int Plan<T>::update(const Tables &t) {
 
 template <typename T>
 int Plan<T>::update_device(const Tables &t, cudaStream_t stream) {
+  if (t.kind != kKindMsm) return MSMPB_ERR_UNSUPPORTED;  // MSM level stencils only
   MSM_CUDA_TRY(cudaSetDevice(device_));
   if (!rebuild_ev_)
     MSM_CUDA_TRY(cudaEventCreateWithFlags(&rebuild_ev_, cudaEventDisableTiming));
@@ -812,6 +823,10 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   ea.gamma0_over_a0 = gamma0_a0_;
   ea.energy = energy ? energy : energy_;
   ea.qstats = qstats_;
+  // PME weighs the grid charges before the solve and dots the weighted
+  // charges with the result: its grid energy carries w_1^2
+  // (code/pme1.c:86-101); MSM's carries w_L once
+  ea.grid_scale = kind_ == kKindPme ? w[1] : 1.0;
   launch_energy_total(s, ea);
   nl += 2;
   mark(s, kNumPhases, tm);
@@ -881,7 +896,8 @@ int Plan<T>::evaluate(const EvalRequest &r, double *energy) {
 template <typename T>
 int Plan<T>::adjoint(const AdjointRequest &r) {
   MSM_CUDA_TRY(cudaSetDevice(device_));
-  if (!anterp_scratch_ || !fold_tab_) return MSMPB_ERR_UNSUPPORTED;
+  // the adjoint's pair Hessian is written for the MSM kernel
+  if (kind_ != kKindMsm || !anterp_scratch_ || !fold_tab_) return MSMPB_ERR_UNSUPPORTED;
   if (!r.pos || !r.q || !r.fbar) return MSMPB_ERR_ARGUMENT;
   if (!adj_mem_) {
     // six per-atom records and a second set of level grids

@@ -349,7 +349,7 @@ __global__ void __launch_bounds__(kThreads) k_energy_total(EnergyArgs a) {
   if (threadIdx.x == 0) {
     double uc = 0.5 * q2 * a.coeff1 - 0.5 * qs * qs * a.coeff2 -
                 0.5 * q2 * a.gamma0_over_a0;
-    a.energy[0] = a.w0 * uc + us + 0.5 * ug;
+    a.energy[0] = a.w0 * uc + us + 0.5 * a.grid_scale * ug;
   }
 }
 

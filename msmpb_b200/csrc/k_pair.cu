@@ -20,6 +20,7 @@
 // relative error of 2.4e-7 on a 1 A bond; everywhere else the FP32 result
 // is within rounding of the FP64 one.
 #include "kernels.h"
+#include "pair_fn.cuh"
 
 namespace msm {
 namespace {
@@ -77,31 +78,19 @@ k_pair(int N, const V4<T> *__restrict__ ps, const V4<double> *__restrict__ ps64,
           const double ey = (aj.y + co.shift64[1]) - ai64.y;
           const double ez = (aj.z + co.shift64[2]) - ai64.z;
           const double d2 = ex * ex + ey * ey + ez * ez;
-          const double sd = d2 * pc.inv_a02d - 1.0;
-          double ts = pc.taud[NU - 1], t1 = 0.0;
-#pragma unroll
-          for (int m = NU - 2; m >= 0; --m) {
-            t1 = ts + sd * t1;
-            ts = pc.taud[m] + sd * ts;
-          }
-          const double rinv = 1.0 / sqrt(d2);
-          cph += aj.w * (rinv - ts * pc.inv_a0d);
-          const double cf = aj.w * (-rinv * rinv * rinv - t1 * pc.two_inv_a03d);
+          double v, f;
+          pair_radial64<NU>(pc, d2, v, f);
+          cph += aj.w * v;
+          const double cf = aj.w * f;
           cfx += cf * ex;
           cfy += cf * ey;
           cfz += cf * ez;
           continue;
         }
-        const T s = r2 * pc.inv_a02 - T(1);
-        T ts = pc.tau[NU - 1], t1 = T(0);
-#pragma unroll
-        for (int m = NU - 2; m >= 0; --m) {
-          t1 = ts + s * t1;
-          ts = pc.tau[m] + s * ts;
-        }
-        const T rinv = rsqrt_t<T>(r2);
-        pp += aj.w * (rinv - ts * pc.inv_a0);
-        const T cf = aj.w * (-rinv * rinv * rinv - t1 * pc.two_inv_a03);
+        T v, f;
+        pair_radial<T, NU>(pc, r2, v, f);
+        pp += aj.w * v;
+        const T cf = aj.w * f;
         px += cf * dx;
         py += cf * dy;
         pz += cf * dz;
@@ -128,16 +117,10 @@ k_pair(int N, const V4<T> *__restrict__ ps, const V4<double> *__restrict__ ps64,
       const double ey = (aj.y + co.shift64[1]) - ai64.y;
       const double ez = (aj.z + co.shift64[2]) - ai64.z;
       const double d2 = ex * ex + ey * ey + ez * ez;
-      const double sd = d2 * pc.inv_a02d - 1.0;
-      double ts = pc.taud[NU - 1], t1 = 0.0;
-#pragma unroll
-      for (int m = NU - 2; m >= 0; --m) {
-        t1 = ts + sd * t1;
-        ts = pc.taud[m] + sd * ts;
-      }
-      const double rinv = 1.0 / sqrt(d2);
-      cph += aj.w * (rinv - ts * pc.inv_a0d);
-      const double cf = aj.w * (-rinv * rinv * rinv - t1 * pc.two_inv_a03d);
+      double v, f;
+      pair_radial64<NU>(pc, d2, v, f);
+      cph += aj.w * v;
+      const double cf = aj.w * f;
       cfx += cf * ex;
       cfy += cf * ey;
       cfz += cf * ez;
@@ -179,6 +162,7 @@ void launch_pair(cudaStream_t s, int N, const V4<T> *ps, const V4<double> *ps64,
                  const CellOffset<T> *off, int noff, const PairConsts<T> &pc,
                  V4<T> *out) {
   switch (pc.nu) {
+    case 0: launch_nu<T, 0>(s, N, ps, ps64, pcs, start, g, off, noff, pc, out); break;
     case 4: launch_nu<T, 4>(s, N, ps, ps64, pcs, start, g, off, noff, pc, out); break;
     case 6: launch_nu<T, 6>(s, N, ps, ps64, pcs, start, g, off, noff, pc, out); break;
     case 8: launch_nu<T, 8>(s, N, ps, ps64, pcs, start, g, off, noff, pc, out); break;

@@ -19,6 +19,7 @@
 // for why: their forces are the largest and the most sensitive to position
 // rounding).
 #include "kernels.h"
+#include "pair_fn.cuh"
 
 namespace msm {
 namespace {
@@ -36,16 +37,10 @@ template <typename T, int NU>
 __device__ __forceinline__ void pair_terms(const PairConsts<T> &pc, T dx, T dy,
                                            T dz, T r2, T qj, T &fx, T &fy,
                                            T &fz, T &ph) {
-  const T s = r2 * pc.inv_a02 - T(1);
-  T ts = pc.tau[NU - 1], t1 = T(0);
-#pragma unroll
-  for (int m = NU - 2; m >= 0; --m) {
-    t1 = ts + s * t1;
-    ts = pc.tau[m] + s * ts;
-  }
-  const T rinv = rsqrt_t<T>(r2);
-  ph += qj * (rinv - ts * pc.inv_a0);
-  const T cf = qj * (-rinv * rinv * rinv - t1 * pc.two_inv_a03);
+  T v, f;
+  pair_radial<T, NU>(pc, r2, v, f);
+  ph += qj * v;
+  const T cf = qj * f;
   fx += cf * dx;
   fy += cf * dy;
   fz += cf * dz;
@@ -213,16 +208,10 @@ k_pair_cells(const V4<T> *__restrict__ ps, const V4<double> *__restrict__ ps64,
             const double ey = (aj.y + off[o].shift64[1]) - ri64.y;
             const double ez = (aj.z + off[o].shift64[2]) - ri64.z;
             const double d2 = ex * ex + ey * ey + ez * ez;
-            const double sd = d2 * pc.inv_a02d - 1.0;
-            double ts = pc.taud[NU - 1], t1 = 0.0;
-#pragma unroll
-            for (int mm = NU - 2; mm >= 0; --mm) {
-              t1 = ts + sd * t1;
-              ts = pc.taud[mm] + sd * ts;
-            }
-            const double rinv = 1.0 / sqrt(d2);
-            cph += aj.w * (rinv - ts * pc.inv_a0d);
-            const double cf = aj.w * (-rinv * rinv * rinv - t1 * pc.two_inv_a03d);
+            double v, f;
+            pair_radial64<NU>(pc, d2, v, f);
+            cph += aj.w * v;
+            const double cf = aj.w * f;
             cfx += cf * ex;
             cfy += cf * ey;
             cfz += cf * ez;
@@ -295,6 +284,7 @@ void launch_pair_cells(cudaStream_t s, int ncell, const V4<T> *ps,
                        const Geometry &g, const CellOffset<T> *off, int noff,
                        const PairConsts<T> &pc, V4<T> *out, int *err) {
   switch (pc.nu) {
+    case 0: launch_nu<T, 0>(s, ncell, ps, ps64, start, g, off, noff, pc, out, err); break;
     case 4: launch_nu<T, 4>(s, ncell, ps, ps64, start, g, off, noff, pc, out, err); break;
     case 6: launch_nu<T, 6>(s, ncell, ps, ps64, start, g, off, noff, pc, out, err); break;
     case 8: launch_nu<T, 8>(s, ncell, ps, ps64, start, g, off, noff, pc, out, err); break;

@@ -20,6 +20,7 @@
 // with compensation in the mixed form, and pairs closer than sqrt(close2)
 // are queued per lane and summed in FP64 after the sweep.
 #include "kernels.h"
+#include "pair_fn.cuh"
 
 namespace msm {
 namespace {
@@ -146,16 +147,10 @@ __global__ void k_column_clusters(int ncol, int nc2, const int *__restrict__ sta
 template <typename T, int NU>
 __device__ __forceinline__ void pair_terms(const PairConsts<T> &pc, T r2, T qj,
                                            T &pot, T &fs) {
-  const T s = r2 * pc.inv_a02 - T(1);
-  T ts = pc.tau[NU - 1], t1 = T(0);
-#pragma unroll
-  for (int m = NU - 2; m >= 0; --m) {
-    t1 = ts + s * t1;
-    ts = pc.tau[m] + s * ts;
-  }
-  const T rinv = rsqrt_t<T>(r2);
-  pot = qj * (rinv - ts * pc.inv_a0);
-  fs = qj * (-rinv * rinv * rinv - t1 * pc.two_inv_a03);
+  T v, f;
+  pair_radial<T, NU>(pc, r2, v, f);
+  pot = qj * v;
+  fs = qj * f;
 }
 
 // One pair in FP64 from FP64 cluster-frame positions and the FP64 shift of
@@ -170,16 +165,10 @@ __device__ __forceinline__ void close_pair64(const PairConsts<float> &pc,
   const double ey = (aj.y + sy) - ai.y;
   const double ez = (aj.z + sz) - ai.z;
   const double d2 = ex * ex + ey * ey + ez * ez;
-  const double sd = d2 * pc.inv_a02d - 1.0;
-  double ts = pc.taud[NU - 1], t1 = 0.0;
-#pragma unroll
-  for (int m = NU - 2; m >= 0; --m) {
-    t1 = ts + sd * t1;
-    ts = pc.taud[m] + sd * ts;
-  }
-  const double rinv = 1.0 / sqrt(d2);
-  p += aj.w * (rinv - ts * pc.inv_a0d);
-  const double cf = aj.w * (-rinv * rinv * rinv - t1 * pc.two_inv_a03d);
+  double v, f;
+  pair_radial64<NU>(pc, d2, v, f);
+  p += aj.w * v;
+  const double cf = aj.w * f;
   fx += cf * ex;
   fy += cf * ey;
   fz += cf * ez;
@@ -259,6 +248,17 @@ __device__ __forceinline__ void tile2(const PairConsts<float> &pc, const V4<floa
   if (!(h0 || h1)) return;
   const float2 rr = make_float2(h0 ? r2.x : pc.a02, h1 ? r2.y : pc.a02);
   const float2 qj = make_float2(h0 ? Y.z : 0.f, h1 ? Y.w : 0.f);
+  if constexpr (NU == 0) {  // PME kernel: the two entries one at a time
+    float v0, f0, v1, f1;
+    pair_radial<float, 0>(pc, rr.x, v0, f0);
+    pair_radial<float, 0>(pc, rr.y, v1, f1);
+    const float2 fs = make_float2(qj.x * f0, qj.y * f1);
+    pp = __fadd2_rn(pp, make_float2(qj.x * v0, qj.y * v1));
+    px = __ffma2_rn(fs, dx, px);
+    py = __ffma2_rn(fs, dy, py);
+    pz = __ffma2_rn(fs, dz, pz);
+    return;
+  } else {
   const float2 s = __ffma2_rn(rr, make_float2(pc.inv_a02, pc.inv_a02), make_float2(-1.f, -1.f));
   float2 ts = make_float2(pc.tau[NU - 1], pc.tau[NU - 1]), t1 = make_float2(0.f, 0.f);
 #pragma unroll
@@ -277,6 +277,7 @@ __device__ __forceinline__ void tile2(const PairConsts<float> &pc, const V4<floa
   px = __ffma2_rn(fs, dx, px);
   py = __ffma2_rn(fs, dy, py);
   pz = __ffma2_rn(fs, dz, pz);
+  }
 }
 
 template <typename T, int NU, bool MIXED, bool SELF>
@@ -536,6 +537,7 @@ template <typename T>
 void launch_pair_clusters(cudaStream_t s, const PairClusterArgs<T> &a,
                           const PairConsts<T> &pc) {
   switch (pc.nu) {
+    case 0: launch_nu<T, 0>(s, a, pc); break;
     case 4: launch_nu<T, 4>(s, a, pc); break;
     case 6: launch_nu<T, 6>(s, a, pc); break;
     case 8: launch_nu<T, 8>(s, a, pc); break;

@@ -42,7 +42,10 @@ struct PairConsts {
   T close2;
   double a02d, inv_a02d, inv_a0d, two_inv_a03d;
   double taud[16];
-  int nu;
+  int nu;  // MSM: the B-spline order; 0: the PME kernel erfc(beta r)/r
+  // PME: beta, beta^2, 2 beta / sqrt(pi)
+  T beta, beta2, c_exp;
+  double betad, beta2d, c_expd;
 };
 
 // B-spline piece coefficients for the device
@@ -104,6 +107,7 @@ struct EnergyArgs {
   double w0, coeff1, coeff2, gamma0_over_a0;
   double *energy;  // device scalar
   double *qstats;  // device [qsum, q2sum]
+  double grid_scale = 1.0;  // factor on the grid energy q^1 . e^1 / 2
 };
 void launch_energy_total(cudaStream_t s, const EnergyArgs &a);
 void launch_qstats_final(cudaStream_t s, const double *qparts, int nqparts,

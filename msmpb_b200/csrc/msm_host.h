@@ -21,7 +21,14 @@ struct Params {
   bool fft = true;
 };
 
+// Method of a table set: B-spline MSM, or smooth PME (code/pme0.c, pme1.c),
+// which the engine evaluates as a one-level plan with the direct-space
+// kernel erfc(beta r)/r and the PME influence function as top multiplier.
+constexpr int kKindMsm = 0, kKindPme = 1;
+
 struct Tables {
+  int kind = kKindMsm;
+  double beta = 0;           // PME Ewald splitting parameter
   Params p;
   double tau[16] = {};       // softening polynomial, degree nu-1
   double Q[5 * 10] = {};     // B-spline pieces: Q[j*nu+k] = [t^k] Q_nu(j+t)
@@ -37,6 +44,29 @@ struct Tables {
 
 // Matrix helpers (reference code/forcefield0.c:709-724)
 double invert3(const double a[3][3], double ai[3][3]);
+
+// B-spline pieces Q[j*nu+k] = [t^k] Q_nu(j+t), j < nu/2
+void bspline_pieces(int nu, double *Q);
+
+// Smooth-PME comparator (code/pme0.c, code/pme1.c): host setup of a
+// one-level table set (kind kKindPme) for the engine.
+namespace pme {
+struct Settings {  // the FF_set_* values; <= 0 means the reference default
+  double cutoff = 0, tolDir = 0;
+  int nu = 0;
+  int M[3] = {0, 0, 0};
+};
+// Parameters as FF_build (code/pme0.c:192-260): defaults, beta from
+// erfc(beta a0)/a0 = tolDir, grid from the spacing table. Returns false (and
+// MSMPB_ERR_UNSUPPORTED in *err) where the reference prints and exits: no
+// default grid for this order or cutoff.
+bool select(Params &p, double *beta, double *tolDir, int N, const double edges[3][3],
+            const Settings &s, int *err);
+// Every table of a parameter set (code/pme0.c:262-322, :365-412, :444-503)
+void build_tables(Tables &t, const Params &p, double beta);
+// FF_get_errEst (code/pme0.c:333-361)
+double err_est(const Params &p, const double *q);
+}  // namespace pme
 
 // Parameter selection exactly as FF_build (code/forcefield0.c:271-367).
 // Arguments use the reference's -1 = auto convention. Returns false when the

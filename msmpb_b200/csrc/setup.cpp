@@ -63,6 +63,21 @@ int centred_offset(int d, int n) {
 
 }  // namespace
 
+void bspline_pieces(int nu, double *Q) {
+  double fact = 1;
+  for (int i = 2; i < nu; ++i) fact *= i;
+  for (int j = 0; j < nu / 2; ++j)
+    for (int k = 0; k < nu; ++k) {
+      int64_t s = 0;
+      for (int i = 0; i <= j; ++i) {
+        int64_t pw = 1;
+        for (int e = 0; e < nu - 1 - k; ++e) pw *= (j - i);
+        s += ((i & 1) ? -1 : 1) * choose(nu, i) * pw;
+      }
+      Q[j * nu + k] = (double)(choose(nu - 1, k) * s) / fact;
+    }
+}
+
 double invert3(const double a[3][3], double ai[3][3]) {
   double c[3][3];
   for (int i = 0; i < 3; ++i)
@@ -200,18 +215,7 @@ void make_tau(Tables &t) {
 // (same table as code/forcefield0.c:375-406, derived in closed form)
 void make_bspline(Tables &t) {
   const int nu = t.p.nu;
-  double fact = 1;
-  for (int i = 2; i < nu; ++i) fact *= i;
-  for (int j = 0; j < nu / 2; ++j)
-    for (int k = 0; k < nu; ++k) {
-      int64_t s = 0;
-      for (int i = 0; i <= j; ++i) {
-        int64_t pw = 1;
-        for (int e = 0; e < nu - 1 - k; ++e) pw *= (j - i);
-        s += ((i & 1) ? -1 : 1) * choose(nu, i) * pw;
-      }
-      t.Q[j * nu + k] = (double)(choose(nu - 1, k) * s) / fact;
-    }
+  bspline_pieces(nu, t.Q);
   for (int n = 0; n <= nu; ++n) t.J[n] = (double)choose(nu, n) * std::pow(2., 1 - nu);
 }
 

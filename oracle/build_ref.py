@@ -28,6 +28,12 @@ Outputs (all under oracle/_ref/):
   msmpb_dropin               the same driver source, unmodified, compiled against
                              this project's include/forcefield.h and linked to
                              msmpb_b200/libmsmpb.so (the drop-in check of the CLI)
+  libpme_ref.so              the reference smooth-PME comparator (code/pme0.c,
+                             code/pme1.c, unmodified) with the FFT shim
+  pme_ref                    its CLI driver (code/pme.c) over those sources
+  pme_dropin                 code/pme.c, unmodified, compiled against this
+                             project's include/pme.h and linked to
+                             msmpb_b200/libpme.so
 
 Usage: python oracle/build_ref.py [--reference DIR]
 """
@@ -112,9 +118,32 @@ def build(reference_root="/root/reference", quiet=False):
         run([cc, "-O2", "-std=gnu11", "-w", "-I", os.path.join(root, "include"), drv_copy,
              "-L", our_lib_dir, "-lmsmpb", "-lm", "-Wl,-rpath,$ORIGIN/../../msmpb_b200",
              "-o", os.path.join(OUT, "msmpb_dropin")])
+    build_pme(code, src_dir, inc, fft, cc, root)
     if not quiet:
         print("build_ref: built", OUT)
     return True
+
+
+def build_pme(code, src_dir, inc, fft, cc, root):
+    """The PME comparator: library, driver and drop-in driver."""
+    p0, p1, drv = (os.path.join(code, f) for f in ("pme0.c", "pme1.c", "pme.c"))
+    if not all(os.path.exists(p) for p in (p0, p1, drv)):
+        return
+    glue = os.path.join(src_dir, "pme_glue.c")
+    with open(glue, "w") as f:
+        f.write('#include "pme.h"\n'
+                '/* the drivers define o (code/pme.c:9); a bare library must */\n'
+                'struct O o = {"none"};\n')
+    run([cc, *CFLAGS, "-shared", *inc, p0, p1, fft, glue, "-lm",
+         "-o", os.path.join(OUT, "libpme_ref.so")])
+    run([cc, *CFLAGS, *inc, drv, p0, p1, fft, "-lm", "-o", os.path.join(OUT, "pme_ref")])
+    our_lib_dir = os.path.join(root, "msmpb_b200")
+    if os.path.exists(os.path.join(our_lib_dir, "libpme.so")):
+        drv_copy = os.path.join(src_dir, "pme_dropin.c")
+        shutil.copy(drv, drv_copy)
+        run([cc, "-O2", "-std=gnu11", "-w", "-I", os.path.join(root, "include"), drv_copy,
+             "-L", our_lib_dir, "-l:libpme.so", "-lm", "-Wl,-rpath,$ORIGIN/../../msmpb_b200",
+             "-o", os.path.join(OUT, "pme_dropin")])
 
 
 if __name__ == "__main__":

@@ -27,7 +27,7 @@ _ip = C.POINTER(C.c_int)
 
 def build_oracle(force=False):
     """Compile the C restatement (gcc, no GPU needed)."""
-    srcs = [os.path.join(HERE, "msm_oracle.c"),
+    srcs = [os.path.join(HERE, "msm_oracle.c"), os.path.join(HERE, "pme_oracle.c"),
             os.path.join(HERE, "fftw_shim", "fft_shim.c")]
     if (not force and os.path.exists(ORACLE_SO) and
             all(os.path.getmtime(s) <= os.path.getmtime(ORACLE_SO) for s in srcs)):
@@ -352,6 +352,210 @@ class RefFF:
 
     def close(self):
         if self.ff:
+            self._lib.FF_delete(self.ff)
+            self.ff = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class PmeOracle:
+    """FP64 CPU restatement of the reference smooth-PME path
+    (oracle/pme_oracle.c)."""
+
+    _lib = None
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            lib = Oracle.lib()
+            lib.pmeo_create.restype = C.c_void_p
+            lib.pmeo_create.argtypes = [C.c_int, _dp, C.c_double, C.c_int, _ip, C.c_double]
+            lib.pmeo_destroy.argtypes = [C.c_void_p]
+            lib.pmeo_rebuild.argtypes = [C.c_void_p, _dp]
+            lib.pmeo_params.argtypes = [C.c_void_p, _dp, _ip, _ip, _dp, _dp, _dp]
+            lib.pmeo_coeffs.argtypes = [C.c_void_p, _dp, _dp]
+            lib.pmeo_khat.restype = _dp
+            lib.pmeo_khat.argtypes = [C.c_void_p]
+            lib.pmeo_cL.restype = _dp
+            lib.pmeo_cL.argtypes = [C.c_void_p, C.c_int]
+            lib.pmeo_errEst.restype = C.c_double
+            lib.pmeo_errEst.argtypes = [C.c_void_p, _dp]
+            lib.pmeo_energy.restype = C.c_double
+            lib.pmeo_energy.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp]
+            lib.pmeo_short_range.restype = C.c_double
+            lib.pmeo_short_range.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
+            cls._lib = lib
+        return cls._lib
+
+    def __init__(self, q, edges, cutoff=-1, nu=-1, grid=None, tol_dir=-1):
+        lib = self.lib()
+        self.q = _f64(q)
+        self.N = len(self.q)
+        self.edges = _f64(np.asarray(edges).reshape(3, 3)).copy()
+        g = None
+        if grid is not None:
+            g = np.ascontiguousarray(np.broadcast_to(np.asarray(grid), (3,)), dtype=np.int32)
+        self.h = lib.pmeo_create(self.N, _ptr(self.edges), float(cutoff), int(nu),
+                                 _ptr(g, C.c_int) if g is not None else None, float(tol_dir))
+        if not self.h:
+            raise ValueError("no default PME grid for this order and cutoff")
+        self._read()
+
+    def _read(self):
+        c, n, t, b, d = C.c_double(), C.c_int(), C.c_double(), C.c_double(), C.c_double()
+        M = (C.c_int * 3)()
+        self.lib().pmeo_params(self.h, C.byref(c), C.byref(n), M, C.byref(t), C.byref(b),
+                               C.byref(d))
+        self.cutoff, self.nu, self.grid = c.value, n.value, tuple(M)
+        self.tol_dir, self.beta, self.detA = t.value, b.value, d.value
+
+    def rebuild(self, edges):
+        self.edges = _f64(np.asarray(edges).reshape(3, 3)).copy()
+        self.lib().pmeo_rebuild(self.h, _ptr(self.edges))
+        self._read()
+
+    def energy(self, pos, weight=None, q=None):
+        q = self.q if q is None else _f64(q)
+        pos = _f64(pos)
+        f = np.zeros((self.N, 3))
+        phi = np.zeros(self.N)
+        w = None if weight is None else _f64(weight)
+        e = self.lib().pmeo_energy(self.h, _ptr(q), _ptr(pos), _ptr(w) if w is not None else None,
+                                   _ptr(f), _ptr(phi))
+        return e, f, phi
+
+    def short_range(self, pos, q=None):
+        q = self.q if q is None else _f64(q)
+        f = np.zeros((self.N, 3))
+        phi = np.zeros(self.N)
+        e = self.lib().pmeo_short_range(self.h, _ptr(q), _ptr(_f64(pos)), _ptr(f), _ptr(phi))
+        return e, f, phi
+
+    def coeffs(self):
+        c1, c2 = C.c_double(), C.c_double()
+        self.lib().pmeo_coeffs(self.h, C.byref(c1), C.byref(c2))
+        return c1.value, c2.value
+
+    def khat(self):
+        n = self.grid[0] * self.grid[1] * self.grid[2]
+        return np.ctypeslib.as_array(self.lib().pmeo_khat(self.h), (n,)).copy().reshape(self.grid)
+
+    def err_est(self):
+        return self.lib().pmeo_errEst(self.h, _ptr(self.q))
+
+    def __del__(self):
+        if getattr(self, "h", None) and self._lib is not None:
+            self._lib.pmeo_destroy(self.h)
+            self.h = None
+
+
+REF_PME_SO = os.path.join(HERE, "_ref", "libpme_ref.so")
+
+
+class PmeStruct(C.Structure):
+    """struct FF of the reference's code/pme.h:16-44."""
+    _fields_ = [
+        ("N", C.c_int), ("q", _dp), ("A", C.c_double * 9), ("Ai", C.c_double * 9),
+        ("detA", C.c_double), ("cutoff", C.c_double), ("orderAcc", C.c_int),
+        ("topGridDim", C.c_int * 3), ("nlist", _ip), ("nlist_len", C.c_int),
+        ("nlist_interaction_count", C.c_int), ("tolDir", C.c_double),
+        ("fftw_in", C.c_void_p), ("forward", C.c_void_p), ("backward", C.c_void_p),
+        ("beta", C.c_double), ("Q", _dp), ("cL", _dp * 3), ("khat", _dp),
+        ("coeff1", C.c_double), ("coeff2", C.c_double),
+        ("time_partcl2partcl", C.c_double), ("time_nlist", C.c_double),
+        ("time_grid2grid", C.c_double), ("time_stencil", C.c_double),
+        ("time_anterpolation", C.c_double), ("time_interpolation", C.c_double),
+    ]
+
+
+def bind_pme_api(lib, struct=PmeStruct):
+    """Signatures of the PME C API (code/pme.h:45-68)."""
+    P = C.POINTER(struct)
+    sig = {
+        "FF_new": (P, [C.c_int, _dp, _dp]),
+        "FF_set_cutoff": (None, [P, C.c_double]),
+        "FF_set_orderAcc": (None, [P, C.c_int]),
+        "FF_set_topGridDim": (None, [P, _ip]),
+        "FF_set_tolDir": (None, [P, C.c_double]),
+        "FF_build": (None, [P, _dp]),
+        "FF_get_cutoff": (C.c_double, [P]),
+        "FF_get_orderAcc": (C.c_int, [P]),
+        "FF_get_topGridDim": (None, [P, _ip]),
+        "FF_get_tolDir": (C.c_double, [P]),
+        "FF_get_errEst": (C.c_double, [P, C.c_int, _dp]),
+        "FF_rebuild": (None, [P, _dp, _dp]),
+        "FF_energy": (C.c_double, [P, _dp, _dp, _dp]),
+        "FF_delete": (None, [P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+class RefPme:
+    """The reference PME library (oracle/_ref/libpme_ref.so, built from
+    code/pme0.c and code/pme1.c) through its own C API."""
+
+    _lib = None
+
+    @classmethod
+    def available(cls):
+        return os.path.exists(REF_PME_SO)
+
+    @classmethod
+    def lib(cls):
+        if cls._lib is None:
+            if not os.path.exists(REF_PME_SO):
+                raise FileNotFoundError(REF_PME_SO + " (run oracle/build_ref.py)")
+            cls._lib = bind_pme_api(C.CDLL(REF_PME_SO))
+        return cls._lib
+
+    def __init__(self, q, pos, edges, cutoff=None, nu=None, grid=None, tol_dir=None):
+        lib = self.lib()
+        self.q = _f64(q).copy()
+        self.N = len(self.q)
+        self.edges = _f64(np.asarray(edges).reshape(3, 3)).copy()
+        self.pos = _f64(pos).copy()
+        self.ff = lib.FF_new(self.N, _ptr(self.q), _ptr(self.edges))
+        if cutoff is not None:
+            lib.FF_set_cutoff(self.ff, float(cutoff))
+        if grid is not None:
+            self._g = np.ascontiguousarray(np.broadcast_to(np.asarray(grid), (3,)),
+                                           dtype=np.int32)
+            lib.FF_set_topGridDim(self.ff, _ptr(self._g, C.c_int))
+        if nu is not None:
+            lib.FF_set_orderAcc(self.ff, int(nu))
+        if tol_dir is not None:
+            lib.FF_set_tolDir(self.ff, float(tol_dir))
+        lib.FF_build(self.ff, _ptr(self.pos))
+        s = self.ff.contents
+        self.cutoff, self.nu, self.grid = s.cutoff, s.orderAcc, tuple(s.topGridDim)
+        self.tol_dir, self.beta = s.tolDir, s.beta
+
+    def energy(self, pos=None):
+        pos = self.pos if pos is None else _f64(pos)
+        f = np.zeros((self.N, 3))
+        e = self._lib.FF_energy(self.ff, _ptr(f), _ptr(pos), None)
+        return e, f
+
+    def err_est(self):
+        return self._lib.FF_get_errEst(self.ff, self.N, _ptr(self.q))
+
+    def struct(self):
+        return self.ff.contents
+
+    def khat(self):
+        g = self.grid
+        return np.ctypeslib.as_array(self.ff.contents.khat, (g[0] * g[1] * g[2],)).copy().reshape(g)
+
+    def close(self):
+        if getattr(self, "ff", None):
             self._lib.FF_delete(self.ff)
             self.ff = None
 
