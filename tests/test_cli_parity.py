@@ -103,3 +103,55 @@ def test_cli_driver_parity(tmp_path, case, explicit, precision):
             assert abs(ov[k] - v) <= tol * energies[k], (k, ov[k], v)
         else:  # set-up figures that do not depend on the arithmetic
             assert abs(ov[k] - v) <= 1e-12 * max(abs(v), 1e-300), (k, ov[k], v)
+
+
+# ---- the PME comparator's driver (code/pme.c) ----
+PME_REF = os.path.join(ROOT, "oracle", "_ref", "pme_ref")
+PME_DROPIN = os.path.join(ROOT, "oracle", "_ref", "pme_dropin")
+PME_GOLDEN = os.path.join(ROOT, "tests", "golden", "pme")
+# keys that depend only on the inputs and the parameter choice
+PME_EXACT = ("data", "nu", "beta", "TopLevelMx", "TopLevelMy", "TopLevelMz", "NumberOfLevels",
+             "Edge row1", "Edge row2", "Edge row3", "cutoff", "nbar", "tol_dir", "detA",
+             "fref", "uref", "Q2", "uintra")
+# driver arguments per fixture (code/pme.c:40-58; --nu is parsed into a
+# shadowing local there, so the order stays at its default in both builds)
+PME_ARGS = {"spceN300_auto": [], "spceN900_a7_tol1e-6": ["--a0", "7.0", "--tol-dir", "1e-6"],
+            "spceN2250_a10_M32": ["--a0", "10.0", "-M", "32"],
+            "spceN600_a9_nu4": ["--a0", "9.0"]}
+# (the driver sums an intramolecular energy over consecutive atom triples,
+# code/pme.c:235-260, reading past the arrays unless N is a multiple of 3:
+# only the water boxes are driven through it)
+
+
+@pytest.mark.skipif(not (os.path.exists(PME_REF) and os.path.exists(PME_DROPIN)),
+                    reason="reference PME drivers not built (oracle/build_ref.py)")
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", sorted(PME_ARGS))
+def test_pme_cli_driver_parity(tmp_path, case, precision):
+    d = dict(np.load(os.path.join(PME_GOLDEN, case + ".npz")))
+    base = str(tmp_path / case)
+    write_inputs(d, base)
+    env = dict(os.environ)
+    env["MSMPB_PRECISION"] = precision
+    ref = run(PME_REF, base, PME_ARGS[case], env)
+    ours = run(PME_DROPIN, base, PME_ARGS[case], env)
+    assert [k for k, _ in ours] == [k for k, _ in ref]
+    rv, ov = dict(ref), dict(ours)
+    tol = 1e-10 if precision == "fp64" else 1e-5
+    u = abs(rv["utotal"])
+    fscale = max(rv["fref"], float(np.sqrt((d["force"] ** 2).sum() / len(d["q"]))))
+    for k, v in rv.items():
+        if k.startswith(("time_", "nlist_")):
+            continue
+        if k in PME_EXACT:
+            assert ov[k] == v, k
+        elif k in ("utotal", "utotal_kcal_mol", "potabserror"):
+            scale = 332.0636 * u if k == "utotal_kcal_mol" else u
+            assert abs(ov[k] - v) <= tol * scale, (k, ov[k], v)
+        elif k in ("deltaF", "deltaF/Fref"):
+            s = fscale if k == "deltaF" else fscale / rv["fref"]
+            assert abs(ov[k] - v) <= 10 * tol * s, (k, ov[k], v)
+        elif k == "poterror":
+            assert abs(ov[k] - v) <= tol, (k, ov[k], v)
+        else:
+            raise AssertionError("unchecked key %s" % k)
