@@ -420,6 +420,41 @@ def batch_timing(dev, torch, flush, reps=10, warmup=3, precisions=("mixed", "fp6
     return out
 
 
+def pme_timing(q, pos, edges, pos_d, q_d, f_d, phi_d, e_d, torch, flush, f_hi, e_hi,
+               msm_ms, msm64_ms, reps=10):
+    """The reference's comparator method, smooth PME with its default
+    parameters (a0 = 9 A here as for MSM, order 6, tolDir 1e-5, grid from
+    its spacing table), on the same box: time per evaluation in both
+    precisions and force error against the same high-accuracy MSM
+    reference as the MSM numbers."""
+    from msmpb_b200.pme import PME
+    out = {}
+    for prec in ("mixed", "fp64"):
+        p = PME(q, pos, edges, cutoff=9.0, precision=prec, device=pos_d.device.index)
+        p.set_timing(False)
+        t = time_device(p, pos_d, q_d, f_d, phi_d, e_d, reps, 3, torch, flush)
+        out["%s_ms" % prec] = round(float(np.mean(t)), 4)
+        out["grid"] = list(p.grid)
+        out["beta"] = p.beta
+        if f_hi is not None:
+            f = f_d.cpu().numpy()
+            out["%s_force_rms_rel" % prec] = float(np.sqrt(((f - f_hi) ** 2).sum() /
+                                                           (f_hi ** 2).sum()))
+            out["%s_energy_rel" % prec] = abs(float(e_d.item()) - e_hi) / abs(e_hi)
+        p.set_timing(True)
+        p.energy_device(pos_d.data_ptr(), q_d.data_ptr(), f_d.data_ptr(), phi_d.data_ptr(),
+                        e_d.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        out["%s_phase_ms" % prec] = {k: round(v, 4) for k, v in p.phase_times().items()}
+        p.close()
+    out["msm_mixed_ms"] = round(msm_ms, 4)
+    out["msm_fp64_ms"] = round(msm64_ms, 4)
+    out["note"] = ("smooth PME (code/pme0.c, pme1.c defaults: order 6, tolDir 1e-5, default "
+                   "grid) at a0 = 9 A on the same box and inputs; errors against the "
+                   "high-accuracy MSM reference of the accuracy block")
+    return out
+
+
 def time_device(ff, pos_d, q_d, f_d, phi_d, e_d, steps, warmup, torch, flush):
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
@@ -515,6 +550,7 @@ def run_ours(args):
 
     # ---- accuracy against a high-accuracy FP64 MSM (nu=10, a0=12, h=1.0) ----
     acc = None
+    f_hi = e_hi = None
     if not args.skip_accuracy:
         ffh = ForceField(q, pos, edges, order=10, cutoff=12.0, levels=1, top_grid=216,
                          precision="fp64", device=local)
@@ -536,6 +572,10 @@ def run_ours(args):
                "energy_rel_mixed": abs(e_mixed - e_hi) / abs(e_hi),
                "mixed_vs_fp64_force_rms_rel": float(
                    np.sqrt(((f_mixed - f_fp64) ** 2).sum()) / np.sqrt((f_fp64 ** 2).sum()))}
+
+    # ---- the smooth-PME comparator on the same box (cost and error) ----
+    pme = None if args.skip_pme else pme_timing(q, pos, edges, pos_d, q_d, f_d, phi_d, e_d,
+                                                torch, flush, f_hi, e_hi, ms, ms64)
 
     # ---- end to end through the host C ABI, pinned host arrays ----
     pos_h = torch.from_numpy(pos.copy()).pin_memory()
@@ -595,6 +635,7 @@ def run_ours(args):
         "box_change": rebuild,
         "adjoint": adjoint,
         "batch": batch,
+        "pme": pme,
         "gpu_launches": launches, "clocks": clocks,
     }
     if rank == 0:
@@ -728,6 +769,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--skip-batch", action="store_true")
+    ap.add_argument("--skip-pme", action="store_true")
     ap.add_argument("--only-batch", action="store_true",
                     help="time only the many-systems batch (steps = timed replays)")
     ap.add_argument("--batch-precision", default="mixed,fp64")
