@@ -15,170 +15,11 @@
 namespace msm {
 namespace {
 
-constexpr int kThreads = 256;
 constexpr int kMaxFactors = 24;
 constexpr int kMaxRadix = 64;
 
-struct FftLines {
-  int n;        // line length
-  int nlines;   // number of lines
-  int inner;    // element stride of a line (product of the faster dims)
-  int lpb;      // lines per block
-  int nf;       // number of radix stages
-  int radix[kMaxFactors];
-};
-
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-
-// exp(sign * 2 pi i * num / den), argument reduced exactly
-__device__ __forceinline__ double2 twiddle(int sign, long num, long den) {
-  long r = num % den;
-  double s, c;
-  sincospi(2.0 * (double)r / (double)den, &s, &c);
-  return make_double2(c, sign * s);
-}
-
-// One radix stage over every line held in shared memory
-__device__ void stockham_stage(const FftLines &f, int R, int Ns, int sign,
-                               const double2 *src, double2 *dst) {
-  const int n = f.n, m = n / R;
-  double2 v[kMaxRadix], y[kMaxRadix];
-  for (int t = threadIdx.x; t < f.lpb * m; t += blockDim.x) {
-    const int line = t / m, j = t % m;
-    const double2 *s = src + line * n;
-    double2 *d = dst + line * n;
-    const int k = j % Ns;
-    for (int r = 0; r < R; ++r) {
-      double2 a = s[j + r * m];
-      v[r] = r == 0 ? a : cmul(a, twiddle(sign, (long)k * r, (long)Ns * R));
-    }
-    if (R == 2) {
-      y[0] = make_double2(v[0].x + v[1].x, v[0].y + v[1].y);
-      y[1] = make_double2(v[0].x - v[1].x, v[0].y - v[1].y);
-    } else if (R == 4) {
-      double2 a0 = make_double2(v[0].x + v[2].x, v[0].y + v[2].y);
-      double2 a1 = make_double2(v[0].x - v[2].x, v[0].y - v[2].y);
-      double2 b0 = make_double2(v[1].x + v[3].x, v[1].y + v[3].y);
-      double2 b1 = make_double2(v[1].x - v[3].x, v[1].y - v[3].y);
-      // multiply b1 by sign * i
-      double2 b1i = make_double2(-sign * b1.y, sign * b1.x);
-      y[0] = make_double2(a0.x + b0.x, a0.y + b0.y);
-      y[2] = make_double2(a0.x - b0.x, a0.y - b0.y);
-      y[1] = make_double2(a1.x + b1i.x, a1.y + b1i.y);
-      y[3] = make_double2(a1.x - b1i.x, a1.y - b1i.y);
-    } else {
-      for (int q = 0; q < R; ++q) {
-        double2 acc = v[0];
-        for (int r = 1; r < R; ++r) {
-          double2 w = twiddle(sign, (long)r * q, R);
-          double2 p = cmul(v[r], w);
-          acc.x += p.x;
-          acc.y += p.y;
-        }
-        y[q] = acc;
-      }
-    }
-    const int base = (j / Ns) * Ns * R + k;
-    for (int r = 0; r < R; ++r) d[base + r * Ns] = y[r];
-  }
-}
-
-// Runs the stages of one direction; returns the buffer holding the result.
-__device__ double2 *run_stages(const FftLines &f, int sign, double2 *a,
-                               double2 *b) {
-  int Ns = 1;
-  for (int s = 0; s < f.nf; ++s) {
-    const int R = f.radix[s];
-    stockham_stage(f, R, Ns, sign, a, b);
-    __syncthreads();
-    double2 *t = a;
-    a = b;
-    b = t;
-    Ns *= R;
-  }
-  return a;
-}
-
-__device__ __forceinline__ long line_elem(const FftLines &f, int gline, int e) {
-  return (long)(gline / f.inner) * ((long)f.n * f.inner) + gline % f.inner +
-         (long)e * f.inner;
-}
-
-// mode 0: complex in -> forward -> complex out
-// mode 1: real T in -> forward -> complex out
-// mode 2: complex in -> forward, * (w khat), inverse -> complex out
-// mode 3: complex in -> inverse -> real T out (scaled)
-// mode 4: complex in -> inverse -> complex out
-template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_fft_pass(FftLines f, int mode, const T *__restrict__ rin,
-           const double2 *in, double2 *out, const double *__restrict__ khat,
-           double w, T *__restrict__ rout, double scale) {
-  extern __shared__ double2 smem[];
-  double2 *a = smem, *b = smem + f.lpb * f.n;
-  const int line0 = blockIdx.x * f.lpb;
-  for (int t = threadIdx.x; t < f.lpb * f.n; t += blockDim.x) {
-    const int line = t / f.n, e = t % f.n, g = line0 + line;
-    double2 v = make_double2(0., 0.);
-    if (g < f.nlines) {
-      const long gi = line_elem(f, g, e);
-      v = (mode == 1) ? make_double2((double)rin[gi], 0.) : in[gi];
-    }
-    a[t] = v;
-  }
-  __syncthreads();
-  const int sign = (mode >= 3) ? +1 : -1;
-  double2 *res = run_stages(f, sign, a, b);
-  if (mode == 2) {
-    for (int t = threadIdx.x; t < f.lpb * f.n; t += blockDim.x) {
-      const int line = t / f.n, e = t % f.n, g = line0 + line;
-      if (g < f.nlines) {
-        const double kv = w * khat[line_elem(f, g, e)];
-        res[t].x *= kv;
-        res[t].y *= kv;
-      }
-    }
-    __syncthreads();
-    double2 *other = (res == a) ? b : a;
-    res = run_stages(f, +1, res, other);
-  }
-  for (int t = threadIdx.x; t < f.lpb * f.n; t += blockDim.x) {
-    const int line = t / f.n, e = t % f.n, g = line0 + line;
-    if (g >= f.nlines) continue;
-    const long gi = line_elem(f, g, e);
-    if (mode == 3)
-      rout[gi] = (T)(res[t].x * scale);
-    else
-      out[gi] = res[t];
-  }
-}
-
-FftLines make_lines(int n, int nlines, int inner) {
-  FftLines f{};
-  f.n = n;
-  f.nlines = nlines;
-  f.inner = inner;
-  int r = n;
-  while (r % 4 == 0 && f.nf < kMaxFactors) { f.radix[f.nf++] = 4; r /= 4; }
-  for (int p : {2, 3, 5, 7})
-    while (r % p == 0 && f.nf < kMaxFactors) { f.radix[f.nf++] = p; r /= p; }
-  for (int p = 11; r > 1 && f.nf < kMaxFactors; p += 2)
-    while (r % p == 0 && f.nf < kMaxFactors) { f.radix[f.nf++] = p; r /= p; }
-  int lpb = std::max(1, 1024 / std::max(1, n));
-  f.lpb = std::min(lpb, nlines);
-  return f;
-}
-
-template <typename T>
-void run_pass(cudaStream_t s, const FftLines &f, int mode, const T *rin,
-              const double2 *in, double2 *out, const double *khat, double w,
-              T *rout, double scale) {
-  size_t smem = 2 * (size_t)f.lpb * f.n * sizeof(double2);
-  int blocks = (f.nlines + f.lpb - 1) / f.lpb;
-  k_fft_pass<T><<<blocks, kThreads, smem, s>>>(f, mode, rin, in, out, khat, w,
-                                               rout, scale);
 }
 
 // ---------------------------------------------------------------------------
@@ -197,12 +38,16 @@ struct FftAxis {
   int radix[kMaxFactors];
 };
 
+// radix 4 first, then 2, 3, 5, 7, then any other prime
 FftAxis make_axis(int n) {
-  FftLines l = make_lines(n, 1, 1);
   FftAxis a{};
   a.n = n;
-  a.nf = l.nf;
-  for (int i = 0; i < l.nf; ++i) a.radix[i] = l.radix[i];
+  int r = n;
+  while (r % 4 == 0 && a.nf < kMaxFactors) { a.radix[a.nf++] = 4; r /= 4; }
+  for (int p : {2, 3, 5, 7})
+    while (r % p == 0 && a.nf < kMaxFactors) { a.radix[a.nf++] = p; r /= p; }
+  for (int p = 11; r > 1 && a.nf < kMaxFactors; p += 2)
+    while (r % p == 0 && a.nf < kMaxFactors) { a.radix[a.nf++] = p; r /= p; }
   return a;
 }
 
@@ -411,20 +256,108 @@ k_fft_xlines(FftAxis ax, int nlines, const double *__restrict__ khat, double w, 
   }
 }
 
+// Larger grids: one launch per axis pass. A CTA transforms L lines of
+// length n along one axis (element e of line g at base(g) + e * inner, with
+// base(g) = (g / inner) n inner + g % inner). Lines g, g+1 are adjacent in
+// memory when inner > 1, so threads take consecutive lines; rows (inner ==
+// 1) are read along the row and transposed into shared memory through a
+// pitch of L + 1. Modes: 0 forward, 1 real T in then forward, 2 forward,
+// times w khat, inverse, 3 inverse then real T out (scaled), 4 inverse.
+constexpr int kLineSmemMax = 200 * 1024;
+
+struct LineShape {
+  int L, LP;  // lines per CTA, shared-memory pitch between elements
+};
+
+// The most lines (<= 32) that keep three CTAs on an SM (<= 72 KB each),
+// else the most that fit at all
+LineShape line_shape(int n, int inner) {
+  for (size_t cap : {(size_t)72 * 1024, (size_t)kLineSmemMax})
+    for (int L = 32; L > 1; L >>= 1) {
+      const int LP = inner == 1 ? L + 1 : L;
+      if ((2 * (size_t)LP * n + n) * sizeof(double2) <= cap) return {L, LP};
+    }
+  return {1, 1};
+}
+
+size_t line_smem(int n, const LineShape &ls) {
+  return (2 * (size_t)ls.LP * n + n) * sizeof(double2);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kPlaneThreads)
+k_fft_lines(FftAxis ax, int nlines, int inner, LineShape ls, int mode, const T *__restrict__ rin,
+            double2 *buf, const double *__restrict__ khat, double w, T *__restrict__ rout,
+            double scale) {
+  extern __shared__ double2 smem[];
+  const int n = ax.n, L = ls.L, LP = ls.LP;
+  double2 *a = smem, *b = smem + LP * n, *W = smem + 2 * LP * n;
+  root_table(n, W);
+  const int line0 = blockIdx.x * L;
+  const bool rows = inner == 1;
+  auto gaddr = [&](int g, int e) -> long {
+    return (long)(g / inner) * ((long)n * inner) + g % inner + (long)e * inner;
+  };
+  for (int t = threadIdx.x; t < L * n; t += blockDim.x) {
+    const int l = rows ? t / n : t % L, e = rows ? t % n : t / L, g = line0 + l;
+    double2 v = make_double2(0., 0.);
+    if (g < nlines) {
+      const long gi = gaddr(g, e);
+      v = mode == 1 ? make_double2((double)rin[gi], 0.) : buf[gi];
+    }
+    a[e * LP + l] = v;
+  }
+  __syncthreads();
+  double2 *res = axis_fft(ax, L, 1, LP, true, mode >= 3 ? +1 : -1, W, a, b);
+  if (mode == 2) {
+    for (int t = threadIdx.x; t < L * n; t += blockDim.x) {
+      const int l = rows ? t / n : t % L, e = rows ? t % n : t / L, g = line0 + l;
+      const double kv = g < nlines ? w * khat[gaddr(g, e)] : 0.;
+      double2 &v = res[e * LP + l];
+      v.x *= kv;
+      v.y *= kv;
+    }
+    __syncthreads();
+    double2 *o = res == a ? b : a;
+    res = axis_fft(ax, L, 1, LP, true, +1, W, res, o);
+  }
+  for (int t = threadIdx.x; t < L * n; t += blockDim.x) {
+    const int l = rows ? t / n : t % L, e = rows ? t % n : t / L, g = line0 + l;
+    if (g >= nlines) continue;
+    const long gi = gaddr(g, e);
+    const double2 v = res[e * LP + l];
+    if (mode == 3)
+      rout[gi] = (T)(v.x * scale);
+    else
+      buf[gi] = v;
+  }
+}
+
+template <typename T>
+void line_pass(cudaStream_t s, int n, int nlines, int inner, int mode, const T *rin,
+               double2 *buf, const double *khat, double w, T *rout, double scale) {
+  const FftAxis ax = make_axis(n);
+  const LineShape ls = line_shape(n, inner);
+  const int blocks = (nlines + ls.L - 1) / ls.L;
+  k_fft_lines<T><<<blocks, kPlaneThreads, line_smem(n, ls), s>>>(ax, nlines, inner, ls, mode, rin,
+                                                                buf, khat, w, rout, scale);
+}
+
 bool plane_path(const int M[3]) {
   return plane_smem(M) <= kPlaneSmemMax && xlines_smem(M[0]) <= kPlaneSmemMax;
 }
 
 }  // namespace
 
-// One-time kernel attribute: lines up to 4096 points need 128 KB of
-// shared memory (two buffers of one line). Called outside stream capture.
+// One-time kernel attributes (a line of up to 4096 points with its twiddle
+// table needs 192 KB of shared memory). Called outside stream capture.
 void top_solve_prepare() {
   static bool done = false;
   if (done) return;
-  const int bytes = 2 * 4096 * (int)sizeof(double2);
-  cudaFuncSetAttribute(k_fft_pass<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_fft_pass<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_fft_lines<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kLineSmemMax);
+  cudaFuncSetAttribute(k_fft_lines<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       kLineSmemMax);
   cudaFuncSetAttribute(k_fft_plane<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kPlaneSmemMax);
   cudaFuncSetAttribute(k_fft_plane<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -465,15 +398,11 @@ void launch_top_solve(cudaStream_t s, const int M[3], const T *q,
     k_fft_plane<T><<<M0, kPlaneThreads, ps, s>>>(ay, az, 1, nullptr, buf0, e, scale);
     return;
   }
-  FftLines fz = make_lines(M2, M0 * M1, 1);
-  FftLines fy = make_lines(M1, M0 * M2, M2);
-  FftLines fx = make_lines(M0, M1 * M2, M1 * M2);
-  run_pass<T>(s, fz, 1, q, nullptr, buf0, nullptr, 0., nullptr, 0.);
-  run_pass<T>(s, fy, 0, nullptr, buf0, buf0, nullptr, 0., nullptr, 0.);
-  run_pass<T>(s, fx, 2, nullptr, buf0, buf0, khat, weight, nullptr, 0.);
-  FftLines iy = fy;
-  run_pass<T>(s, iy, 4, nullptr, buf0, buf0, nullptr, 0., nullptr, 0.);
-  run_pass<T>(s, fz, 3, nullptr, buf0, nullptr, nullptr, 0., e, scale);
+  line_pass<T>(s, M2, M0 * M1, 1, 1, q, buf0, nullptr, 0., nullptr, 0.);
+  line_pass<T>(s, M1, M0 * M2, M2, 0, nullptr, buf0, nullptr, 0., nullptr, 0.);
+  line_pass<T>(s, M0, M1 * M2, M1 * M2, 2, nullptr, buf0, khat, weight, nullptr, 0.);
+  line_pass<T>(s, M1, M0 * M2, M2, 4, nullptr, buf0, nullptr, 0., nullptr, 0.);
+  line_pass<T>(s, M2, M0 * M1, 1, 3, nullptr, buf0, nullptr, 0., e, scale);
 }
 
 template void launch_top_solve<float>(cudaStream_t, const int *, const float *,

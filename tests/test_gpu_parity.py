@@ -201,6 +201,24 @@ def test_box_smaller_than_cutoff(variant, monkeypatch):
             ff.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_large_top_grid(precision):
+    """A one-level plan whose top grid (96 x 90 x 98) is too large for the
+    plane-staged FFT: the five line passes of the large-grid path, against
+    the oracle's FFT."""
+    q, pos, edges = systems.water(400, 24.0, 11)
+    o = Oracle(q, edges, cutoff=8.0, nu=6, levels=1, top_grid=[96, 90, 98])
+    eo, fo, po = o.energy(pos)
+    ff = ForceField(q, pos, edges, cutoff=8.0, order=6, levels=1, top_grid=(96, 90, 98),
+                    precision=precision)
+    e, f, phi = ff.energy(pos, potentials=True)
+    te, tf, tp = TOL[precision]
+    assert abs(e - eo) / abs(eo) < te
+    assert force_err(f, fo, q, edges) < tf
+    assert rel_rms(phi, po) < tp
+    ff.close()
+
+
 def test_repeat_and_charge_update():
     """Repeated calls give identical results; charge edits between calls
     are seen (FF_new keeps the caller's pointer, code/forcefield0.c:172)."""
