@@ -338,7 +338,7 @@ def box_change_timing(ff, edges, pos, pos_d, q_d, f_d, phi_d, e_d, torch, reps=5
 
 
 def batch_timing(dev, torch, flush, reps=10, warmup=3, precisions=("mixed", "fp64"),
-                 branches=0, per_system=True):
+                 branches=0, per_system=True, count=256):
     """Many independent systems in one graph launch against per-system
     launches: 256 charge-neutral +-1 ion boxes, N uniform in [500, 20000],
     density 0.1 / A^3, 2 A minimum separation, order cycled over 4/6/8,
@@ -348,7 +348,7 @@ def batch_timing(dev, torch, flush, reps=10, warmup=3, precisions=("mixed", "fp6
     from msmpb_b200 import systems
     from msmpb_b200.forcefield import Batch, ForceField
     t0 = time.perf_counter()
-    sysl = systems.ion_batch(256, seed=5, workers=min(8, os.cpu_count() or 1))
+    sysl = systems.ion_batch(count, seed=5, workers=min(8, os.cpu_count() or 1))
     gen_s = time.perf_counter() - t0
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
@@ -421,7 +421,7 @@ def batch_timing(dev, torch, flush, reps=10, warmup=3, precisions=("mixed", "fp6
 
 
 def pme_timing(q, pos, edges, pos_d, q_d, f_d, phi_d, e_d, torch, flush, f_hi, e_hi,
-               msm_ms, msm64_ms, reps=10):
+               msm_ms, msm64_ms, reps=10, warmup=3, precisions=("mixed", "fp64")):
     """The reference's comparator method, smooth PME with its default
     parameters (a0 = 9 A here as for MSM, order 6, tolDir 1e-5, grid from
     its spacing table), on the same box: time per evaluation in both
@@ -429,10 +429,10 @@ def pme_timing(q, pos, edges, pos_d, q_d, f_d, phi_d, e_d, torch, flush, f_hi, e
     reference as the MSM numbers."""
     from msmpb_b200.pme import PME
     out = {}
-    for prec in ("mixed", "fp64"):
+    for prec in precisions:
         p = PME(q, pos, edges, cutoff=9.0, precision=prec, device=pos_d.device.index)
         p.set_timing(False)
-        t = time_device(p, pos_d, q_d, f_d, phi_d, e_d, reps, 3, torch, flush)
+        t = time_device(p, pos_d, q_d, f_d, phi_d, e_d, reps, warmup, torch, flush)
         out["%s_ms" % prec] = round(float(np.mean(t)), 4)
         out["grid"] = list(p.grid)
         out["beta"] = p.beta
@@ -447,8 +447,9 @@ def pme_timing(q, pos, edges, pos_d, q_d, f_d, phi_d, e_d, torch, flush, f_hi, e
         torch.cuda.synchronize()
         out["%s_phase_ms" % prec] = {k: round(v, 4) for k, v in p.phase_times().items()}
         p.close()
-    out["msm_mixed_ms"] = round(msm_ms, 4)
-    out["msm_fp64_ms"] = round(msm64_ms, 4)
+    if np.isfinite(msm_ms):
+        out["msm_mixed_ms"] = round(msm_ms, 4)
+        out["msm_fp64_ms"] = round(msm64_ms, 4)
     out["note"] = ("smooth PME (code/pme0.c, pme1.c defaults: order 6, tolDir 1e-5, default "
                    "grid) at a0 = 9 A on the same box and inputs; errors against the "
                    "high-accuracy MSM reference of the accuracy block")
@@ -489,7 +490,8 @@ def run_ours(args):
         flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
         out = batch_timing(dev, torch, flush, reps=args.steps, warmup=args.warmup,
                            precisions=args.batch_precision.split(","),
-                           branches=args.batch_branches, per_system=not args.batch_only_graph)
+                           branches=args.batch_branches, per_system=not args.batch_only_graph,
+                           count=args.batch_systems)
         if rank == 0:
             print(json.dumps({"batch": out}))
         if pg is not None:
@@ -498,6 +500,21 @@ def run_ours(args):
     q, pos, edges, kw = workload(WORKLOAD)
     N = len(q)
     lib = _lib.load()
+    if args.only_pme:
+        flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+        pos_d = torch.from_numpy(pos).to(dev)
+        q_d = torch.from_numpy(q).to(dev)
+        f_d = torch.zeros((N, 3), dtype=torch.float64, device=dev)
+        phi_d = torch.zeros(N, dtype=torch.float64, device=dev)
+        e_d = torch.zeros(1, dtype=torch.float64, device=dev)
+        out = pme_timing(q, pos, edges, pos_d, q_d, f_d, phi_d, e_d, torch, flush, None, None,
+                         float("nan"), float("nan"), reps=args.steps, warmup=args.warmup,
+                         precisions=args.batch_precision.split(","))
+        if rank == 0:
+            print(json.dumps({"pme": out}))
+        if pg is not None:
+            pg.destroy_process_group()
+        return 0
 
     ff = ForceField(q, pos, edges, **kw, precision="mixed", device=local)
     ff.set_timing(False)
@@ -773,12 +790,17 @@ def main():
     ap.add_argument("--only-batch", action="store_true",
                     help="time only the many-systems batch (steps = timed replays)")
     ap.add_argument("--batch-precision", default="mixed,fp64")
+    ap.add_argument("--batch-systems", type=int, default=256)
+    ap.add_argument("--only-pme", action="store_true",
+                    help="time only the PME comparator on the 1M-atom box")
     ap.add_argument("--batch-branches", type=int, default=0, help="0 = tuned")
     ap.add_argument("--batch-only-graph", action="store_true",
                     help="skip the per-system launch comparison")
     ap.add_argument("--ref-procs", type=int, default=0)
     args = ap.parse_args()
-    if args.warmup < 3 and args.impl == "ours":
+    # the headline keeps >= 3 warm-up steps; the single-section modes exist
+    # for short profiler runs and take what they are given
+    if args.warmup < 3 and args.impl == "ours" and not (args.only_batch or args.only_pme):
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
