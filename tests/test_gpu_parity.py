@@ -219,6 +219,38 @@ def test_large_top_grid(precision):
     ff.close()
 
 
+TINY = [  # (N, order, top grid, levels, cutoff)
+    (2, 4, 4, 1, 4.0), (3, 6, 6, 1, 4.5), (8, 8, 8, 1, 5.0), (33, 10, 8, 1, 5.0),
+    (8, 10, 4, 1, 4.0), (33, 6, 4, 2, 4.0), (33, 4, 4, 3, 3.0), (16, 8, 6, 2, 4.5),
+]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("n,nu,m,levels,a0", TINY)
+def test_tiny_systems(n, nu, m, levels, a0, precision):
+    """Few atoms (ragged clusters of 2..33), every order, grids smaller than
+    the B-spline order (charges wrap several times), up to three levels,
+    atoms given outside the primary box (the reference wraps fractional
+    coordinates, code/forcefield1.c:349-352)."""
+    rng = np.random.default_rng(100 * n + nu)
+    edges = np.diag([10.0, 11.0, 9.5])
+    q = rng.uniform(-1, 1, n)
+    if n > 1:
+        q -= q.mean()
+    pos = rng.uniform(0, 1, (n, 3)) @ edges.T
+    pos[::2] += edges @ rng.integers(-2, 3, (3,))  # some atoms a few boxes away
+    o = Oracle(q, edges, cutoff=a0, nu=nu, levels=levels, top_grid=[m, m, m])
+    eo, fo, po = o.energy(pos)
+    ff = ForceField(q, pos, edges, cutoff=a0, order=nu, levels=levels, top_grid=m,
+                    precision=precision)
+    e, f, phi = ff.energy(pos, potentials=True)
+    te, tf, tp = TOL[precision]
+    assert abs(e - eo) <= te * max(abs(eo), 1e-3)
+    assert force_err(f, fo, q, edges) < tf
+    assert rel_rms(phi, po) < tp
+    ff.close()
+
+
 def test_repeat_and_charge_update():
     """Repeated calls give identical results; charge edits between calls
     are seen (FF_new keeps the caller's pointer, code/forcefield0.c:172)."""
