@@ -15,8 +15,11 @@ extern "C" {
 
 /* Status codes (FF_last_error and int-returning entry points). The
  * reference prints and continues, or exits (code/forcefield0.c:152,
- * :210-213); this library never exits, never traps the GPU, and records the
- * first failure of a call here. */
+ * :210-213); this library never exits and never traps the GPU. FF_last_error
+ * holds the status of the latest working call (FF_build, FF_rebuild,
+ * FF_rebuild_device, FF_energy, FF_energy_potentials, FF_energy_device,
+ * FF_adjoint_device, FF_sync): each clears it first. Device-side checks of an
+ * asynchronous evaluation surface at the next call or at FF_sync. */
 #define MSMPB_OK 0
 #define MSMPB_ERR_ARGUMENT 1     /* invalid size, pointer or parameter */
 #define MSMPB_ERR_STATE 2        /* call order violated (e.g. energy before build) */
@@ -133,7 +136,8 @@ int FF_batch_energy_device(FFBatch *batch, const double *const *position_d,
                            double *energy_d, void *stream);
 
 /* Branches of the current graph (after tuning: the chosen count), kernels
- * it launches, the first error of the batch's calls; and release. */
+ * it launches, the status of the latest FF_batch_energy_device call; and
+ * release. */
 int FF_batch_branches(const FFBatch *batch);
 int FF_batch_kernel_launches(const FFBatch *batch);
 int FF_batch_last_error(const FFBatch *batch);

@@ -24,6 +24,10 @@ extern "C" {
 /* MIXED: direct-space sum (erfc kernel), charge assignment and
  * interpolation in FP32 with compensated per-atom sums, close pairs in FP64;
  * FFT, multiplier, energy sums and constant terms in FP64. FP64: all FP64. */
+/* FF_last_error: the status of the latest working call (FF_build,
+ * FF_rebuild, FF_energy, FF_energy_potentials, FF_energy_device, FF_sync),
+ * each of which clears it first. */
+
 #define MSMPB_PRECISION_MIXED 0
 #define MSMPB_PRECISION_FP64 1
 

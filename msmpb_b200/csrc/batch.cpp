@@ -263,6 +263,7 @@ int FF_batch_energy_device(FFBatch *b, const double *const *position_d,
                            double *const *force_d, double *const *potential_d,
                            double *energy_d, void *stream) {
   if (!b) return MSMPB_ERR_ARGUMENT;
+  b->last_error = MSMPB_OK;  // the status of this call
   if (!position_d || !charge_d) return fail(b, MSMPB_ERR_ARGUMENT);
   for (size_t i = 0; i < b->ffs.size(); ++i)
     if (!position_d[i] || !charge_d[i]) return fail(b, MSMPB_ERR_ARGUMENT);

@@ -30,6 +30,12 @@ void set_error(FF *ff, int code) {
   if (ff && code != MSMPB_OK) ff->last_error = code;
 }
 
+// FF_last_error reports the outcome of the latest working call: each of
+// them (build, rebuild, evaluation, adjoint, sync) clears it first
+void begin_call(FF *ff) {
+  if (ff) ff->last_error = MSMPB_OK;
+}
+
 bool timing_enabled() {
   static int cached = -1;
   if (cached < 0) {
@@ -193,6 +199,7 @@ bool FF_get_FFT(FF *ff) { return ff->FFT; }
 
 void FF_build(FF *ff, int N, double (*position)[3], double edges[3][3],
               double margin) {
+  begin_call(ff);
   (void)position;
   HostState *h = host(ff);
   if (!h || ff->N <= 0 || !ff->q || !edges || N != ff->N) {
@@ -225,6 +232,7 @@ void FF_build(FF *ff, int N, double (*position)[3], double edges[3][3],
 
 void FF_rebuild(FF *ff, double edges[3][3], double (*position)[3],
                 double margin) {
+  begin_call(ff);
   (void)position;
   HostState *h = host(ff);
   if (!h || !h->built) {
@@ -254,6 +262,7 @@ void FF_rebuild(FF *ff, double edges[3][3], double (*position)[3],
 }
 
 int FF_rebuild_device(FF *ff, double edges[3][3], void *stream) {
+  begin_call(ff);
   HostState *h = host(ff);
   if (!h || !h->built) return ff->last_error = MSMPB_ERR_STATE;
   if (!ff->dev) return ff->last_error = MSMPB_ERR_NODEVICE;
@@ -274,6 +283,7 @@ int FF_rebuild_device(FF *ff, double edges[3][3], void *stream) {
 
 double FF_energy_potentials(FF *ff, double (*force)[3], double (*position)[3],
                             double *weight, double *potential) {
+  begin_call(ff);
   HostState *h = host(ff);
   if (!h || !h->built) {
     set_error(ff, MSMPB_ERR_STATE);
@@ -318,6 +328,7 @@ double FF_energy(FF *ff, double (*force)[3], double (*position)[3],
 int FF_energy_device(FF *ff, const double *position_d, const double *charge_d,
                      const double *weight, double *force_d,
                      double *potential_d, double *energy_d, void *stream) {
+  begin_call(ff);
   HostState *h = host(ff);
   if (!h || !h->built) return ff->last_error = MSMPB_ERR_STATE;
   if (!ff->dev) return ff->last_error = MSMPB_ERR_NODEVICE;
@@ -341,6 +352,7 @@ int FF_adjoint_device(FF *ff, const double *position_d, const double *charge_d,
                       const double *weight, const double *force_bar_d, double energy_bar,
                       double *charge_grad_d, double *position_grad_d, int reuse_forward,
                       void *stream) {
+  begin_call(ff);
   HostState *h = host(ff);
   if (!h || !h->built) return ff->last_error = MSMPB_ERR_STATE;
   if (!ff->dev) return ff->last_error = MSMPB_ERR_NODEVICE;
@@ -365,6 +377,7 @@ long FF_evaluation_count(const FF *ff) {
 }
 
 int FF_sync(FF *ff) {
+  begin_call(ff);
   if (!ff->dev) return MSMPB_ERR_NODEVICE;
   int st = msm::engine_sync(ff->dev);
   if (st != MSMPB_OK) ff->last_error = st;

@@ -227,6 +227,23 @@ k_segment_sort_z(int ncell, const int *__restrict__ start, int *__restrict__ per
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
   int b = start[c], e = start[c + 1];
+  constexpr int kCap = 32;
+  if (e - b <= kCap) {
+    // rank sort: all loads independent, each atom's place = the number of
+    // atoms before it in (z, index) order; the same order as below
+    const int n = e - b;
+    int id[kCap];
+    T kz[kCap];
+    for (int i = 0; i < n; ++i) id[i] = perm[b + i];
+    for (int i = 0; i < n; ++i) kz[i] = key[id[i]].z;
+    for (int i = 0; i < n; ++i) {
+      int r = 0;
+      for (int j = 0; j < n; ++j)
+        r += (kz[j] < kz[i] || (kz[j] == kz[i] && id[j] < id[i])) ? 1 : 0;
+      perm[b + r] = id[i];
+    }
+    return;
+  }
   for (int k = b + 1; k < e; ++k) {
     const int v = perm[k];
     const T kv = key[v].z;

@@ -32,6 +32,12 @@ void set_error(FF *ff, int code) {
   if (ff && code != MSMPB_OK) ff->last_error = code;
 }
 
+// FF_last_error reports the outcome of the latest working call: each of
+// them (build, rebuild, evaluation, adjoint, sync) clears it first
+void begin_call(FF *ff) {
+  if (ff) ff->last_error = MSMPB_OK;
+}
+
 double *copy_array(const double *src, size_t n) {
   double *d = static_cast<double *>(std::malloc(sizeof(double) * (n ? n : 1)));
   if (d && n) std::memcpy(d, src, sizeof(double) * n);
@@ -137,6 +143,7 @@ void FF_get_topGridDim(FF *ff, int topGridDim[3]) {
 double FF_get_tolDir(FF *ff) { return ff->tolDir; }
 
 void FF_build(FF *ff, double (*position)[3]) {
+  begin_call(ff);
   (void)position;  // the pair set is rebuilt on the GPU at every evaluation
   HostState *h = host(ff);
   if (!h || ff->N <= 0 || !ff->q) {
@@ -182,6 +189,7 @@ double FF_get_errEst(FF *ff, int N, double *charge) {
 }
 
 void FF_rebuild(FF *ff, double edges[3][3], double (*position)[3]) {
+  begin_call(ff);
   (void)position;
   HostState *h = host(ff);
   if (!h || !h->built) {
@@ -212,6 +220,7 @@ void FF_rebuild(FF *ff, double edges[3][3], double (*position)[3]) {
 
 double FF_energy_potentials(FF *ff, double (*force)[3], double (*position)[3],
                             double *weight, double *potential) {
+  begin_call(ff);
   HostState *h = host(ff);
   if (!h || !h->built) {
     set_error(ff, MSMPB_ERR_STATE);
@@ -250,6 +259,7 @@ double FF_energy(FF *ff, double (*force)[3], double (*position)[3], double *weig
 int FF_energy_device(FF *ff, const double *position_d, const double *charge_d,
                      const double *weight, double *force_d, double *potential_d,
                      double *energy_d, void *stream) {
+  begin_call(ff);
   HostState *h = host(ff);
   if (!h || !h->built) return ff->last_error = MSMPB_ERR_STATE;
   if (!ff->dev) return ff->last_error = MSMPB_ERR_NODEVICE;
@@ -270,6 +280,7 @@ int FF_energy_device(FF *ff, const double *position_d, const double *charge_d,
 }
 
 int FF_sync(FF *ff) {
+  begin_call(ff);
   if (!ff->dev) return MSMPB_ERR_NODEVICE;
   const int st = msm::engine_sync(ff->dev);
   if (st != MSMPB_OK) ff->last_error = st;

@@ -251,6 +251,30 @@ def test_tiny_systems(n, nu, m, levels, a0, precision):
     ff.close()
 
 
+def test_non_finite_input_is_reported():
+    """A NaN position or an infinite charge is caught on the device (the
+    atom is binned at a safe cell and a check flag set): the call reports
+    MSMPB_ERR_DEVICE_CHECK instead of reading out of bounds, and the next
+    valid call is clean."""
+    from msmpb_b200 import _lib as L
+    from msmpb_b200.forcefield import MSMError
+    d = load("spceN300_M24_a9_nu4")
+    ff = make_ff(d, "mixed")
+    pos = d["pos"].copy()
+    pos[5, 1] = np.nan
+    with pytest.raises(MSMError) as ex:
+        ff.energy(pos)
+    assert ex.value.code == L.ERR_DEVICE_CHECK
+    q = d["q"].copy()
+    q[7] = np.inf
+    with pytest.raises(MSMError) as ex:
+        ff.energy(d["pos"], charges=q)
+    assert ex.value.code == L.ERR_DEVICE_CHECK
+    e, f = ff.energy(d["pos"], charges=d["q"])
+    assert abs(e - float(d["energy"])) / abs(float(d["energy"])) < TOL["mixed"][0]
+    ff.close()
+
+
 def test_repeat_and_charge_update():
     """Repeated calls give identical results; charge edits between calls
     are seen (FF_new keeps the caller's pointer, code/forcefield0.c:172)."""
