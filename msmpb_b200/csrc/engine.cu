@@ -743,7 +743,7 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   launch_gather<T>(s, N_, pperm_, prel_, pcell_, psorted_, pcs_, pinv_);
   if (kMixed) launch_permute64(s, N_, pperm_, prel64_, psorted64_);
   launch_gather<T>(s, N_, gperm_, gfrac_, gcell_, gsorted_, gcs_, ginv_);
-  nl += 3 + 6 + 2 + 2 + 2 + (kMixed ? 1 : 0);
+  nl += 3 + scan_launches(ncp_) + scan_launches(ncg_) + 2 + 2 + 2 + (kMixed ? 1 : 0);
   const bool clusters = pair_variant_ == 2 && clusters_ok_;
   if (clusters) {  // cluster build (part of the binning phase)
     const V4<double> *src64 =
@@ -777,7 +777,7 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
     ca.err = err_d_;
     ca.self_images = self_images_ ? 1 : 0;
     launch_pair_clusters<T>(s, ca, pc_);
-    nl += 1 + 3 + 1;
+    nl += 1 + scan_launches(ncol_) + 1;
   } else if (pair_variant_ == 0 && pair_cells_supported(noff_, N_)) {
     launch_pair_cells<T>(s, ncp_, psorted_, psorted64_, pstart_, geom_, off_d_,
                          noff_, pc_, pout_, err_d_);

@@ -168,6 +168,34 @@ k_scan_top(int *bsum, int nb) {
   if (threadIdx.x == 0) bsum[nb] = carry;
 }
 
+// Short arrays (small systems, column counts): one block walks the tiles in
+// order with a running carry, one launch instead of three.
+constexpr int kScanSingleMax = 4 * kScanTile;
+
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_single(const int *__restrict__ in, int n, int *__restrict__ out) {
+  __shared__ int sh[32];
+  int carry = 0;
+  for (int base = 0; base < n; base += kScanTile) {
+    int vals[kScanItems];
+    int v = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+      const int idx = base + threadIdx.x * kScanItems + k;
+      vals[k] = idx < n ? in[idx] : 0;
+      v += vals[k];
+    }
+    int total;
+    int ex = block_exclusive_scan(v, sh, &total) + carry;
+    for (int k = 0; k < kScanItems; ++k) {
+      const int idx = base + threadIdx.x * kScanItems + k;
+      if (idx < n) out[idx] = ex;
+      ex += vals[k];
+    }
+    carry += total;
+  }
+  if (threadIdx.x == 0) out[n] = carry;
+}
+
 __global__ void __launch_bounds__(kScanThreads)
 k_scan_apply(const int *__restrict__ in, int n, const int *__restrict__ bsum,
              int nb, int *__restrict__ out) {
@@ -402,7 +430,13 @@ void launch_qstats_final(cudaStream_t s, const double *qparts, int nqparts,
 
 size_t scan_temp_ints(int n) { return (size_t)(n / kScanTile + 2); }
 
+int scan_launches(int n) { return n <= kScanSingleMax ? 1 : 3; }
+
 void launch_scan(cudaStream_t s, const int *in, int *out, int n, int *tmp) {
+  if (n <= kScanSingleMax) {
+    k_scan_single<<<1, kScanThreads, 0, s>>>(in, n, out);
+    return;
+  }
   int nb = std::max(1, (n + kScanTile - 1) / kScanTile);
   k_scan_reduce<<<nb, kScanThreads, 0, s>>>(in, n, tmp);
   k_scan_top<<<1, kScanThreads, 0, s>>>(tmp, nb);

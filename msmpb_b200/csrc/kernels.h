@@ -70,6 +70,7 @@ void launch_charge_stats(cudaStream_t s, int N, const double *q,
 // exclusive scan of n ints into out[0..n] (out[n] = total)
 size_t scan_temp_ints(int n);
 void launch_scan(cudaStream_t s, const int *in, int *out, int n, int *tmp);
+int scan_launches(int n);  // kernels one launch_scan of n entries issues
 void launch_scatter(cudaStream_t s, int N, const int *cell, const int *start,
                     int *cursor, int *perm);
 void launch_segment_sort(cudaStream_t s, int ncell, const int *start,
