@@ -352,12 +352,13 @@ int Plan<T>::init(const Tables &t, int device) {
   a.want(&phi_s_, n * sizeof(double));
   for (int **b : {&pcell_, &gcell_, &pperm_, &gperm_, &pinv_, &ginv_, &pcs_, &gcs_})
     a.want(b, n * sizeof(int));
+  // the four counters consecutive, cleared by one memset per evaluation
   a.want(&pcount_, (ncp_ + 1) * sizeof(int));
-  a.want(&pstart_, (ncp_ + 1) * sizeof(int));
   a.want(&pcursor_, (ncp_ + 1) * sizeof(int));
   a.want(&gcount_, (ncg_ + 1) * sizeof(int));
-  a.want(&gstart_, (ncg_ + 1) * sizeof(int));
   a.want(&gcursor_, (ncg_ + 1) * sizeof(int));
+  a.want(&pstart_, (ncp_ + 1) * sizeof(int));
+  a.want(&gstart_, (ncg_ + 1) * sizeof(int));
   a.want(&scan_tmp_, std::max(scan_temp_ints(ncp_), scan_temp_ints(ncg_)) * sizeof(int));
   for (V4<T> **b : {&prel_, &gfrac_, &psorted_, &gsorted_, &pout_, &gout_})
     a.want(b, n * sizeof(V4<T>));
@@ -726,24 +727,24 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   double w[kMaxLevels + 1];
   for (int l = 0; l <= L_; ++l) w[l] = r.weight ? r.weight[l] : 1.0;
   mark(s, kPhaseBin, tm);
-  cudaMemsetAsync(pcount_, 0, (ncp_ + 1) * sizeof(int), s);
-  cudaMemsetAsync(gcount_, 0, (ncg_ + 1) * sizeof(int), s);
-  cudaMemsetAsync(pcursor_, 0, (ncp_ + 1) * sizeof(int), s);
-  cudaMemsetAsync(gcursor_, 0, (ncg_ + 1) * sizeof(int), s);
+  // the four cell counters are consecutive in the arena: one clear
+  cudaMemsetAsync(pcount_, 0,
+                  reinterpret_cast<char *>(gcursor_ + ncg_ + 1) -
+                      reinterpret_cast<char *>(pcount_),
+                  s);
   launch_charge_stats(s, N_, q, qparts_, nq_);
   launch_qstats_final(s, qparts_, nq_, qstats_);
   launch_prep<T>(s, N_, pos, q, geom_, pcell_, gcell_, pcount_, gcount_, prel_,
                  gfrac_, prel64_, err_d_);
   launch_scan(s, pcount_, pstart_, ncp_, scan_tmp_);
   launch_scan(s, gcount_, gstart_, ncg_, scan_tmp_);
-  launch_scatter(s, N_, pcell_, pstart_, pcursor_, pperm_);
-  launch_scatter(s, N_, gcell_, gstart_, gcursor_, gperm_);
-  launch_segment_sort_z<T>(s, ncp_, pstart_, pperm_, prel_);
-  launch_segment_sort(s, ncg_, gstart_, gperm_);
-  launch_gather<T>(s, N_, pperm_, prel_, pcell_, psorted_, pcs_, pinv_);
-  if (kMixed) launch_permute64(s, N_, pperm_, prel64_, psorted64_);
-  launch_gather<T>(s, N_, gperm_, gfrac_, gcell_, gsorted_, gcs_, ginv_);
-  nl += 3 + scan_launches(ncp_) + scan_launches(ncg_) + 2 + 2 + 2 + (kMixed ? 1 : 0);
+  launch_bin_scatter(s, N_, pcell_, pstart_, pcursor_, pperm_, gcell_, gstart_, gcursor_,
+                     gperm_);
+  launch_bin_sort<T>(s, ncp_, pstart_, pperm_, prel_, ncg_, gstart_, gperm_);
+  launch_bin_gather<T>(s, N_, GatherSide<T>{pperm_, prel_, pcell_, psorted_, pcs_, pinv_},
+                       kMixed ? prel64_ : nullptr, kMixed ? psorted64_ : nullptr,
+                       GatherSide<T>{gperm_, gfrac_, gcell_, gsorted_, gcs_, ginv_});
+  nl += 3 + scan_launches(ncp_) + scan_launches(ncg_) + 3;
   const bool clusters = pair_variant_ == 2 && clusters_ok_;
   if (clusters) {  // cluster build (part of the binning phase)
     const V4<double> *src64 =

@@ -217,23 +217,27 @@ k_scan_apply(const int *__restrict__ in, int n, const int *__restrict__ bsum,
   if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = bsum[nb];
 }
 
+// Both cell scatters of the binning in one launch: threads [0, N) place the
+// atoms into pair cells, threads [N, 2N) into grid cells.
+struct ScatterSide {
+  const int *cell, *start;
+  int *cursor, *perm;
+};
+
 __global__ void __launch_bounds__(kThreads)
-k_scatter(int N, const int *__restrict__ cell, const int *__restrict__ start,
-          int *__restrict__ cursor, int *__restrict__ perm) {
+k_scatter2(int N, ScatterSide p, ScatterSide g) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  int c = cell[i];
-  int slot = start[c] + atomicAdd(cursor + c, 1);
-  perm[slot] = i;
+  if (i >= 2 * N) return;
+  const ScatterSide &d = i < N ? p : g;
+  if (i >= N) i -= N;
+  const int c = d.cell[i];
+  const int slot = d.start[c] + atomicAdd(d.cursor + c, 1);
+  d.perm[slot] = i;
 }
 
-// Orders each cell's atoms by atom index, which makes every later
+// Orders one grid cell's atoms by atom index, which makes every later
 // floating-point sum independent of the scatter's arrival order.
-__global__ void __launch_bounds__(kThreads)
-k_segment_sort(int ncell, const int *__restrict__ start, int *__restrict__ perm) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncell) return;
-  int b = start[c], e = start[c + 1];
+__device__ void sort_cell_by_index(int b, int e, int *__restrict__ perm) {
   for (int k = b + 1; k < e; ++k) {
     int v = perm[k];
     int j = k - 1;
@@ -245,16 +249,12 @@ k_segment_sort(int ncell, const int *__restrict__ start, int *__restrict__ perm)
   }
 }
 
-// Orders each pair cell's atoms along z (key[atom].z, the position relative
+// Orders one pair cell's atoms along z (key[atom].z, the position relative
 // to the cell origin), ties by atom index: every column of cells becomes one
 // z-ordered run, and the order depends only on the input.
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_segment_sort_z(int ncell, const int *__restrict__ start, int *__restrict__ perm,
-                 const V4<T> *__restrict__ key) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncell) return;
-  int b = start[c], e = start[c + 1];
+__device__ void sort_cell_by_z(int b, int e, int *__restrict__ perm,
+                               const V4<T> *__restrict__ key) {
   constexpr int kCap = 32;
   if (e - b <= kCap) {
     // rank sort: all loads independent, each atom's place = the number of
@@ -287,25 +287,39 @@ k_segment_sort_z(int ncell, const int *__restrict__ start, int *__restrict__ per
   }
 }
 
+// Both per-cell sorts in one launch: threads [0, ncp) sort pair cells along
+// z, threads [ncp, ncp + ncg) sort grid cells by atom index.
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
-k_gather(int N, const int *__restrict__ perm, const V4<T> *__restrict__ src,
-         const int *__restrict__ cell, V4<T> *__restrict__ dst,
-         int *__restrict__ cell_sorted, int *__restrict__ inv) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= N) return;
-  int i = perm[k];
-  dst[k] = src[i];
-  cell_sorted[k] = cell[i];
-  inv[i] = k;
+k_sort_cells(int ncp, const int *__restrict__ pstart, int *__restrict__ pperm,
+             const V4<T> *__restrict__ key, int ncg, const int *__restrict__ gstart,
+             int *__restrict__ gperm) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < ncp)
+    sort_cell_by_z<T>(pstart[c], pstart[c + 1], pperm, key);
+  else if (c < ncp + ncg)
+    sort_cell_by_index(gstart[c - ncp], gstart[c - ncp + 1], gperm);
 }
 
+// Both gathers into sorted order in one launch (and the FP64 copy of the
+// pair-cell records in the mixed form): slot k takes atom perm[k].
+template <typename T>
 __global__ void __launch_bounds__(kThreads)
-k_permute64(int N, const int *__restrict__ perm, const V4<double> *__restrict__ src,
-            V4<double> *__restrict__ dst) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < N) dst[k] = src[perm[k]];
+k_gather2(int N, GatherSide<T> p, const V4<double> *__restrict__ src64,
+          V4<double> *__restrict__ dst64, GatherSide<T> g) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  int i = p.perm[k];
+  p.dst[k] = p.src[i];
+  p.cell_sorted[k] = p.cell[i];
+  p.inv[i] = k;
+  if (dst64) dst64[k] = src64[i];
+  i = g.perm[k];
+  g.dst[k] = g.src[i];
+  g.cell_sorted[k] = g.cell[i];
+  g.inv[i] = k;
 }
+
 
 // Per atom in input order: F_i = w0 F_short + q_i E_i and
 // phi_i = w0 (q_i c1 - Q c2 - q_i gamma0/a0 + phi_short) + phi_long.
@@ -413,11 +427,6 @@ void launch_prep(cudaStream_t s, int N, const double *pos, const double *q,
       N, pos, q, g, pcell, gcell, pcount, gcount, prel, gfrac, prel64, err);
 }
 
-void launch_permute64(cudaStream_t s, int N, const int *perm,
-                      const V4<double> *src, V4<double> *dst) {
-  k_permute64<<<blocks_for(N, kThreads), kThreads, 0, s>>>(N, perm, src, dst);
-}
-
 void launch_charge_stats(cudaStream_t s, int N, const double *q,
                          double *partials, int nparts) {
   k_charge_stats<<<nparts, kThreads, 0, s>>>(N, q, partials);
@@ -443,30 +452,24 @@ void launch_scan(cudaStream_t s, const int *in, int *out, int n, int *tmp) {
   k_scan_apply<<<nb, kScanThreads, 0, s>>>(in, n, tmp, nb, out);
 }
 
-void launch_scatter(cudaStream_t s, int N, const int *cell, const int *start,
-                    int *cursor, int *perm) {
-  k_scatter<<<blocks_for(N, kThreads), kThreads, 0, s>>>(N, cell, start,
-                                                         cursor, perm);
-}
-
-void launch_segment_sort(cudaStream_t s, int ncell, const int *start,
-                         int *perm) {
-  k_segment_sort<<<blocks_for(ncell, kThreads), kThreads, 0, s>>>(ncell, start,
-                                                                  perm);
+void launch_bin_scatter(cudaStream_t s, int N, const int *pcell, const int *pstart,
+                        int *pcursor, int *pperm, const int *gcell, const int *gstart,
+                        int *gcursor, int *gperm) {
+  k_scatter2<<<blocks_for(2L * N, kThreads), kThreads, 0, s>>>(
+      N, ScatterSide{pcell, pstart, pcursor, pperm}, ScatterSide{gcell, gstart, gcursor, gperm});
 }
 
 template <typename T>
-void launch_segment_sort_z(cudaStream_t s, int ncell, const int *start,
-                           int *perm, const V4<T> *key) {
-  k_segment_sort_z<T><<<blocks_for(ncell, kThreads), kThreads, 0, s>>>(ncell, start,
-                                                                       perm, key);
+void launch_bin_sort(cudaStream_t s, int ncp, const int *pstart, int *pperm, const V4<T> *key,
+                     int ncg, const int *gstart, int *gperm) {
+  k_sort_cells<T><<<blocks_for((long)ncp + ncg, kThreads), kThreads, 0, s>>>(
+      ncp, pstart, pperm, key, ncg, gstart, gperm);
 }
 
 template <typename T>
-void launch_gather(cudaStream_t s, int N, const int *perm, const V4<T> *src,
-                   const int *cell, V4<T> *dst, int *cell_sorted, int *inv) {
-  k_gather<T><<<blocks_for(N, kThreads), kThreads, 0, s>>>(
-      N, perm, src, cell, dst, cell_sorted, inv);
+void launch_bin_gather(cudaStream_t s, int N, const GatherSide<T> &p,
+                       const V4<double> *src64, V4<double> *dst64, const GatherSide<T> &g) {
+  k_gather2<T><<<blocks_for(N, kThreads), kThreads, 0, s>>>(N, p, src64, dst64, g);
 }
 
 int combine_blocks(int N) { return blocks_for(N, kThreads); }
@@ -487,14 +490,14 @@ void launch_energy_total(cudaStream_t s, const EnergyArgs &a) {
                                const double *, const Geometry &, int *,      \
                                int *, int *, int *, V4<T> *, V4<T> *,         \
                                V4<double> *, int *);                          \
-  template void launch_gather<T>(cudaStream_t, int, const int *,             \
-                                 const V4<T> *, const int *, V4<T> *, int *,  \
-                                 int *);                                      \
+  template void launch_bin_gather<T>(cudaStream_t, int, const GatherSide<T> &,  \
+                                     const V4<double> *, V4<double> *,           \
+                                     const GatherSide<T> &);                     \
   template void launch_combine<T>(cudaStream_t, const CombineArgs &,         \
                                   const int *, const int *, const V4<T> *,    \
                                   const V4<T> *, int);                        \
-  template void launch_segment_sort_z<T>(cudaStream_t, int, const int *,     \
-                                         int *, const V4<T> *);
+  template void launch_bin_sort<T>(cudaStream_t, int, const int *, int *,      \
+                                    const V4<T> *, int, const int *, int *);
 MSM_INST_ATOMS(float)
 MSM_INST_ATOMS(double)
 

@@ -62,26 +62,34 @@ void launch_prep(cudaStream_t s, int N, const double *pos, const double *q,
                  const Geometry &g, int *pcell, int *gcell, int *pcount,
                  int *gcount, V4<T> *prel, V4<T> *gfrac, V4<double> *prel64,
                  int *err);
-// dst[k] = src[perm[k]]
-void launch_permute64(cudaStream_t s, int N, const int *perm,
-                      const V4<double> *src, V4<double> *dst);
 void launch_charge_stats(cudaStream_t s, int N, const double *q,
                          double *partials, int nparts);
 // exclusive scan of n ints into out[0..n] (out[n] = total)
 size_t scan_temp_ints(int n);
 void launch_scan(cudaStream_t s, const int *in, int *out, int n, int *tmp);
 int scan_launches(int n);  // kernels one launch_scan of n entries issues
-void launch_scatter(cudaStream_t s, int N, const int *cell, const int *start,
-                    int *cursor, int *perm);
-void launch_segment_sort(cudaStream_t s, int ncell, const int *start,
-                         int *perm);
-// orders each cell by key[atom].z, ties by atom index
+// Binning after the scans, one launch each: both cell scatters (pair cells,
+// grid cells); both per-cell sorts (pair cells by key[atom].z, ties by atom
+// index; grid cells by atom index); both gathers into sorted order, plus the
+// FP64 copy of the pair records (src64/dst64, may be null).
+void launch_bin_scatter(cudaStream_t s, int N, const int *pcell, const int *pstart,
+                        int *pcursor, int *pperm, const int *gcell, const int *gstart,
+                        int *gcursor, int *gperm);
 template <typename T>
-void launch_segment_sort_z(cudaStream_t s, int ncell, const int *start,
-                           int *perm, const V4<T> *key);
+void launch_bin_sort(cudaStream_t s, int ncp, const int *pstart, int *pperm, const V4<T> *key,
+                     int ncg, const int *gstart, int *gperm);
+// dst[k] = src[perm[k]], cell_sorted[k] = cell[perm[k]], inv[perm[k]] = k
 template <typename T>
-void launch_gather(cudaStream_t s, int N, const int *perm, const V4<T> *src,
-                   const int *cell, V4<T> *dst, int *cell_sorted, int *inv);
+struct GatherSide {
+  const int *perm;
+  const V4<T> *src;
+  const int *cell;
+  V4<T> *dst;
+  int *cell_sorted, *inv;
+};
+template <typename T>
+void launch_bin_gather(cudaStream_t s, int N, const GatherSide<T> &p,
+                       const V4<double> *src64, V4<double> *dst64, const GatherSide<T> &g);
 struct CombineArgs {
   int N;
   double w0, coeff1, coeff2, gamma0_over_a0;
