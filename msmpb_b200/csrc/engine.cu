@@ -1,17 +1,21 @@
 // Device plan and the launch sequence of one MSM evaluation
 // (code/forcefield1.c:101-235 restated for one B200):
 //
-//   bin + sort atoms (pair cells, finest-grid cells)   deterministic order
-//   short-range pair sum                                 k_pair
-//   anterpolation -> q^1                                 k_anterpolate
+//   bin + sort atoms (pair cells, finest-grid cells)   k_prep, scans, k_scatter2,
+//                                                        k_sort_cells, k_gather2
+//   cluster build                                        k_column_clusters, k_cluster_fill
+//   short-range pair sum                                 k_pair_clusters_f32/_f64
+//   anterpolation -> q^1                                 k_anterp_tiles, k_anterp_fold
 //   restriction q^l -> q^{l+1}, l < L                    k_restrict
-//   top level: FFT(q^L) * khat_L -> e^L (FP64)           k_fft_pass x5
+//   top level: FFT(q^L) * khat_L -> e^L (FP64)           k_fft_plane/k_fft_xlines
+//                                                        or k_fft_lines x5
 //   for l = L-1..1: e^l = prolong(e^{l+1}) + w_l K_l q^l  k_prolong, k_pad, stencil
-//   interpolation of e^1 -> E, phi_long                  k_interpolate
+//   interpolation of e^1 -> E, phi_long                  k_grid_dot, k_interpolate
 //   per-atom combine, energy reductions (FP64)           k_combine, k_energy_total
 //
 // Everything after the input copy is captured once into a CUDA graph and
-// replayed; the graph is re-captured only when pointers or weights change.
+// replayed; the graph is re-captured only when pointers, weights or the box
+// change (after a box change it is updated in place where it can be).
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
