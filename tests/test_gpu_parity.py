@@ -220,7 +220,7 @@ def test_large_top_grid(precision):
 
 
 TINY = [  # (N, order, top grid, levels, cutoff)
-    (2, 4, 4, 1, 4.0), (3, 6, 6, 1, 4.5), (8, 8, 8, 1, 5.0), (33, 10, 8, 1, 5.0),
+    (1, 6, 6, 1, 4.5), (2, 4, 4, 1, 4.0), (3, 6, 6, 1, 4.5), (8, 8, 8, 1, 5.0), (33, 10, 8, 1, 5.0),
     (8, 10, 4, 1, 4.0), (33, 6, 4, 2, 4.0), (33, 4, 4, 3, 3.0), (16, 8, 6, 2, 4.5),
 ]
 
@@ -228,7 +228,7 @@ TINY = [  # (N, order, top grid, levels, cutoff)
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("n,nu,m,levels,a0", TINY)
 def test_tiny_systems(n, nu, m, levels, a0, precision):
-    """Few atoms (ragged clusters of 2..33), every order, grids smaller than
+    """Few atoms (one ion, ragged clusters of 2..33), every order, grids smaller than
     the B-spline order (charges wrap several times), up to three levels,
     atoms given outside the primary box (the reference wraps fractional
     coordinates, code/forcefield1.c:349-352)."""
