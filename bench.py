@@ -456,6 +456,65 @@ def pme_timing(q, pos, edges, pos_d, q_d, f_d, phi_d, e_d, torch, flush, f_hi, e
     return out
 
 
+# (order, top grid M, cutoff a0) of each trial of the reference's MSM-versus-PME
+# comparison (code/journal/Figure4_run.py:7-28), one level
+CURVE_TRIALS = [(4, 90, 9.0), (4, 84, 9.0), (4, 80, 9.0), (4, 72, 9.0), (4, 70, 9.0),
+                (6, 60, 9.0), (6, 56, 9.0), (6, 54, 9.0), (6, 50, 9.0), (6, 48, 9.0),
+                (4, 54, 12.0), (4, 50, 12.0), (4, 48, 12.0), (4, 42, 12.0), (4, 40, 12.0),
+                (6, 42, 12.0), (6, 40, 12.0), (6, 36, 12.0), (6, 32, 12.0), (6, 30, 12.0)]
+
+
+def curves_timing(dev, torch, flush, reps=10, warmup=3):
+    """MSM and PME cost and error over the trials of the reference's
+    comparison, on a seeded box of 21,950 rigid 3-site waters (65,850 atoms)
+    of edge 88 A, the size and density of that comparison's snapshot. Both
+    methods in the mixed form, device-resident, time per evaluation (median
+    of reps graph replays, L2 flushed before each); force error = RMS force
+    difference over the RMS force of a high-accuracy FP64 MSM (order 10,
+    a0 = 12 A, one level, 180^3 grid) on the same inputs."""
+    from msmpb_b200 import systems
+    from msmpb_b200.forcefield import ForceField
+    from msmpb_b200.pme import PME
+    q, pos, edges = systems.water(21950, 88.0, 4)
+    N = len(q)
+    stream = torch.cuda.current_stream()
+    pos_d = torch.from_numpy(pos).to(dev)
+    q_d = torch.from_numpy(q).to(dev)
+    f_d = torch.zeros((N, 3), dtype=torch.float64, device=dev)
+    phi_d = torch.zeros(N, dtype=torch.float64, device=dev)
+    e_d = torch.zeros(1, dtype=torch.float64, device=dev)
+    hi = ForceField(q, pos, edges, order=10, cutoff=12.0, levels=1, top_grid=180,
+                    precision="fp64", device=dev.index)
+    hi.set_timing(False)
+    hi.energy_device(pos_d.data_ptr(), q_d.data_ptr(), f_d.data_ptr(), phi_d.data_ptr(),
+                     e_d.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    hi.sync()
+    f_hi = f_d.cpu().numpy().copy()
+    hi.close()
+    den = float(np.sqrt((f_hi ** 2).sum()))
+    rows = []
+    for nu, M, a0 in CURVE_TRIALS:
+        row = {"nu": nu, "M": M, "a0": a0}
+        for name in ("msm", "pme"):
+            if name == "msm":
+                x = ForceField(q, pos, edges, order=nu, cutoff=a0, levels=1, top_grid=M,
+                               precision="mixed", device=dev.index)
+            else:
+                x = PME(q, pos, edges, order=nu, cutoff=a0, grid=M, precision="mixed",
+                        device=dev.index)
+            x.set_timing(False)
+            t = time_device(x, pos_d, q_d, f_d, phi_d, e_d, reps, warmup, torch, flush)
+            f = f_d.cpu().numpy()
+            row[name + "_ms"] = round(statistics.median(t), 4)
+            row[name + "_force_err"] = float(np.sqrt(((f - f_hi) ** 2).sum())) / den
+            x.close()
+        rows.append(row)
+    return {"system": "21,950 seeded rigid 3-site waters (65,850 atoms), cubic 88 A box",
+            "reference": "FP64 GPU MSM, order 10, a0 = 12 A, L = 1, 180^3 grid",
+            "precision": "mixed", "trials": rows}
+
+
 def time_device(ff, pos_d, q_d, f_d, phi_d, e_d, steps, warmup, torch, flush):
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
@@ -486,6 +545,14 @@ def run_ours(args):
         return 1
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.only_curves:
+        flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+        out = curves_timing(dev, torch, flush, reps=args.steps, warmup=args.warmup)
+        if rank == 0:
+            print(json.dumps({"curves": out}))
+        if pg is not None:
+            pg.destroy_process_group()
+        return 0
     if args.only_batch:
         flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
         out = batch_timing(dev, torch, flush, reps=args.steps, warmup=args.warmup,
@@ -791,6 +858,9 @@ def main():
                     help="time only the many-systems batch (steps = timed replays)")
     ap.add_argument("--batch-precision", default="mixed,fp64")
     ap.add_argument("--batch-systems", type=int, default=256)
+    ap.add_argument("--only-curves", action="store_true",
+                    help="MSM and PME time and force error over the parameter grid of "
+                         "the reference's MSM-versus-PME comparison")
     ap.add_argument("--only-pme", action="store_true",
                     help="time only the PME comparator on the 1M-atom box")
     ap.add_argument("--batch-branches", type=int, default=0, help="0 = tuned")
@@ -800,7 +870,8 @@ def main():
     args = ap.parse_args()
     # the headline keeps >= 3 warm-up steps; the single-section modes exist
     # for short profiler runs and take what they are given
-    if args.warmup < 3 and args.impl == "ours" and not (args.only_batch or args.only_pme):
+    if args.warmup < 3 and args.impl == "ours" and not (args.only_batch or args.only_pme or
+                                                        args.only_curves):
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
