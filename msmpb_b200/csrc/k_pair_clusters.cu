@@ -248,12 +248,11 @@ __device__ __forceinline__ void tile2(const PairConsts<float> &pc, const V4<floa
   if (!(h0 || h1)) return;
   const float2 rr = make_float2(h0 ? r2.x : pc.a02, h1 ? r2.y : pc.a02);
   const float2 qj = make_float2(h0 ? Y.z : 0.f, h1 ? Y.w : 0.f);
-  if constexpr (NU == 0) {  // PME kernel: the two entries one at a time
-    float v0, f0, v1, f1;
-    pair_radial<float, 0>(pc, rr.x, v0, f0);
-    pair_radial<float, 0>(pc, rr.y, v1, f1);
-    const float2 fs = make_float2(qj.x * f0, qj.y * f1);
-    pp = __fadd2_rn(pp, make_float2(qj.x * v0, qj.y * v1));
+  if constexpr (NU == 0) {  // PME kernel, packed (pair_fn.cuh)
+    float2 v, f;
+    pme_radial2(pc, rr, v, f);
+    const float2 fs = __fmul2_rn(qj, f);
+    pp = __ffma2_rn(qj, v, pp);
     px = __ffma2_rn(fs, dx, px);
     py = __ffma2_rn(fs, dy, py);
     pz = __ffma2_rn(fs, dz, pz);

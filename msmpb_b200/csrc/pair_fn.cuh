@@ -63,4 +63,31 @@ __device__ __forceinline__ void pair_radial64(const PairConsts<T> &pc, double d2
   }
 }
 
+// PME kernel on two pairs at once in packed FP32 (the mixed form's tile
+// loop): erfc(z), z = beta r >= 0, by the Chebyshev-fitted form of Numerical
+// Recipes (Press et al., 2nd ed., sec. 6.2, "erfcc"; fractional error below
+// 1.2e-7 for all z >= 0),
+//   erfc(z) = t exp(-z^2) exp(P(t)),  t = 1 / (1 + z/2),
+// so that exp(-z^2), which the force term needs as well, is computed once.
+// Returns V = erfc(z)/r and f = -(V + 2 beta/sqrt(pi) exp(-z^2)) / r^2.
+__device__ __forceinline__ void pme_radial2(const PairConsts<float> &pc, float2 r2,
+                                            float2 &v, float2 &f) {
+  const float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+  const float2 z = __fmul2_rn(__fmul2_rn(r2, rinv), make_float2(pc.beta, pc.beta));
+  const float2 d = __ffma2_rn(z, make_float2(0.5f, 0.5f), make_float2(1.f, 1.f));
+  const float2 t = make_float2(__fdividef(1.f, d.x), __fdividef(1.f, d.y));
+  constexpr float c[10] = {-1.26551223f, 1.00002368f, 0.37409196f, 0.09678418f,
+                           -0.18628806f, 0.27886807f, -1.13520398f, 1.48851587f,
+                           -0.82215223f, 0.17087277f};
+  float2 p = make_float2(c[9], c[9]);
+#pragma unroll
+  for (int k = 8; k >= 0; --k) p = __ffma2_rn(p, t, make_float2(c[k], c[k]));
+  const float2 mz2 = __fmul2_rn(r2, make_float2(-pc.beta2, -pc.beta2));
+  const float2 ez2 = make_float2(__expf(mz2.x), __expf(mz2.y));
+  const float2 g = make_float2(__expf(p.x), __expf(p.y));
+  v = __fmul2_rn(__fmul2_rn(__fmul2_rn(t, ez2), g), rinv);
+  const float2 s = __ffma2_rn(make_float2(pc.c_exp, pc.c_exp), ez2, v);
+  f = __fmul2_rn(s, __fmul2_rn(rinv, make_float2(-rinv.x, -rinv.y)));
+}
+
 }  // namespace msm
