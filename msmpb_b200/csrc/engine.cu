@@ -1,9 +1,10 @@
 // Device plan and the launch sequence of one MSM evaluation
 // (code/forcefield1.c:101-235 restated for one B200):
 //
-//   bin + sort atoms (pair cells, finest-grid cells)   k_prep, scans, k_scatter2,
+//   bin + sort atoms (pair cells, finest-grid cells),   k_prep, k_qstats_final, scans,
+//   charge sums                                          k_scatter2,
 //                                                        k_sort_cells, k_gather2
-//   cluster build                                        k_column_clusters, k_cluster_fill
+//   cluster build (column counts in k_scatter2)          scan, k_cluster_fill
 //   short-range pair sum                                 k_pair_clusters_f32/_f64
 //   anterpolation -> q^1                                 k_anterp_tiles, k_anterp_fold
 //   restriction q^l -> q^{l+1}, l < L                    k_restrict
@@ -346,7 +347,7 @@ int Plan<T>::init(const Tables &t, int device) {
       }
   }
   const size_t n = N_;
-  nq_ = std::min(1024, std::max(1, (N_ + 255) / 256));
+  nq_ = prep_blocks(N_);
   ncomb_ = combine_blocks(N_);
   ngrid_ = grid_dot_blocks((size_t)ncg_);
   Arena &a = arena_;
@@ -736,24 +737,22 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
                   reinterpret_cast<char *>(gcursor_ + ncg_ + 1) -
                       reinterpret_cast<char *>(pcount_),
                   s);
-  launch_charge_stats(s, N_, q, qparts_, nq_);
-  launch_qstats_final(s, qparts_, nq_, qstats_);
   launch_prep<T>(s, N_, pos, q, geom_, pcell_, gcell_, pcount_, gcount_, prel_,
-                 gfrac_, prel64_, err_d_);
+                 gfrac_, prel64_, err_d_, qparts_);
+  launch_qstats_final(s, qparts_, nq_, qstats_);
   launch_scan(s, pcount_, pstart_, ncp_, scan_tmp_);
   launch_scan(s, gcount_, gstart_, ncg_, scan_tmp_);
+  const bool clusters = pair_variant_ == 2 && clusters_ok_;
   launch_bin_scatter(s, N_, pcell_, pstart_, pcursor_, pperm_, gcell_, gstart_, gcursor_,
-                     gperm_);
+                     gperm_, clusters ? ncol_ : 0, geom_.nc[2], clcount_);
   launch_bin_sort<T>(s, ncp_, pstart_, pperm_, prel_, ncg_, gstart_, gperm_);
   launch_bin_gather<T>(s, N_, GatherSide<T>{pperm_, prel_, pcell_, psorted_, pcs_, pinv_},
                        kMixed ? prel64_ : nullptr, kMixed ? psorted64_ : nullptr,
                        GatherSide<T>{gperm_, gfrac_, gcell_, gsorted_, gcs_, ginv_});
-  nl += 3 + scan_launches(ncp_) + scan_launches(ncg_) + 3;
-  const bool clusters = pair_variant_ == 2 && clusters_ok_;
+  nl += 2 + scan_launches(ncp_) + scan_launches(ncg_) + 3;
   if (clusters) {  // cluster build (part of the binning phase)
     const V4<double> *src64 =
         kMixed ? psorted64_ : reinterpret_cast<const V4<double> *>(psorted_);
-    launch_column_clusters(s, ncol_, geom_.nc[2], pstart_, clcount_);
     launch_scan(s, clcount_, clstart_, ncol_, scan_tmp_);
     launch_cluster_fill<T>(s, maxcl_, ncol_, geom_.nc[2], pstart_, clstart_, pcs_,
                            src64, cz_, cpos_, cpos64_, cinfo_, cubox_);
@@ -782,7 +781,7 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
     ca.err = err_d_;
     ca.self_images = self_images_ ? 1 : 0;
     launch_pair_clusters<T>(s, ca, pc_);
-    nl += 1 + scan_launches(ncol_) + 1;
+    nl += scan_launches(ncol_) + 1;
   } else if (pair_variant_ == 0 && pair_cells_supported(noff_, N_)) {
     launch_pair_cells<T>(s, ncp_, psorted_, psorted64_, pstart_, geom_, off_d_,
                          noff_, pc_, pout_, err_d_);

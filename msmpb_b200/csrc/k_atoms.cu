@@ -24,8 +24,36 @@ k_prep(int N, const double *__restrict__ pos, const double *__restrict__ q,
        Geometry g, int *__restrict__ pcell, int *__restrict__ gcell,
        int *__restrict__ pcount, int *__restrict__ gcount,
        V4<T> *__restrict__ prel, V4<T> *__restrict__ gfrac,
-       V4<double> *__restrict__ prel64, int *err) {
+       V4<double> *__restrict__ prel64, int *err, double *__restrict__ qparts) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  // this block's sums of q and q^2 (FP64, fixed order), one pair per block
+  {
+    double a = 0., b = 0.;
+    if (i < N) {
+      a = q[i];
+      b = a * a;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    __shared__ double wa[kThreads / 32], wb[kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+      wa[warp] = a;
+      wb[warp] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double sa = 0., sb = 0.;
+      for (int w = 0; w < kThreads / 32; ++w) {
+        sa += wa[w];
+        sb += wb[w];
+      }
+      qparts[2 * blockIdx.x] = sa;
+      qparts[2 * blockIdx.x + 1] = sb;
+    }
+  }
   if (i >= N) return;
   double r0 = pos[3 * i], r1 = pos[3 * i + 1], r2 = pos[3 * i + 2];
   double qi = q[i];
@@ -80,33 +108,6 @@ k_prep(int N, const double *__restrict__ pos, const double *__restrict__ q,
   b.z = (T)t[2];
   b.w = (T)qi;
   gfrac[i] = b;
-}
-
-// Block-level partial sums of q and q^2 (FP64)
-__global__ void __launch_bounds__(kThreads)
-k_charge_stats(int N, const double *__restrict__ q, double *partials) {
-  __shared__ double s1[kThreads], s2[kThreads];
-  double a = 0., b = 0.;
-  for (int i = blockIdx.x * kThreads + threadIdx.x; i < N;
-       i += gridDim.x * kThreads) {
-    double v = q[i];
-    a += v;
-    b += v * v;
-  }
-  s1[threadIdx.x] = a;
-  s2[threadIdx.x] = b;
-  __syncthreads();
-  for (int w = kThreads / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) {
-      s1[threadIdx.x] += s1[threadIdx.x + w];
-      s2[threadIdx.x] += s2[threadIdx.x + w];
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    partials[2 * blockIdx.x] = s1[0];
-    partials[2 * blockIdx.x + 1] = s2[0];
-  }
 }
 
 // ---- exclusive scan (three phases) ----
@@ -218,16 +219,22 @@ k_scan_apply(const int *__restrict__ in, int n, const int *__restrict__ bsum,
 }
 
 // Both cell scatters of the binning in one launch: threads [0, N) place the
-// atoms into pair cells, threads [N, 2N) into grid cells.
+// atoms into pair cells, threads [N, 2N) into grid cells, and threads
+// [2N, 2N + ncol) count each pair-cell column's clusters of 8 atoms (for the
+// cluster pair sum; ncol = 0 when it is not used).
 struct ScatterSide {
   const int *cell, *start;
   int *cursor, *perm;
 };
 
 __global__ void __launch_bounds__(kThreads)
-k_scatter2(int N, ScatterSide p, ScatterSide g) {
+k_scatter2(int N, ScatterSide p, ScatterSide g, int ncol, int nc2, int *__restrict__ clcount) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= 2 * N) return;
+  if (i >= 2 * N) {
+    const int c = i - 2 * N;
+    if (c < ncol) clcount[c] = (p.start[(c + 1) * nc2] - p.start[c * nc2] + 7) >> 3;
+    return;
+  }
   const ScatterSide &d = i < N ? p : g;
   if (i >= N) i -= N;
   const int c = d.cell[i];
@@ -422,15 +429,12 @@ template <typename T>
 void launch_prep(cudaStream_t s, int N, const double *pos, const double *q,
                  const Geometry &g, int *pcell, int *gcell, int *pcount,
                  int *gcount, V4<T> *prel, V4<T> *gfrac, V4<double> *prel64,
-                 int *err) {
+                 int *err, double *qparts) {
   k_prep<T><<<blocks_for(N, kThreads), kThreads, 0, s>>>(
-      N, pos, q, g, pcell, gcell, pcount, gcount, prel, gfrac, prel64, err);
+      N, pos, q, g, pcell, gcell, pcount, gcount, prel, gfrac, prel64, err, qparts);
 }
 
-void launch_charge_stats(cudaStream_t s, int N, const double *q,
-                         double *partials, int nparts) {
-  k_charge_stats<<<nparts, kThreads, 0, s>>>(N, q, partials);
-}
+int prep_blocks(int N) { return (int)blocks_for(N, kThreads); }
 
 void launch_qstats_final(cudaStream_t s, const double *qparts, int nqparts,
                          double *qstats) {
@@ -454,9 +458,10 @@ void launch_scan(cudaStream_t s, const int *in, int *out, int n, int *tmp) {
 
 void launch_bin_scatter(cudaStream_t s, int N, const int *pcell, const int *pstart,
                         int *pcursor, int *pperm, const int *gcell, const int *gstart,
-                        int *gcursor, int *gperm) {
-  k_scatter2<<<blocks_for(2L * N, kThreads), kThreads, 0, s>>>(
-      N, ScatterSide{pcell, pstart, pcursor, pperm}, ScatterSide{gcell, gstart, gcursor, gperm});
+                        int *gcursor, int *gperm, int ncol, int nc2, int *clcount) {
+  k_scatter2<<<blocks_for(2L * N + ncol, kThreads), kThreads, 0, s>>>(
+      N, ScatterSide{pcell, pstart, pcursor, pperm}, ScatterSide{gcell, gstart, gcursor, gperm},
+      ncol, nc2, clcount);
 }
 
 template <typename T>
@@ -489,7 +494,7 @@ void launch_energy_total(cudaStream_t s, const EnergyArgs &a) {
   template void launch_prep<T>(cudaStream_t, int, const double *,            \
                                const double *, const Geometry &, int *,      \
                                int *, int *, int *, V4<T> *, V4<T> *,         \
-                               V4<double> *, int *);                          \
+                               V4<double> *, int *, double *);                \
   template void launch_bin_gather<T>(cudaStream_t, int, const GatherSide<T> &,  \
                                      const V4<double> *, V4<double> *,           \
                                      const GatherSide<T> &);                     \

@@ -137,13 +137,6 @@ k_cluster_fill(int maxcl, int ncol, int nc2, const int *__restrict__ start,
   }
 }
 
-__global__ void k_column_clusters(int ncol, int nc2, const int *__restrict__ start,
-                                  int *__restrict__ count) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncol) return;
-  count[c] = (start[(c + 1) * nc2] - start[c * nc2] + 7) >> 3;
-}
-
 template <typename T, int NU>
 __device__ __forceinline__ void pair_terms(const PairConsts<T> &pc, T r2, T qj,
                                            T &pot, T &fs) {
@@ -537,11 +530,6 @@ void launch_nu(cudaStream_t s, const PairClusterArgs<T> &a, const PairConsts<T> 
 }  // namespace
 
 int cluster_capacity(int N, int ncol) { return N / 8 + ncol + 1; }
-
-void launch_column_clusters(cudaStream_t s, int ncol, int nc2, const int *start,
-                            int *count) {
-  k_column_clusters<<<(ncol + 255) / 256, 256, 0, s>>>(ncol, nc2, start, count);
-}
 
 template <typename T>
 void launch_cluster_fill(cudaStream_t s, int maxcl, int ncol, int nc2,

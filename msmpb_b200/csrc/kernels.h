@@ -61,20 +61,22 @@ template <typename T>
 void launch_prep(cudaStream_t s, int N, const double *pos, const double *q,
                  const Geometry &g, int *pcell, int *gcell, int *pcount,
                  int *gcount, V4<T> *prel, V4<T> *gfrac, V4<double> *prel64,
-                 int *err);
-void launch_charge_stats(cudaStream_t s, int N, const double *q,
-                         double *partials, int nparts);
+                 int *err, double *qparts);
+// blocks of launch_prep: it writes one (sum q, sum q^2) pair per block to
+// qparts, which launch_qstats_final reduces
+int prep_blocks(int N);
 // exclusive scan of n ints into out[0..n] (out[n] = total)
 size_t scan_temp_ints(int n);
 void launch_scan(cudaStream_t s, const int *in, int *out, int n, int *tmp);
 int scan_launches(int n);  // kernels one launch_scan of n entries issues
 // Binning after the scans, one launch each: both cell scatters (pair cells,
-// grid cells); both per-cell sorts (pair cells by key[atom].z, ties by atom
+// grid cells; with ncol > 0 also each pair-cell column's cluster count,
+// ceil(atoms / 8), into clcount); both per-cell sorts (pair cells by key[atom].z, ties by atom
 // index; grid cells by atom index); both gathers into sorted order, plus the
 // FP64 copy of the pair records (src64/dst64, may be null).
 void launch_bin_scatter(cudaStream_t s, int N, const int *pcell, const int *pstart,
                         int *pcursor, int *pperm, const int *gcell, const int *gstart,
-                        int *gcursor, int *gperm);
+                        int *gcursor, int *gperm, int ncol, int nc2, int *clcount);
 template <typename T>
 void launch_bin_sort(cudaStream_t s, int ncp, const int *pstart, int *pperm, const V4<T> *key,
                      int ncg, const int *gstart, int *gperm);
@@ -179,8 +181,6 @@ struct PairClusterArgs {
                               // own images reach its tiles and are skipped
 };
 int cluster_capacity(int N, int ncol);
-void launch_column_clusters(cudaStream_t s, int ncol, int nc2, const int *start,
-                            int *count);
 // src64: FP64 cell-relative positions and charges in sorted order
 template <typename T>
 void launch_cluster_fill(cudaStream_t s, int maxcl, int ncol, int nc2,
