@@ -718,7 +718,7 @@ int Plan<T>::enqueue_chain(cudaStream_t s, T *const *qg, T *const *eg, const dou
     launch_stencil<T>(s, sh_[l], tile_[l], padded_, level_taps(l),
                       stencil_tap_pitch(sh_[l].S[2], !kMixed), (T)w[l], eg[l], part_);
     if (tm) cudaEventRecord(lev_ev_[l][1], s);
-    nl += 3;
+    nl += 2 + stencil_launches(sh_[l], tile_[l]);
   }
   return nl;
 }

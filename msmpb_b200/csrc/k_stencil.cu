@@ -641,6 +641,13 @@ void launch_stencil(cudaStream_t s, const StencilShape &sh, const StencilTile &t
   }
 }
 
+// kernels one launch_stencil issues: the sweep, plus the reduction of the
+// split tap-plane partial sums when the tile splits them
+int stencil_launches(const StencilShape &sh, const StencilTile &tl) {
+  if (!stencil_templated(sh) || tl.nz <= 0) return 1;
+  return tl.nsplit > 1 ? 2 : 1;
+}
+
 template void launch_pad<float>(cudaStream_t, const StencilShape &,
                                 const float *, float *);
 template void launch_pad<double>(cudaStream_t, const StencilShape &,

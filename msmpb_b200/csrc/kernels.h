@@ -268,6 +268,7 @@ template <typename T>
 void launch_stencil(cudaStream_t s, const StencilShape &sh,
                     const StencilTile &tile, const T *padded, const T *kh,
                     int khz, T weight, T *e, T *part);
+int stencil_launches(const StencilShape &sh, const StencilTile &tile);
 
 // ---- adjoint (k_adjoint.cu, k_grid.cu) ----
 struct AdjointCombineArgs {
