@@ -12,11 +12,17 @@ synthetic positions. One step = one evaluation.
             and energy copied out every step
   roofline  the pair-sum kernel (the dominant kernel) against the measured
             FP32 FFMA peak of this GPU, with the level-1 stencil beside it
-  cpu_baseline  the reference's own C code (oracle/_ref, patched build) on a
-            1/8 sample of the workload (same density, spacing, order, cutoff)
+  cpu_baseline  the reference's own C code (oracle/_ref, patched build,
+            rebuilt here with -O3 -march=native) on the same workload: one
+            FF_energy of the 999,999-atom box on one host core, run in a
+            separate process while the GPU is timed; the GPU's energy and
+            force error against it are reported beside it
 
-``--impl reference`` times the reference CPU code instead: one process per
-host core, each evaluating its own sample replica every step.
+``--impl reference`` times the reference CPU code on the same workload
+instead: each of the K steps is one FF_energy of the 999,999-atom box; the
+steps are spread over worker processes on the host cores (the reference is
+serial), each with its own copy of the system and its neighbour list built
+beforehand; value = K N / wall time of the timed region.
 
 Multi-GPU (torchrun): independent replicas, one per GPU (the MSM evaluation
 of one system has no data-parallel split here): weak scaling, no collective
@@ -42,10 +48,13 @@ METRIC = "MSM energy+force evals/s (atoms/s) mixed vs FP64 on one B200 at fixed 
 WORKLOAD = "water1M"
 WORKLOAD_DESC = ("333,333 rigid 3-site waters (999,999 atoms), cubic 215.30 A box, "
                  "nu=6, a0=9 A, 5 levels, top grid 9^3 (finest 144^3)")
-SAMPLE = "water125k"
-SAMPLE_DESC = ("41,667 waters (125,001 atoms), cubic 107.65 A box, nu=6, a0=9 A, "
-               "4 levels, top grid 9^3 (finest 72^3): same density, spacing, order "
-               "and cutoff as the workload at 1/8 of its size")
+# the workload as both arms name it (identical in the two JSON lines)
+WORKLOAD_CONFIG = {"workload": WORKLOAD, "atoms": 999999, "box_A": 215.30, "order": 6,
+                   "cutoff_A": 9.0, "levels": 5, "top_grid": 9, "finest_grid": 144,
+                   "seed": 2, "description": WORKLOAD_DESC}
+# host memory one reference process holds for the 1M-atom box (its flat pair
+# list alone is ~2.1 GB), with margin
+REF_WORKER_BYTES = 5 << 30
 L2_FLUSH_BYTES = 512 << 20
 
 
@@ -53,10 +62,6 @@ def workload(name):
     from msmpb_b200 import systems
     if name == WORKLOAD:
         return systems.config("water1M")
-    if name == SAMPLE:
-        n = 41667
-        q, p, e = systems.water(n, systems.water_edge(n), 7)
-        return q, p, e, dict(order=6, cutoff=9.0, levels=4, top_grid=9)
     raise KeyError(name)
 
 
@@ -564,6 +569,11 @@ def run_ours(args):
         if pg is not None:
             pg.destroy_process_group()
         return 0
+    # the CPU baseline (rank 0 of a 1-GPU run) runs in its own process from
+    # here on, while the GPU is timed
+    cpu_leg = None
+    if rank == 0 and world == 1 and not args.skip_cpu and not args.only_pme:
+        cpu_leg = CpuBaseline()
     q, pos, edges, kw = workload(WORKLOAD)
     N = len(q)
     lib = _lib.load()
@@ -699,19 +709,20 @@ def run_ours(args):
     # ---- many small systems: one graph launch against per-system launches ----
     batch = None if args.skip_batch else batch_timing(dev, torch, flush)
 
-    # ---- CPU baseline (rank 0, one GPU only) ----
+    # ---- CPU baseline (rank 0, one GPU only): the reference on the same box ----
     cpu = None
-    if rank == 0 and world == 1 and not args.skip_cpu:
-        cpu = cpu_baseline(dev, torch)
+    if cpu_leg is not None:
+        cpu = cpu_leg.result(N, {"mixed": (e_mixed, f_mixed), "fp64": (e_fp64, f_fp64)})
 
     out = {
         "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64 (FP32 bulk, FP64 FFT and sums)", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "description": WORKLOAD_DESC,
-                   "precision": "mixed", "l2": "flushed before every timed step (512 MB write)",
-                   "inputs": "resident in HBM", "parallelism": "replicas" if world > 1 else "1 GPU"},
+        "config": dict(WORKLOAD_CONFIG),
+        "timing": {"precision": "mixed", "l2": "flushed before every timed step (512 MB write)",
+                   "inputs": "resident in HBM",
+                   "parallelism": "replicas" if world > 1 else "1 GPU"},
         "fp64": {"value": N * world / (ms64 * 1e-3), "ms_per_step": ms64,
                  "mixed_speedup": ms64 / ms},
         "energy": {"mixed": e_mixed, "fp64": e_fp64},
@@ -731,114 +742,195 @@ def run_ours(args):
 
 
 # ---------------------------------------------------------------------------
-def cpu_baseline(dev, torch):
-    """The reference's C code on the 1/8 sample, timed on one host core, and
-    the GPU's error on the same sample against it."""
-    from msmpb_b200.forcefield import ForceField
-    q, pos, edges, kw = workload(SAMPLE)
-    n = len(q)
-    kind, t_best, e_ref, f_ref = None, None, None, None
+def _ref_library():
+    """The reference library to time: the patched build recompiled here with
+    -O3 -march=native (oracle/build_ref.build_native), else the portable
+    patched build, else None (then the oracle port stands in)."""
     try:
+        from oracle import build_ref
         from oracle.oracle import RefFF
+        path = build_ref.build_native()
+        if path:
+            return path, "reference", "patched reference, gcc -O3 -march=native"
         if RefFF.available():
-            r = RefFF(q, pos, edges, cutoff=kw["cutoff"], nu=kw["order"],
-                      levels=kw["levels"], top_grid=kw["top_grid"])
-            t0 = time.perf_counter()
-            e_ref, f_ref = r.energy()
-            t_best = time.perf_counter() - t0
-            r.close()
-            kind = "reference"
+            from oracle.oracle import REF_SO
+            return REF_SO, "reference", "patched reference, gcc -O3"
     except Exception:
-        kind = None
-    if kind is None:
-        from oracle.oracle import Oracle
-        o = Oracle(q, edges, cutoff=kw["cutoff"], nu=kw["order"], levels=kw["levels"],
-                   top_grid=kw["top_grid"])
+        pass
+    return None, "port", "oracle/msm_oracle.c (FP64 restatement), gcc -O3"
+
+
+def _cpu_leg(lib_path, out_dir, conn):
+    """One FF_energy of the workload on one core (a spawned process: no CUDA
+    here). Sends (kind, build seconds, energy seconds, energy) and leaves the
+    forces in out_dir/forces.npy."""
+    sys.path.insert(0, ROOT)
+    try:
+        q, pos, edges, kw = workload(WORKLOAD)
         t0 = time.perf_counter()
-        e_ref, f_ref, _ = o.energy(pos)
-        t_best = time.perf_counter() - t0
-        kind = "port"
-    errs = {}
-    for prec in ("mixed", "fp64"):
-        ffs = ForceField(q, pos, edges, **kw, precision=prec)
-        e, f = ffs.energy(pos)
-        ffs.close()
-        errs[prec] = {"energy_rel": abs(e - e_ref) / abs(e_ref),
-                      "force_rms_rel": float(np.sqrt(((f - f_ref) ** 2).sum() /
-                                                     (f_ref ** 2).sum()))}
-    return {"value": n / t_best, "unit": "atoms/s", "cores": 1, "kind": kind,
-            "sample": SAMPLE_DESC + "; one FF_energy call (neighbour list built "
-                      "beforehand by FF_build, not timed)",
-            "seconds": t_best, "gpu_error_vs_cpu_on_sample": errs}
+        if lib_path:
+            from oracle.oracle import RefFF
+            r = RefFF(q, pos, edges, cutoff=kw["cutoff"], nu=kw["order"],
+                      levels=kw["levels"], top_grid=kw["top_grid"], lib_path=lib_path)
+            run = r.energy
+        else:
+            from oracle.oracle import Oracle
+            o = Oracle(q, edges, cutoff=kw["cutoff"], nu=kw["order"], levels=kw["levels"],
+                       top_grid=kw["top_grid"])
+            run = lambda: o.energy(pos)[:2]  # noqa: E731
+        t1 = time.perf_counter()
+        e, f = run()
+        t2 = time.perf_counter()
+        np.save(os.path.join(out_dir, "forces.npy"), f)
+        conn.send(("ok", t1 - t0, t2 - t1, float(e)))
+    except Exception as ex:  # reported in the JSON line, never fatal
+        conn.send(("error", repr(ex)))
+    conn.close()
+
+
+class CpuBaseline:
+    """The reference's CPU code on the benched workload itself, on one host
+    core, in a spawned process that runs while the GPU is timed."""
+
+    def __init__(self):
+        import tempfile
+        self.lib, self.kind, self.build = _ref_library()
+        self.dir = tempfile.mkdtemp(prefix="msmpb_cpu_")
+        ctx = mp.get_context("spawn")
+        self.conn, child = ctx.Pipe(duplex=False)
+        self.proc = ctx.Process(target=_cpu_leg, args=(self.lib, self.dir, child))
+        self.proc.start()
+        child.close()
+
+    def result(self, n, forces):
+        """forces: {precision: (energy, forces)} of the GPU on the same inputs."""
+        import shutil
+        try:
+            msg = self.conn.recv()
+        except EOFError:
+            msg = ("error", "the CPU process ended without a result")
+        self.proc.join()
+        out = None
+        if msg[0] == "ok":
+            _, t_build, t_energy, e_ref = msg
+            f_ref = np.load(os.path.join(self.dir, "forces.npy"))
+            errs = {}
+            for prec, (e, f) in forces.items():
+                errs[prec] = {"energy_rel": abs(e - e_ref) / abs(e_ref),
+                              "force_rms_rel": float(np.sqrt(((f - f_ref) ** 2).sum() /
+                                                             (f_ref ** 2).sum()))}
+            out = {"value": n / t_energy, "unit": "atoms/s", "cores": 1, "kind": self.kind,
+                   "sample": "the full workload (999,999 atoms, 5 levels): one FF_energy "
+                             "call on one host core; neighbour list built beforehand by "
+                             "FF_build (%.1f s, not timed); %s" % (t_build, self.build),
+                   "seconds": t_energy, "energy": e_ref,
+                   "gpu_error_vs_cpu": errs}
+        else:
+            out = {"value": None, "unit": "atoms/s", "cores": 1, "kind": self.kind,
+                   "error": msg[1]}
+        shutil.rmtree(self.dir, ignore_errors=True)
+        return out
 
 
 # ---------------------------------------------------------------------------
-def _ref_worker(seed_off, steps, warmup, barrier, out_q):
+def _ref_worker(widx, lib_path, warmup, steps, bar, out_q):
+    """One reference process of the --impl reference arm: builds the
+    workload (neighbour list included) untimed, runs its warm-up
+    evaluations, waits for every worker, then times its share of the steps."""
     sys.path.insert(0, ROOT)
-    from msmpb_b200 import systems
-    from oracle.oracle import Oracle, RefFF
-    n = 41667
-    q, pos, edges = systems.water(n, systems.water_edge(n), 100 + seed_off)
-    kw = dict(cutoff=9.0, nu=6, levels=4, top_grid=9)
-    if RefFF.available():
-        r = RefFF(q, pos, edges, **kw)
-        run = lambda: r.energy()  # noqa: E731
-        kind = "reference"
+    import resource
+    q, pos, edges, kw = workload(WORKLOAD)
+    if lib_path:
+        from oracle.oracle import RefFF
+        r = RefFF(q, pos, edges, cutoff=kw["cutoff"], nu=kw["order"], levels=kw["levels"],
+                  top_grid=kw["top_grid"], lib_path=lib_path)
+        run = r.energy
     else:
-        o = Oracle(q, edges, **kw)
-        run = lambda: o.energy(pos)  # noqa: E731
-        kind = "port"
-    times = []
-    for k in range(warmup + steps):
-        barrier.wait()
-        t0 = time.perf_counter()
+        from oracle.oracle import Oracle
+        o = Oracle(q, edges, cutoff=kw["cutoff"], nu=kw["order"], levels=kw["levels"],
+                   top_grid=kw["top_grid"])
+        run = lambda: o.energy(pos)[:2]  # noqa: E731
+    for _ in range(warmup):
         run()
-        dt = time.perf_counter() - t0
-        if k >= warmup:
-            times.append(dt)
-    out_q.put((seed_off, kind, len(q), times))
+    bar.wait()
+    t_start = time.perf_counter()
+    times, e = [], None
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        e, _ = run()
+        times.append(time.perf_counter() - t0)
+    t_end = time.perf_counter()
+    rss = resource.getrusage(resource.RUSAGE_SELF).ru_maxrss * 1024
+    out_q.put((widx, len(q), times, t_start, t_end, e, rss))
+
+
+def _host_memory_available():
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return None
 
 
 def run_reference(args):
+    """The reference's CPU implementation on the benched workload: K steps,
+    each one FF_energy of the 999,999-atom box, spread over worker processes
+    (one per host core the step count can use, bounded by host memory)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    lib_path, kind, build = _ref_library()
     try:
-        from oracle import build_ref
-        from oracle.oracle import RefFF
-        if not RefFF.available():
-            build_ref.build(quiet=True)
-    except Exception:
-        pass
-    cores = max(1, min(os.cpu_count() or 1, args.ref_procs or 64))
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        cores = os.cpu_count() or 1
+    mem = _host_memory_available()
+    mem_cap = max(1, int(0.8 * mem) // REF_WORKER_BYTES) if mem else cores
+    cap = max(1, min(cores, mem_cap, args.ref_procs or cores))
+    K = args.steps
+    per = -(-K // min(cap, K))              # steps per worker
+    procs_n = -(-K // per)                  # fewest workers giving that
+    shares = [per] * (K // per) + ([K % per] if K % per else [])
+    warm = -(-args.warmup // procs_n)       # warm-up calls per worker
     ctx = mp.get_context("spawn")
-    bar = ctx.Barrier(cores)
+    bar = ctx.Barrier(procs_n)
     out_q = ctx.Queue()
-    procs = [ctx.Process(target=_ref_worker, args=(i, args.steps, args.warmup, bar, out_q))
-             for i in range(cores)]
+    procs = [ctx.Process(target=_ref_worker, args=(i, lib_path, warm, shares[i], bar, out_q))
+             for i in range(procs_n)]
     for p in procs:
         p.start()
     res = [out_q.get() for _ in procs]
     for p in procs:
         p.join()
-    kind = res[0][1]
-    n = res[0][2]
-    step = [max(r[3][k] for r in res) for k in range(args.steps)]
-    ms = float(np.mean(step)) * 1e3
-    value = cores * n / (ms * 1e-3)
+    n = res[0][1]
+    wall = max(r[4] for r in res) - min(r[3] for r in res)
+    evals = [t for r in res for t in r[2]]
+    ms = wall / K * 1e3
+    value = K * n / wall
+    sample = ("each step is one FF_energy call of the full workload (999,999 atoms, "
+              "5 levels); %d steps over %d worker processes (%d each, at most %d at a "
+              "time: the host has %d cores; each worker %.1f GB of host memory), "
+              "neighbour lists built and %d warm-up call(s) per worker before the timed "
+              "region; one FF_energy takes %.1f s (median) on one core; %s"
+              % (K, procs_n, per, procs_n, cores, max(r[6] for r in res) / 1e9, warm,
+                 statistics.median(evals), build))
     out = {
         "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "steps": K, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "description": WORKLOAD_DESC},
+        "config": dict(WORKLOAD_CONFIG),
         "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": "atoms/s", "cores": cores, "kind": kind,
-                         "sample": "each step: every core evaluates its own replica of "
-                                   + SAMPLE_DESC + " (one FF_energy call)"},
+        "cpu_baseline": {"value": value, "unit": "atoms/s", "cores": procs_n, "kind": kind,
+                         "sample": sample},
         "e2e": {"value": value, "unit": "atoms/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "per_call_s": {"median": statistics.median(evals), "min": min(evals),
+                       "max": max(evals)},
+        "energy": res[0][5],
     }
     print(json.dumps(out))
     return 0

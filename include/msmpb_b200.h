@@ -194,7 +194,9 @@ double msmpb_measure_fp32_tflops(int device, int milliseconds);
  *
  * The first call on a device looks up the array's address there
  * (cudaGetSymbolAddress, which may load the library's GPU code); make it
- * before any stream capture. All calls on a device share the array: calls
+ * before any stream capture. The address is kept until the process exits:
+ * do not reset the device (cudaDeviceReset or a primary-context reset)
+ * between calls. All calls on a device share the array: calls
  * whose GPU work overlaps race, so order them on one stream or with events.
  * Returns MSMPB_OK, MSMPB_ERR_ARGUMENT, MSMPB_ERR_UNSUPPORTED, or
  * MSMPB_ERR_NODEVICE / MSMPB_ERR_CUDA when a CUDA call fails. */

@@ -44,6 +44,15 @@ template <typename T> __device__ __forceinline__ T rsqrt_t(T x);
 template <> __device__ __forceinline__ float rsqrt_t<float>(float x) { return rsqrtf(x); }
 template <> __device__ __forceinline__ double rsqrt_t<double>(double x) { return rsqrt(x); }
 
+// cudaFuncSetAttribute acts on the device current at the call, so one-time
+// kernel set-ups are tracked per device ordinal (ordinals beyond the table
+// are set up on every call).
+constexpr int kMaxDevices = 64;
+inline int device_slot() {
+  int d = -1;
+  return (cudaGetDevice(&d) == cudaSuccess && d >= 0 && d < kMaxDevices) ? d : -1;
+}
+
 // Device error flag bits (read back by the host after each evaluation)
 enum DeviceCheck : int {
   kCheckOk = 0,

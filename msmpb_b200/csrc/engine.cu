@@ -18,6 +18,7 @@
 // replayed; the graph is re-captured only when pointers, weights or the box
 // change (after a box change it is updated in place where it can be).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -52,6 +53,12 @@ struct FFDevice {
 };
 
 namespace msm {
+
+// Stamps for engine_version (see Plan::version_).
+long next_version() {
+  static std::atomic<long> counter{0};
+  return ++counter;
+}
 namespace {
 
 #define MSM_CUDA_TRY(expr)                       \
@@ -196,7 +203,8 @@ class Plan : public FFDevice {
   double J_[11] = {};
   double coeff1_ = 0, coeff2_ = 0, gamma0_a0_ = 0;
   int ncp_ = 0, ncg_ = 0, noff_ = 0;
-  int ncol_ = 0, maxcl_ = 0, ncoloff_ = 0, K2_ = 0;
+  int ncol_ = 0, maxcl_ = 0, ncoloff_ = 0, K2_ = 0, ozero_ = 0;
+  bool ortho_ = false;
   bool clusters_ok_ = false;
   bool self_images_ = false;  // a lattice vector shorter than a0
   int kind_ = kKindMsm;       // kKindPme: one-level PME plan
@@ -245,7 +253,10 @@ class Plan : public FFDevice {
   bool have_graph_ = false;
   bool graph_stale_ = false;  // kernel parameters changed (new box)
   long nevals_ = 0;           // forward evaluations so far
-  long version_ = 0;          // box updates so far
+  // process-wide unique stamp of the current box tables: a new engine and
+  // every box update take the next value, so a replaced engine never
+  // matches a stamp recorded for its predecessor
+  long version_ = next_version();
   // adjoint buffers (allocated on first use)
   void *adj_mem_ = nullptr;
   V4<T> *fbs_ = nullptr, *dip_ = nullptr, *adj_a_ = nullptr, *adj_b_ = nullptr,
@@ -613,12 +624,14 @@ int Plan<T>::update_box(const Tables &t, cudaStream_t s, bool stencils_on_device
       ColumnOffset c{};
       c.du = du;
       c.dv = dv;
+      if (du == 0 && dv == 0) ozero_ = (int)coloffs_.size();
       for (int r = 0; r < 3; ++r)
         c.base[r] = p.A[r][0] * ((double)du / geom_.nc[0]) +
                     p.A[r][1] * ((double)dv / geom_.nc[1]);
       coloffs_.push_back(c);
     }
   ncoloff_ = (int)coloffs_.size();
+  ortho_ = ortho;
   K2_ = K[2];
   for (int r = 0; r < 3; ++r) cz_[r] = p.A[r][2] / geom_.nc[2];
   // the close-pair record packs the column index in 23 bits and the image
@@ -689,7 +702,7 @@ int Plan<T>::update_box(const Tables &t, cudaStream_t s, bool stencils_on_device
   // geometry and constants are kernel parameters: the next graph launch
   // re-captures and updates the instantiated graph in place
   graph_stale_ = true;
-  ++version_;
+  version_ = next_version();
   return MSMPB_OK;
 }
 
@@ -769,6 +782,11 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
     ca.ncoloff = ncoloff_;
     const double rb = std::sqrt((double)pc_.a02) * (1.0 + 1e-4) + 1e-6;
     ca.rbox2 = (float)(rb * rb);
+    const double rn = std::sqrt((double)pc_.close2) * (1.0 + 1e-4) + 1e-5;
+    ca.rnear2 = (float)(rn * rn);
+    ca.ortho = ortho_ ? 1 : 0;
+    ca.ozero = ozero_;
+    for (int k = 0; k < 3; ++k) ca.cw[k] = (float)(geom_.A[4 * k] / geom_.nc[k]);
     for (int r = 0; r < 3; ++r) ca.cz[r] = cz_[r];
     ca.start = pstart_;
     ca.clstart = clstart_;

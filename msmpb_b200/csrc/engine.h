@@ -67,7 +67,8 @@ struct AdjointRequest {
 int engine_adjoint(FFDevice *d, const AdjointRequest &r);
 // Enqueues one device-pointer evaluation (r.pos, r.q, r.force, r.phi,
 // r.energy_dev; r.host false) on s with no waits or host work, for capture
-// into a caller's graph; engine_version changes with every box update.
+// into a caller's graph; engine_version changes with every box update and
+// differs between engines (a rebuilt or re-targeted FF gets a new engine).
 // engine_begin, outside any capture, orders such an evaluation about to run
 // on s after a pending device rebuild and counts it.
 int engine_enqueue(FFDevice *d, const EvalRequest &r, cudaStream_t s);

@@ -10,6 +10,8 @@
 // multiply and inverse x in one launch.
 #include <algorithm>
 
+#include <mutex>
+
 #include "kernels.h"
 
 namespace msm {
@@ -349,11 +351,15 @@ bool plane_path(const int M[3]) {
 
 }  // namespace
 
-// One-time kernel attributes (a line of up to 4096 points with its twiddle
-// table needs 192 KB of shared memory). Called outside stream capture.
+// One-time kernel attributes, per device (a line of up to 4096 points with
+// its twiddle table needs 192 KB of shared memory). Called outside stream
+// capture.
 void top_solve_prepare() {
-  static bool done = false;
-  if (done) return;
+  static std::mutex mu;
+  static bool done[kMaxDevices];
+  const int dev = device_slot();
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && done[dev]) return;
   cudaFuncSetAttribute(k_fft_lines<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        kLineSmemMax);
   cudaFuncSetAttribute(k_fft_lines<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -364,7 +370,7 @@ void top_solve_prepare() {
                        (int)kPlaneSmemMax);
   cudaFuncSetAttribute(k_fft_xlines, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kPlaneSmemMax);
-  done = true;
+  if (dev >= 0) done[dev] = true;
 }
 
 // largest supported line length (radix factors <= kMaxRadix, smem <= 128 KB)

@@ -6,6 +6,8 @@
 // q * Q_nu(n + nu/2 + t) to grid point m - n for n in [-nu/2, nu/2), per axis.
 #include <algorithm>
 
+#include <mutex>
+
 #include "kernels.h"
 
 namespace msm {
@@ -969,8 +971,11 @@ void launch_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
 
 template <typename T>
 void anterpolate_prepare() {
-  static bool done = false;
-  if (done) return;
+  static std::mutex mu;
+  static bool done[kMaxDevices];
+  const int dev = device_slot();
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && done[dev]) return;
   MSM_NU_SWITCH_ALL(cudaFuncSetAttribute(k_anterpolate_slab<T, NU, kAnterpBX>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          kAnterpSmemBudget));
@@ -986,7 +991,7 @@ void anterpolate_prepare() {
   MSM_NU_SWITCH_ALL(cudaFuncSetAttribute(k_prolong<T, NU>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (prolong_smem<T, NU>())));
-  done = true;
+  if (dev >= 0) done[dev] = true;
 }
 
 template <typename T>

@@ -483,20 +483,22 @@ void launch_fold(cudaStream_t s, const StencilShape &sh, const StencilTile &tl,
 }
 
 // Levels (and plans) that share an instantiation need the largest request:
-// the attribute is per kernel function, so it is only ever raised.
+// the attribute is per kernel function and per device, so it is only ever
+// raised, and the level granted is kept per device.
 template <typename T, int S>
 void set_smem_attr(int bytes, bool fold) {
   constexpr int R = TileDefaults<T>::R, TX = TileDefaults<T>::TX;
   static std::mutex mu;
-  static int current[2] = {48 * 1024, 48 * 1024};
+  static int current[kMaxDevices][2];
+  const int dev = device_slot();
   std::lock_guard<std::mutex> lock(mu);
-  if (bytes <= current[fold]) return;
+  if (dev >= 0 && bytes <= std::max(current[dev][fold], 48 * 1024)) return;
   const cudaError_t err =
       fold ? cudaFuncSetAttribute(k_stencil_fold<T, S, R>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)
            : cudaFuncSetAttribute(k_stencil_tiled<T, S, R, TX>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (err == cudaSuccess) current[fold] = bytes;
+  if (err == cudaSuccess && dev >= 0) current[dev][fold] = bytes;
 }
 
 #define MSM_S_CASES(X) \

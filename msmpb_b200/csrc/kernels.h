@@ -167,6 +167,11 @@ template <typename T>
 struct PairClusterArgs {
   int maxcl, ncol, nc0, nc1, nc2, K2, ncoloff;
   float rbox2;      // squared cutoff plus margin for the box test
+  float rnear2;     // squared close-pair distance plus margin (FP32 form:
+                    // j atoms this near the i-cluster box take the checked path)
+  int ortho;        // orthorhombic box: per-column z windows from the xy gap
+  int ozero;        // index of the (0, 0) column offset
+  float cw[3];      // cell widths along x, y, z (orthorhombic boxes)
   double cz[3];     // A (0, 0, 1/nc2): one cell along the column
   const int *start;     // pair-cell starts (ncell + 1)
   const int *clstart;   // first cluster of each column (ncol + 1)

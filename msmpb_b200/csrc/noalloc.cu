@@ -12,8 +12,11 @@
 // Set-up: the first call on a device (the device current at that call) looks
 // up the array's device address with cudaGetSymbolAddress, which can load
 // this library's GPU code onto the device; make that first call before any
-// stream capture. The first call for each stencil width S[2] also raises that
-// kernel's shared-memory limit (cudaFuncSetAttribute).
+// stream capture. The first call for each stencil width S[2] on a device also
+// raises that kernel's shared-memory limit there (cudaFuncSetAttribute). The
+// address is kept for the life of the process: do not reset the device
+// (cudaDeviceReset, or a reset of its primary context) between calls, since
+// later calls would write through the stale address.
 //
 // Sharing: every call on a device uses the same array, which keeps the last
 // call's contents. Nothing in it has to start at zero: each call clears the

@@ -4,10 +4,13 @@
 // of candidate tiles (CTA thread shape and tap-plane split) on the level's
 // own buffers and keeps the fastest; smaller levels use the model-based
 // default (stencil_default_tile). Results are cached in a text file, one
-// line per (device, precision, grid, stencil):
-//   <device name>|<fp32|fp64>|M0,M1,M2|S0,S1,S2|<folded|full> nz ty nsplit ms
-// at $MSMPB_TUNE_CACHE, else $HOME/.cache/msmpb_b200/stencil_tiles.txt.
-// MSMPB_TUNE=0 disables tuning (default tiles only).
+// line per (format, device, precision, grid, stencil):
+//   <format>|<device name>|<fp32|fp64>|M0,M1,M2|S0,S1,S2|<folded|full> nz ty nsplit ms
+// at $MSMPB_TUNE_CACHE, else $HOME/.cache/msmpb_b200/stencil_tiles.txt. A
+// cached tile is used only after the same checks as a freshly timed one
+// (shape limits, buffer capacities, stencil_prepare); a line that fails them
+// (another library version, a hand-edited file) is ignored and the level is
+// tuned again. MSMPB_TUNE=0 disables tuning (default tiles only).
 #include <sys/stat.h>
 
 #include <algorithm>
@@ -25,6 +28,10 @@ namespace {
 
 std::mutex g_cache_mu;
 
+// Bumped whenever the candidate set or the meaning of a tile changes, so
+// that lines written by another version never match.
+constexpr const char *kCacheFormat = "st2";
+
 std::string cache_path() {
   const char *p = std::getenv("MSMPB_TUNE_CACHE");
   if (p && *p) return p;
@@ -41,8 +48,8 @@ std::string cache_key(const StencilShape &sh, bool fp64, int device) {
   cudaDeviceProp prop{};
   cudaGetDeviceProperties(&prop, device);
   char buf[512];
-  std::snprintf(buf, sizeof buf, "%s|%s|%d,%d,%d|%d,%d,%d|%s", prop.name,
-                fp64 ? "fp64" : "fp32", sh.M[0], sh.M[1], sh.M[2], sh.S[0],
+  std::snprintf(buf, sizeof buf, "%s|%s|%s|%d,%d,%d|%d,%d,%d|%s", kCacheFormat,
+                prop.name, fp64 ? "fp64" : "fp32", sh.M[0], sh.M[1], sh.M[2], sh.S[0],
                 sh.S[1], sh.S[2], sh.sym ? "folded" : "full");
   for (char *c = buf; *c; ++c)
     if (*c == ' ') *c = '_';
@@ -113,6 +120,25 @@ std::vector<StencilTile> stencil_candidates(const StencilShape &sh, bool fp64) {
   return out;
 }
 
+// Whether a tile can run on a level: its shape within the kernels' limits,
+// its padded grid and split-K partial sums within the buffers the plan
+// allocated, and its kernel's shared memory granted (stencil_prepare). Both
+// cached and freshly timed tiles pass through here.
+template <typename T>
+bool tile_usable(const StencilShape &sh0, const StencilTile &t, size_t padded_cap,
+                 size_t part_cap) {
+  if (t.nz <= 0 || t.ty <= 0 || t.nz * t.ty > 256 || t.nsplit < 1 || t.tx <= 0) return false;
+  const int nI = sh0.sym ? sh0.S[0] / 2 + 1 : sh0.S[0];
+  if (t.nsplit > nI) return false;
+  StencilShape sh = sh0;
+  stencil_padded_dims(sh, t, sizeof(T) == 8, sh.P);
+  if (sh.P[0] <= 0 || sh.P[1] <= 0 || sh.P[2] <= 0) return false;
+  if ((size_t)sh.P[0] * sh.P[1] * sh.P[2] > padded_cap) return false;
+  const size_t mtot = (size_t)sh0.M[0] * sh0.M[1] * sh0.M[2];
+  if (t.nsplit > 1 && (size_t)t.nsplit * mtot > part_cap) return false;
+  return stencil_prepare<T>(sh, t) >= 0;
+}
+
 template <typename T>
 StencilTile stencil_autotune(cudaStream_t s, int device, const StencilShape &sh0,
                              const StencilTile &fallback, const T *padded,
@@ -123,22 +149,21 @@ StencilTile stencil_autotune(cudaStream_t s, int device, const StencilShape &sh0
   StencilTile cached;
   if (cache_lookup(key, cached)) {
     cached.tx = fallback.tx;
-    if (best_ms) *best_ms = -1.0;
-    return cached;
+    if (tile_usable<T>(sh0, cached, padded_cap, part_cap)) {
+      if (best_ms) *best_ms = -1.0;
+      return cached;
+    }
   }
   StencilTile best = fallback;
   double best_t = 1e30;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  const long mtot = (long)sh0.M[0] * sh0.M[1] * sh0.M[2];
   for (StencilTile t : stencil_candidates(sh0, fp64)) {
     t.tx = fallback.tx;
+    if (!tile_usable<T>(sh0, t, padded_cap, part_cap)) continue;
     StencilShape sh = sh0;
     stencil_padded_dims(sh, t, fp64, sh.P);
-    if ((size_t)sh.P[0] * sh.P[1] * sh.P[2] > padded_cap) continue;
-    if (t.nsplit > 1 && (size_t)t.nsplit * mtot > part_cap) continue;
-    if (stencil_prepare<T>(sh, t) < 0) continue;
     float ms[3];
     bool ok = true;
     launch_stencil<T>(s, sh, t, padded, kh, khz, T(0), e, part);  // warm-up

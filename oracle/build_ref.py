@@ -34,8 +34,14 @@ Outputs (all under oracle/_ref/):
   pme_dropin                 code/pme.c, unmodified, compiled against this
                              project's include/pme.h and linked to
                              msmpb_b200/libpme.so
+  src/lib/                   the sources of the patched library (forcefield0.c
+                             and forcefield.h copied, forcefield1.c patched),
+                             so that ``build_native()`` can rebuild it where
+                             the reference tree is absent
+  native/libmsmpb_ref_native.so  that rebuild with -march=native for the host
+                             it runs on (made on demand by bench.py's CPU arms)
 
-Usage: python oracle/build_ref.py [--reference DIR]
+Usage: python oracle/build_ref.py [--reference DIR]   (default: $MSMPB_REFERENCE)
 """
 import argparse
 import os
@@ -58,6 +64,10 @@ P2_NEW = "ql[((i+ofx)*(gd.y + py) + (j+ofy))*(gd.z + pz) + k + ofz]"
 
 CFLAGS = ["-O3", "-std=gnu11", "-fPIC", "-w"]
 
+# where the reference project lies: the MSMPB_REFERENCE environment variable,
+# else the read-only checkout of this build container
+REFERENCE = os.environ.get("MSMPB_REFERENCE", "/root/reference")
+
 
 def _replace_once(text, old, new):
     if text.count(old) != 1:
@@ -77,7 +87,7 @@ def run(cmd):
     subprocess.run(cmd, check=True)
 
 
-def build(reference_root="/root/reference", quiet=False):
+def build(reference_root=REFERENCE, quiet=False):
     code = os.path.join(reference_root, "code")
     ff0 = os.path.join(code, "forcefield0.c")
     ff1 = os.path.join(code, "forcefield1.c")
@@ -99,6 +109,14 @@ def build(reference_root="/root/reference", quiet=False):
                 '/* the library reads o.test (code/forcefield0.c:469); the\n'
                 '   drivers define o (code/msmpb.c:9), a bare library must */\n'
                 'struct O o = {"none"};\n')
+    # the library's sources in a directory of their own (the drop-in driver
+    # copies below must not see the reference header beside them)
+    lib_src = os.path.join(src_dir, "lib")
+    os.makedirs(lib_src, exist_ok=True)
+    for f in ("forcefield0.c", "forcefield.h"):
+        shutil.copy(os.path.join(code, f), os.path.join(lib_src, f))
+    for f in ("forcefield1_patched.c", "ref_glue.c"):
+        shutil.copy(os.path.join(src_dir, f), os.path.join(lib_src, f))
     inc = ["-I", SHIM, "-I", code]
     fft = os.path.join(SHIM, "fft_shim.c")
     cc = os.environ.get("CC", "gcc")
@@ -122,6 +140,30 @@ def build(reference_root="/root/reference", quiet=False):
     if not quiet:
         print("build_ref: built", OUT)
     return True
+
+
+def build_native(quiet=True):
+    """Rebuild the patched reference library from oracle/_ref/src/ with
+    ``-O3 -march=native`` for the host this runs on (the portable build above
+    uses -O3 only, since it may run on another machine). Returns the library
+    path, or None when the sources or the compiler are missing."""
+    src_dir = os.path.join(OUT, "src", "lib")
+    srcs = [os.path.join(src_dir, f) for f in
+            ("forcefield0.c", "forcefield1_patched.c", "ref_glue.c")]
+    if not all(os.path.exists(p) for p in srcs + [os.path.join(src_dir, "forcefield.h")]):
+        return None
+    out_dir = os.path.join(OUT, "native")
+    os.makedirs(out_dir, exist_ok=True)
+    lib = os.path.join(out_dir, "libmsmpb_ref_native.so")
+    cc = os.environ.get("CC", "gcc")
+    cmd = [cc, *CFLAGS, "-march=native", "-shared", "-I", SHIM, "-I", src_dir, *srcs,
+           os.path.join(SHIM, "fft_shim.c"), "-lm", "-o", lib + ".tmp"]
+    try:
+        subprocess.run(cmd, check=True, capture_output=quiet)
+        os.replace(lib + ".tmp", lib)
+    except (OSError, subprocess.CalledProcessError):
+        return None
+    return lib
 
 
 def build_pme(code, src_dir, inc, fft, cc, root):
@@ -148,7 +190,7 @@ def build_pme(code, src_dir, inc, fft, cc, root):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=REFERENCE)
     ap.add_argument("--clean", action="store_true")
     a = ap.parse_args()
     if a.clean and os.path.isdir(OUT):

@@ -290,18 +290,19 @@ class RefFF:
         return os.path.exists(REF_UNPATCHED_SO if unpatched else REF_SO)
 
     @classmethod
-    def lib(cls, unpatched=False):
-        key = bool(unpatched)
-        if key not in cls._libs:
-            path = REF_UNPATCHED_SO if unpatched else REF_SO
+    def lib(cls, unpatched=False, path=None):
+        """The patched (default) or unpatched build; ``path`` names another
+        build of the patched sources (build_ref.build_native)."""
+        path = path or (REF_UNPATCHED_SO if unpatched else REF_SO)
+        if path not in cls._libs:
             if not os.path.exists(path):
                 raise FileNotFoundError(path + " (run oracle/build_ref.py)")
-            cls._libs[key] = bind_ff_api(C.CDLL(path))
-        return cls._libs[key]
+            cls._libs[path] = bind_ff_api(C.CDLL(path))
+        return cls._libs[path]
 
     def __init__(self, q, pos, edges, cutoff=None, nu=None, levels=None,
-                 top_grid=None, margin=0.0, unpatched=False):
-        lib = self.lib(unpatched)
+                 top_grid=None, margin=0.0, unpatched=False, lib_path=None):
+        lib = self.lib(unpatched, lib_path)
         self._lib = lib
         self.q = _f64(q).copy()  # FF_new keeps the caller's pointer
         self.N = len(self.q)

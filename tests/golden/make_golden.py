@@ -10,7 +10,7 @@ Sources:
   differences in q (exact, U is quadratic in q);
 * published values from results/TableII.json, results/Figure1.txt.
 
-Usage: python tests/golden/make_golden.py [--reference /root/reference]
+Usage: python tests/golden/make_golden.py [--reference DIR]   (default: $MSMPB_REFERENCE)
 """
 import argparse
 import json
@@ -82,5 +82,5 @@ def make(reference):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=build_ref.REFERENCE)
     make(ap.parse_args().reference)

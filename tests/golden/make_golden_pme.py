@@ -9,7 +9,7 @@ parameters (grid, beta), the constant-term coefficients, the error estimate
 and, for small systems, per-atom potentials by central differences in q
 (exact: U is quadratic in q).
 
-Usage: python tests/golden/make_golden_pme.py [--reference /root/reference]
+Usage: python tests/golden/make_golden_pme.py [--reference DIR]   (default: $MSMPB_REFERENCE)
 """
 import argparse
 import json
@@ -79,5 +79,5 @@ def make(reference):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=build_ref.REFERENCE)
     make(ap.parse_args().reference)

@@ -118,3 +118,59 @@ def test_autograd_binding():
     assert np.allclose(p.grad.cpu().numpy(), dr, rtol=1e-12, atol=1e-12)
     assert np.allclose(qq.grad.cpu().numpy(), dq, rtol=1e-12, atol=1e-12)
     ff.close()
+
+
+def test_force_matching_water3000():
+    """The differentiation workload: 1000 rigid 3-site waters (3,000 atoms,
+    cubic 31.04 A box), order 6, cutoff 9 A, automatic grid; the
+    force-matching loss L = sum_i |F_i - F_tgt_i|^2 with F_tgt the forces of
+    the same system under charges perturbed by N(0, 0.01^2) (seed 4). The
+    autograd gradient of L with respect to positions and charges (FP64 form)
+    against FP64 central differences (step 1e-5) of the oracle's L on 32
+    atoms (96 position and 32 charge components), to 1e-6; the forward
+    forces against the oracle's to 1e-10 (code/forcefield1.c:225-231)."""
+    q, pos, edges, kw = systems.config("water3000")
+    n = len(q)
+    rng = np.random.default_rng(4)
+    q_tgt = q + rng.normal(0.0, 0.01, n)
+    ff = ForceField(q, pos, edges, **kw, precision="fp64")
+    ff.set_timing(False)
+    o = Oracle(q, edges, cutoff=ff.cutoff, nu=ff.order, levels=ff.levels,
+               top_grid=ff.top_grid)
+    assert (ff.levels, ff.top_grid) == (1, (27, 27, 27))
+    _, f_tgt, _ = o.energy(pos, q=q_tgt)
+    _, f_o, _ = o.energy(pos)
+
+    dev = torch.device("cuda", 0)
+    p = torch.tensor(pos, device=dev, requires_grad=True)
+    qq = torch.tensor(q, device=dev, requires_grad=True)
+    u, f = msm_energy_forces(ff, p, qq)
+    assert np.sqrt(((f.detach().cpu().numpy() - f_o) ** 2).sum() / (f_o ** 2).sum()) < 1e-10
+    lval = ((f - torch.tensor(f_tgt, device=dev)) ** 2).sum()
+    lval.backward()
+    dr = p.grad.cpu().numpy()
+    dq = qq.grad.cpu().numpy()
+
+    def lo(pp, qv):
+        _, ff_o, _ = o.energy(pp, q=qv)
+        return float(((ff_o - f_tgt) ** 2).sum())
+
+    atoms = np.sort(rng.choice(n, 32, replace=False))
+    h = 1e-5
+    fd_r, ad_r, fd_q, ad_q = [], [], [], []
+    for k in atoms:
+        for a in range(3):
+            pp, pm = pos.copy(), pos.copy()
+            pp[k, a] += h
+            pm[k, a] -= h
+            fd_r.append((lo(pp, q) - lo(pm, q)) / (2 * h))
+            ad_r.append(dr[k, a])
+        qp, qm = q.copy(), q.copy()
+        qp[k] += h
+        qm[k] -= h
+        fd_q.append((lo(pos, qp) - lo(pos, qm)) / (2 * h))
+        ad_q.append(dq[k])
+    fd_r, ad_r, fd_q, ad_q = map(np.array, (fd_r, ad_r, fd_q, ad_q))
+    assert np.linalg.norm(ad_r - fd_r) / np.linalg.norm(fd_r) < 1e-6
+    assert np.linalg.norm(ad_q - fd_q) / np.linalg.norm(fd_q) < 1e-6
+    ff.close()

@@ -137,6 +137,25 @@ def test_batch_recaptures_on_change():
 
 
 @pytest.mark.gpu
+def test_batch_recaptures_after_member_engine_replaced():
+    """FF_set_precision (like a second FF_build or FF_set_device) replaces a
+    member's device engine and frees the old one's buffers: the next batch
+    call must capture again rather than replay nodes that point into the
+    freed engine."""
+    members = small_batch(count=4, seed=15)
+    b = Batch([m[3] for m in members], branches=2)
+    buf = Buffers(members)
+    buf.run(b)
+    members[1][3].set_precision("fp64")
+    members[1][3].set_timing(False)
+    members[2][3].set_precision("mixed")
+    members[2][3].set_timing(False)
+    e, f, phi = buf.run(b)
+    assert_same_as_single(members, e, f, phi)
+    b.close()
+
+
+@pytest.mark.gpu
 def test_batch_rejects_repeated_member():
     members = small_batch(count=2, seed=14)
     with pytest.raises(MSMError) as ex:

@@ -134,6 +134,30 @@ def test_four_levels_shared_stencil_width(precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_five_levels_headline_depth(precision):
+    """The grid hierarchy of the 1M-atom workload (215.30 A box, order 6,
+    cutoff 9 A, 5 levels, top grid 9^3): finest grid 144^3, the truncated
+    25^3 stencil at levels 1-3 (144^3, 72^3, 36^3), the full-period 18^3
+    stencil at level 4 and the 9^3 FFT at level 5 (code/forcefield1.c:158-191,
+    stencils code/forcefield0.c:661-675), here with 6,000 atoms: the reference
+    library's own energy and forces and the oracle's potentials
+    (tests/golden/make_golden_l5.py)."""
+    d = load("water215_L5")
+    ff = make_ff(d, precision)
+    assert (ff.levels, ff.top_grid) == (5, (9, 9, 9))
+    for level in (1, 2, 3):
+        assert ff.khat(level).shape == (25, 25, 25)
+    assert ff.khat(4).shape == (18, 18, 18)
+    e, f, phi = ff.energy(d["pos"], potentials=True)
+    te, tf, tp = TOL[precision]
+    scale = abs(float(d["energy"]))
+    assert abs(e - float(d["energy"])) / scale < te
+    assert force_err(f, d["force"], d["q"], d["edges"]) < tf
+    assert rel_rms(phi, d["phi"]) < tp
+    assert abs(0.5 * d["q"] @ phi - e) / scale < te * 10
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_level_weights(precision):
     """Weighted evaluation is linear in each level weight (the oracle's
     definition; the reference only defines unit weights)."""

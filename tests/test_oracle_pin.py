@@ -28,7 +28,16 @@ def oracle_for(d):
                   levels=p["levels"], top_grid=p["top_grid"])
 
 
-@pytest.mark.parametrize("case", [n for n in names() if not n.startswith("Box44")])
+# water215_L5 (the 5-level hierarchy of the 1M-atom workload) takes the
+# oracle about two minutes (the 144^3 grid with a 25^3 stencil); its
+# generator (tests/golden/make_golden_l5.py) ran the same comparison, to
+# 1e-12 in energy and 1e-11 in force, before writing the fixture, and
+# test_oracle_l5_parameters below checks the parameters it derives.
+SLOW_ORACLE = ("water215_L5",)
+
+
+@pytest.mark.parametrize("case", [n for n in names()
+                                  if not n.startswith("Box44") and n not in SLOW_ORACLE])
 def test_oracle_matches_reference_outputs(case):
     d = load(case)
     o = oracle_for(d)
@@ -43,6 +52,17 @@ def test_oracle_matches_reference_outputs(case):
         assert rel_rms(phi, d["phi"]) < 1e-10
     # the quadratic form: U = 1/2 sum_i q_i phi_i
     assert abs(0.5 * d["q"] @ phi - e) / abs(e) < 1e-12
+
+
+def test_oracle_l5_parameters():
+    """The oracle derives the reference's own level count, top grid and
+    stencil half-width for the 5-level fixture, and its stencil widths."""
+    d = load("water215_L5")
+    o = oracle_for(d)
+    assert (o.levels, o.nu, o.top_grid, o.nlim) == (
+        int(d["levels"]), int(d["nu"]), tuple(d["top_grid"]), int(d["nlim"]))
+    for level, width in ((1, 25), (2, 25), (3, 25), (4, 18)):
+        assert o.khat(level).shape == (width,) * 3
 
 
 def test_oracle_box44_published_energy():

@@ -50,6 +50,8 @@ def test_replica_timing_is_max_over_ranks(tmp_path):
 
 
 def test_reference_arm_under_two_ranks():
+    """One step of the reference arm (one FF_energy of the 1M-atom box on
+    one host core, about a minute here) under two ranks."""
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
            "--nproc-per-node=2", "--master-addr=127.0.0.1",
            "--master-port=%d" % _free_port(), "bench.py", "--impl", "reference",
@@ -61,3 +63,6 @@ def test_reference_arm_under_two_ranks():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2
     assert d["value"] > 0 and d["cpu_baseline"]["cores"] == 1
+    # the same workload as the GPU arm names
+    import bench
+    assert d["config"] == bench.WORKLOAD_CONFIG
