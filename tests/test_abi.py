@@ -13,11 +13,12 @@ import pytest
 from golden_cases import load, names, params
 from msmpb_b200 import _lib
 from msmpb_b200.forcefield import ForceField
+from oracle import build_ref
 from oracle.oracle import Oracle
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INCLUDE = os.path.join(ROOT, "include")
-REF_CODE = "/root/reference/code"
+REF_CODE = os.path.join(build_ref.REFERENCE, "code")
 
 
 def header_functions():

@@ -24,12 +24,13 @@ import pytest
 
 from msmpb_b200 import _lib
 from msmpb_b200.pme import PME, PMEError
+from oracle import build_ref
 from oracle.oracle import PmeOracle, RefPme
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(ROOT, "tests", "golden", "pme")
 INCLUDE = os.path.join(ROOT, "include")
-REF_CODE = "/root/reference/code"
+REF_CODE = os.path.join(build_ref.REFERENCE, "code")
 
 
 def cases():
