@@ -150,6 +150,7 @@ class Plan : public FFDevice {
   int tune_levels(size_t pad_cap, size_t part_cap);
   int launch_graph(const EvalRequest &r, cudaStream_t s, const double *pos,
                    const double *q, double *force, double *phi, double *edev);
+  PairClusterArgs<T> cluster_args() const;
   int enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
               const double *q, double *force, double *phi, double *energy);
   // Phase boundary: optional event, and with MSMPB_DEBUG_SYNC=1 (eager
@@ -736,6 +737,38 @@ int Plan<T>::enqueue_chain(cudaStream_t s, T *const *qg, T *const *eg, const dou
   return nl;
 }
 
+// Arguments of the cluster pair kernels over this plan's buffers
+template <typename T>
+PairClusterArgs<T> Plan<T>::cluster_args() const {
+  PairClusterArgs<T> ca{};
+  ca.maxcl = maxcl_;
+  ca.ncol = ncol_;
+  ca.nc0 = geom_.nc[0];
+  ca.nc1 = geom_.nc[1];
+  ca.nc2 = geom_.nc[2];
+  ca.K2 = K2_;
+  ca.ncoloff = ncoloff_;
+  const double rb = std::sqrt((double)pc_.a02) * (1.0 + 1e-4) + 1e-6;
+  ca.rbox2 = (float)(rb * rb);
+  const double rn = std::sqrt((double)pc_.close2) * (1.0 + 1e-4) + 1e-5;
+  ca.rnear2 = (float)(rn * rn);
+  ca.ortho = ortho_ ? 1 : 0;
+  ca.ozero = ozero_;
+  for (int k = 0; k < 3; ++k) ca.cw[k] = (float)(geom_.A[4 * k] / geom_.nc[k]);
+  for (int r = 0; r < 3; ++r) ca.cz[r] = cz_[r];
+  ca.start = pstart_;
+  ca.clstart = clstart_;
+  ca.coloff = coloff_d_;
+  ca.info = cinfo_;
+  ca.ubox = cubox_;
+  ca.cpos = cpos_;
+  ca.cpos64 = cpos64_;
+  ca.out = pout_;
+  ca.err = err_d_;
+  ca.self_images = self_images_ ? 1 : 0;
+  return ca;
+}
+
 template <typename T>
 int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
                      const double *q, double *force, double *phi,
@@ -772,32 +805,7 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   }
   mark(s, kPhasePair, tm);
   if (clusters) {
-    PairClusterArgs<T> ca{};
-    ca.maxcl = maxcl_;
-    ca.ncol = ncol_;
-    ca.nc0 = geom_.nc[0];
-    ca.nc1 = geom_.nc[1];
-    ca.nc2 = geom_.nc[2];
-    ca.K2 = K2_;
-    ca.ncoloff = ncoloff_;
-    const double rb = std::sqrt((double)pc_.a02) * (1.0 + 1e-4) + 1e-6;
-    ca.rbox2 = (float)(rb * rb);
-    const double rn = std::sqrt((double)pc_.close2) * (1.0 + 1e-4) + 1e-5;
-    ca.rnear2 = (float)(rn * rn);
-    ca.ortho = ortho_ ? 1 : 0;
-    ca.ozero = ozero_;
-    for (int k = 0; k < 3; ++k) ca.cw[k] = (float)(geom_.A[4 * k] / geom_.nc[k]);
-    for (int r = 0; r < 3; ++r) ca.cz[r] = cz_[r];
-    ca.start = pstart_;
-    ca.clstart = clstart_;
-    ca.coloff = coloff_d_;
-    ca.info = cinfo_;
-    ca.ubox = cubox_;
-    ca.cpos = cpos_;
-    ca.cpos64 = cpos64_;
-    ca.out = pout_;
-    ca.err = err_d_;
-    ca.self_images = self_images_ ? 1 : 0;
+    const PairClusterArgs<T> ca = cluster_args();
     launch_pair_clusters<T>(s, ca, pc_);
     nl += scan_launches(ncol_) + 1;
   } else if (pair_variant_ == 0 && pair_cells_supported(noff_, N_)) {
@@ -961,8 +969,12 @@ int Plan<T>::adjoint(const AdjointRequest &r) {
     ++nevals_;
   }
   launch_adj_gather<T>(s, N_, pperm_, r.fbar, fbs_);
-  launch_adj_pair<T>(s, N_, psorted_, fbs_, pcs_, pstart_, geom_, off_d_, noff_, pc_, adj_a_,
-                     adj_b_);
+  // the forward just run (or reused) built the clusters of these positions
+  if (pair_variant_ == 2 && clusters_ok_ && adj_pair_clusters_supported<T>())
+    launch_adj_pair_clusters<T>(s, cluster_args(), pc_, fbs_, adj_a_, adj_b_);
+  else
+    launch_adj_pair<T>(s, N_, psorted_, fbs_, pcs_, pstart_, geom_, off_d_, noff_, pc_,
+                       adj_a_, adj_b_);
   launch_adj_dipoles<T>(s, N_, gperm_, r.q, r.fbar, geom_, dip_);
   launch_adj_anterpolate<T>(s, grid_[1], gsorted_, gcs_, gstart_, sc_, dip_, qg2_[1],
                             anterp_scratch_, fold_tab_);

@@ -19,6 +19,8 @@
 // no atomics, fixed order, deterministic); per-column partial sums are added
 // with compensation in the mixed form, and pairs closer than sqrt(close2)
 // are queued per lane and summed in FP64 after the sweep.
+#include <cstdlib>
+
 #include "kernels.h"
 #include "pair_fn.cuh"
 
@@ -495,6 +497,655 @@ __device__ __forceinline__ void pair_clusters(const PairClusterArgs<T> &a,
   a.out[ci.first + ii] = r;
 }
 
+// ---- lanes over j atoms, the 8 i atoms in registers ----
+//
+// One warp per i-cluster as above, but lane = one j atom at a time and every
+// lane holds all 8 i atoms: a j atom costs one shared-memory load for 8 pairs
+// (in the mixed form evaluated two at a time in packed FP32: 4 independent
+// pair groups per j for the pipelines to overlap). Candidates are single
+// atoms: each (column, image) item's run of atoms (for orthorhombic boxes
+// only the cells that the cutoff sphere around the i-cluster box reaches
+// through the column's xy gap) is box-tested atom by atom against the
+// i-cluster's box, and passing atoms are queued in one of two rings: far ones
+// (farther than the close distance from the box: no pair of theirs can be
+// close or the atom itself) go the lean way; near ones are checked pair by
+// pair for the atom itself (skipped) and, in the mixed form, for close pairs
+// (recorded per lane, summed in FP64 after the sweep). Gather form: every
+// pair is summed once from each side; the lanes' partial sums are combined
+// by a fixed butterfly, so the result does not depend on timing.
+constexpr int kRing = 64;        // entries per queue ring (a warp adds <= 32 at a time)
+constexpr int kCloseLane = 6;    // close-pair records per lane and i-cluster
+constexpr int kGroupCap = 32 * kCloseLane;
+
+// One warp's (column, image) items of the current Phase A batch
+struct JlItems {
+  int off[32], s0[32], a0[32], code[32];
+  double shift[32][3];
+};
+
+template <typename T>
+struct JlShared {
+  JlItems items[kWarps];
+  V4<T> far[kWarps][kRing], near[kWarps][kRing];
+  int2 ninfo[kWarps][kRing];
+  int2 rec[kWarps][sizeof(T) == 4 ? 32 * kCloseLane : 1];
+  int2 grp[kWarps][sizeof(T) == 4 ? kGroupCap : 1];
+};
+
+// The candidate j atoms of i-cluster u for one warp. Phase A: the (column,
+// periodic image) items, 32 at a time, one per lane: each item's run of
+// sorted atoms (the cells along the column within K2 of the cluster's cells,
+// for orthorhombic boxes only those the cutoff sphere around the cluster's
+// box reaches through the column's xy gap). Phase B: the concatenated runs,
+// 32 atoms at a time, one per lane: the atom is shifted into the i-cluster's
+// frame and tested against its box. `batch(pass, near, J, jslot, jcode,
+// selfk, sorted)` is called by the whole warp once per batch: pass, the
+// atom is within the cutoff (plus margin) of the box; near, within the close
+// distance of it, or it is an atom of the cluster itself (selfk = its slot
+// in the cluster, else -1); J the shifted position and charge; jslot the
+// atom's cluster slot, jcode its item's (column offset << 8 | image + 128),
+// sorted its index in pair-cell order.
+template <typename T, bool SELF, typename Batch>
+__device__ __forceinline__ void jl_sweep(const PairClusterArgs<T> &a, const ClusterInfo &ci,
+                                         int u, int lane, JlItems &it_sh, Batch &&batch) {
+  const int cx = ci.col / a.nc1, cy = ci.col - cx * a.nc1;
+  const int lo = ci.czf - a.K2, hi = ci.czl + a.K2;
+  const int klo = floor_div(lo, a.nc2);
+  const int nseg = floor_div(hi, a.nc2) - klo + 1;
+  const int nitems = a.ncoloff * nseg;
+  for (int i0 = 0; i0 < nitems; i0 += 32) {
+    int nat = 0, s0 = 0, A = 0, code = 0;
+    double shx = 0., shy = 0., shz = 0.;
+    const int it = i0 + lane;
+    if (it < nitems) {
+      const int o = nseg == 1 ? it : it / nseg;
+      const int k = klo + (it - o * nseg);
+      const ColumnOffset &co = a.coloff[o];
+      int x = cx + co.du, y = cy + co.dv;
+      while (x < 0) x += a.nc0;
+      while (x >= a.nc0) x -= a.nc0;
+      while (y < 0) y += a.nc1;
+      while (y >= a.nc1) y -= a.nc1;
+      int wlo = lo, whi = hi;
+      if (a.ortho) {
+        // the column's slab in the i frame: x in [bx, bx + cw0), y likewise
+        const float bx = (float)co.base[0], by = (float)co.base[1];
+        const float gx =
+            fmaxf(fmaxf(bx - (ci.c.x + ci.h.x), (ci.c.x - ci.h.x) - (bx + a.cw[0])), 0.f);
+        const float gy =
+            fmaxf(fmaxf(by - (ci.c.y + ci.h.y), (ci.c.y - ci.h.y) - (by + a.cw[1])), 0.f);
+        const float rem = a.rbox2 - gx * gx - gy * gy;
+        if (rem <= 0.f) {
+          whi = wlo - 1;
+        } else {
+          const float hw = sqrtf(rem) + 1e-3f;
+          wlo = max(wlo, ci.czf + (int)floorf((ci.c.z - ci.h.z - hw) / a.cw[2]));
+          whi = min(whi, ci.czf + (int)floorf((ci.c.z + ci.h.z + hw) / a.cw[2]));
+        }
+      }
+      const int col = x * a.nc1 + y;
+      const int cb = col * a.nc2;
+      const int c0 = max(wlo, k * a.nc2) - k * a.nc2;
+      const int c1 = min(whi, k * a.nc2 + a.nc2 - 1) - k * a.nc2;
+      if (c0 <= c1) {
+        A = a.start[cb + c0];
+        const int B = a.start[cb + c1 + 1];
+        if (A < B) {
+          nat = B - A;
+          s0 = 8 * a.clstart[col] + (A - a.start[cb]);
+        }
+      }
+      code = (o << 8) | (k + 128);
+      const double dz = (double)(k * a.nc2 - ci.czf);
+      shx = co.base[0] + dz * a.cz[0];
+      shy = co.base[1] + dz * a.cz[1];
+      shz = co.base[2] + dz * a.cz[2];
+    }
+    int incl = nat;
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, dd);
+      if (lane >= dd) incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    it_sh.off[lane] = incl - nat;
+    it_sh.s0[lane] = s0;
+    it_sh.a0[lane] = A;
+    it_sh.code[lane] = code;
+    it_sh.shift[lane][0] = shx;
+    it_sh.shift[lane][1] = shy;
+    it_sh.shift[lane][2] = shz;
+    __syncwarp();
+    for (int b0 = 0; b0 < total; b0 += 32) {
+      const int c = b0 + lane;
+      bool pass = false, near = false;
+      V4<T> J{};
+      int jslot = 0, jcode = 0, selfk = -1, sorted = 0;
+      if (c < total) {
+        int j = 0;  // last item starting at or before c
+#pragma unroll
+        for (int step = 16; step; step >>= 1)
+          if (it_sh.off[j + step] <= c) j += step;
+        jslot = it_sh.s0[j] + (c - it_sh.off[j]);
+        sorted = it_sh.a0[j] + (c - it_sh.off[j]);
+        jcode = it_sh.code[j];
+        J = a.cpos[jslot];
+        const int jc = jslot >> 3;
+        const double czj = (double)__float_as_int(a.ubox[2 * jc].c.w);
+        J.x += (T)(it_sh.shift[j][0] + czj * a.cz[0]);
+        J.y += (T)(it_sh.shift[j][1] + czj * a.cz[1]);
+        J.z += (T)(it_sh.shift[j][2] + czj * a.cz[2]);
+        const float gx = fmaxf(fabsf((float)J.x - ci.c.x) - ci.h.x, 0.f);
+        const float gy = fmaxf(fabsf((float)J.y - ci.c.y) - ci.h.y, 0.f);
+        const float gz = fmaxf(fabsf((float)J.z - ci.c.z) - ci.h.z, 0.f);
+        const float g2 = gx * gx + gy * gy + gz * gz;
+        pass = g2 < a.rbox2;
+        near = g2 < a.rnear2;
+        if (jc == u && (SELF || ((jcode >> 8) == a.ozero && (jcode & 255) == 128))) {
+          selfk = jslot & 7;
+          near = true;
+        }
+      }
+      batch(pass, near, J, jslot, jcode, selfk, sorted);
+    }
+  }
+}
+
+// lanes' 32 partial sums -> lane l holds the total of value l (fixed order)
+template <typename T>
+__device__ __forceinline__ T butterfly32(T (&v)[32], int lane) {
+#pragma unroll
+  for (int sft = 16; sft >= 1; sft >>= 1) {
+    const bool up = (lane & sft) != 0;
+#pragma unroll
+    for (int k = 0; k < sft; ++k) {
+      const T send = up ? v[k] : v[k + sft];
+      const T keep = up ? v[k + sft] : v[k];
+      v[k] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
+    }
+  }
+  return v[0];
+}
+
+// One lane's 8 i atoms (negated: d = x_j - x_i) and partial sums: q_j V in
+// p and q_j g d in x/y/z, g = -f = 1/r^3 + 2 tau'(s)/a0^3 (the field is
+// -sum q_j g d). FP32: packed pairs (2p, 2p+1); FP64: scalars.
+template <typename T> struct JlLane;
+
+template <>
+struct JlLane<float> {
+  float2 nix[4], niy[4], niz[4];
+  float2 ax[4], ay[4], az[4], ap[4];
+  __device__ __forceinline__ void set(int k, const V4<float> &a) {
+    float *x = reinterpret_cast<float *>(&nix[k >> 1]) + (k & 1);
+    float *y = reinterpret_cast<float *>(&niy[k >> 1]) + (k & 1);
+    float *z = reinterpret_cast<float *>(&niz[k >> 1]) + (k & 1);
+    *x = -a.x;
+    *y = -a.y;
+    *z = -a.z;
+  }
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int p = 0; p < 4; ++p) ax[p] = ay[p] = az[p] = ap[p] = make_float2(0.f, 0.f);
+  }
+  __device__ __forceinline__ void values(float (&v)[32]) const {
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      v[2 * p] = ax[p].x;
+      v[2 * p + 1] = ax[p].y;
+      v[8 + 2 * p] = ay[p].x;
+      v[8 + 2 * p + 1] = ay[p].y;
+      v[16 + 2 * p] = az[p].x;
+      v[16 + 2 * p + 1] = az[p].y;
+      v[24 + 2 * p] = ap[p].x;
+      v[24 + 2 * p + 1] = ap[p].y;
+    }
+  }
+  // The 8 pairs of one j atom (position in the i-cluster's frame, charge in
+  // J.w). NEAR: the pair with i atom `selfk` is the atom itself (skipped),
+  // and pairs closer than sqrt(close2) are recorded for the FP64 pass while
+  // the lane's record has room (else summed here).
+  template <int NU, bool NEAR>
+  __device__ __forceinline__ void pairs(const PairConsts<float> &pc, const V4<float> &J,
+                                        int selfk, int jslot, int code, int2 *myrec,
+                                        int &nrec) {
+    const float2 jx = make_float2(J.x, J.x), jy = make_float2(J.y, J.y),
+                 jz = make_float2(J.z, J.z);
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      const float2 dx = __fadd2_rn(jx, nix[p]);
+      const float2 dy = __fadd2_rn(jy, niy[p]);
+      const float2 dz = __fadd2_rn(jz, niz[p]);
+      float2 r2 = __fmul2_rn(dx, dx);
+      r2 = __ffma2_rn(dy, dy, r2);
+      r2 = __ffma2_rn(dz, dz, r2);
+      bool h0 = r2.x < pc.a02, h1 = r2.y < pc.a02;
+      if constexpr (NEAR) {
+        if (selfk == 2 * p) h0 = false;
+        if (selfk == 2 * p + 1) h1 = false;
+        if (h0 && r2.x < pc.close2 && nrec < kCloseLane) {
+          myrec[nrec++] = make_int2(jslot, code | ((2 * p) << 24));
+          h0 = false;
+        }
+        if (h1 && r2.y < pc.close2 && nrec < kCloseLane) {
+          myrec[nrec++] = make_int2(jslot, code | ((2 * p + 1) << 24));
+          h1 = false;
+        }
+      }
+      const float2 rr = make_float2(h0 ? r2.x : pc.a02, h1 ? r2.y : pc.a02);
+      const float2 qj = make_float2(h0 ? J.w : 0.f, h1 ? J.w : 0.f);
+      float2 v, g;
+      if constexpr (NU == 0) {  // PME kernel, packed (pair_fn.cuh)
+        float2 f;
+        pme_radial2(pc, rr, v, f);
+        g = make_float2(-f.x, -f.y);
+      } else {
+        const float2 s = __ffma2_rn(rr, make_float2(pc.inv_a02, pc.inv_a02),
+                                    make_float2(-1.f, -1.f));
+        // tau(s) and tau'(s) by two independent Horner chains
+        float2 ts = make_float2(pc.tau[NU - 1], pc.tau[NU - 1]);
+        float2 t1 = make_float2((NU - 1) * pc.tau[NU - 1], (NU - 1) * pc.tau[NU - 1]);
+#pragma unroll
+        for (int m = NU - 2; m >= 0; --m) {
+          ts = __ffma2_rn(s, ts, make_float2(pc.tau[m], pc.tau[m]));
+          if (m >= 1) t1 = __ffma2_rn(s, t1, make_float2(m * pc.tau[m], m * pc.tau[m]));
+        }
+        const float2 rinv = make_float2(rsqrtf(rr.x), rsqrtf(rr.y));
+        v = __ffma2_rn(ts, make_float2(-pc.inv_a0, -pc.inv_a0), rinv);
+        const float2 rinv3 = __fmul2_rn(__fmul2_rn(rinv, rinv), rinv);
+        g = __ffma2_rn(t1, make_float2(pc.two_inv_a03, pc.two_inv_a03), rinv3);
+      }
+      ap[p] = __ffma2_rn(qj, v, ap[p]);
+      const float2 w = __fmul2_rn(qj, g);
+      ax[p] = __ffma2_rn(w, dx, ax[p]);
+      ay[p] = __ffma2_rn(w, dy, ay[p]);
+      az[p] = __ffma2_rn(w, dz, az[p]);
+    }
+  }
+};
+
+template <>
+struct JlLane<double> {
+  double nix[8], niy[8], niz[8];
+  double ax[8], ay[8], az[8], ap[8];
+  __device__ __forceinline__ void set(int k, const V4<double> &a) {
+    nix[k] = -a.x;
+    niy[k] = -a.y;
+    niz[k] = -a.z;
+  }
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) ax[k] = ay[k] = az[k] = ap[k] = 0.;
+  }
+  __device__ __forceinline__ void values(double (&v)[32]) const {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      v[k] = ax[k];
+      v[8 + k] = ay[k];
+      v[16 + k] = az[k];
+      v[24 + k] = ap[k];
+    }
+  }
+  // NEAR: only the atom itself is skipped (the FP64 form has no close path)
+  template <int NU, bool NEAR>
+  __device__ __forceinline__ void pairs(const PairConsts<double> &pc, const V4<double> &J,
+                                        int selfk, int, int, int2 *, int &) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const double dx = J.x + nix[k], dy = J.y + niy[k], dz = J.z + niz[k];
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      bool h = r2 < pc.a02;
+      if constexpr (NEAR) {
+        if (selfk == k) h = false;
+      }
+      const double rr = h ? r2 : pc.a02;
+      const double qj = h ? J.w : 0.;
+      double v, f;
+      pair_radial<double, NU>(pc, rr, v, f);
+      ap[k] = fma(qj, v, ap[k]);
+      const double w = -qj * f;
+      ax[k] = fma(w, dx, ax[k]);
+      ay[k] = fma(w, dy, ay[k]);
+      az[k] = fma(w, dz, az[k]);
+    }
+  }
+};
+
+template <typename T, int NU, bool SELF>
+__device__ __forceinline__ void pair_jl(const PairClusterArgs<T> &a, const PairConsts<T> &pc) {
+  constexpr bool kMixed = sizeof(T) == 4;
+  __shared__ JlShared<T> sh;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int u = blockIdx.x * kWarps + warp;
+  if (u >= a.maxcl || u >= a.clstart[a.ncol]) return;  // whole warp
+  const ClusterInfo ci = a.info[u];
+  const unsigned lt = (1u << lane) - 1u;
+  JlLane<T> L;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    V4<T> ak = a.cpos[u * 8 + k];
+    if (k >= ci.n) ak.x = ak.y = ak.z = -(T)kFar;
+    L.set(k, ak);
+  }
+  L.zero();
+  int2 *myrec = kMixed ? &sh.rec[warp][lane * kCloseLane] : nullptr;
+  int nrec = 0;
+  unsigned fhead = 0, ftail = 0, nhead = 0, ntail = 0;
+  const V4<T> dummy{(T)kFar, (T)kFar, (T)kFar, T(0)};
+
+  auto far_step = [&](int cnt) {
+    V4<T> J = sh.far[warp][(fhead + lane) & (kRing - 1)];
+    if (lane >= cnt) J = dummy;
+    L.template pairs<NU, false>(pc, J, -1, 0, 0, myrec, nrec);
+    fhead += cnt;
+  };
+  auto near_step = [&](int cnt) {
+    const int e = (nhead + lane) & (kRing - 1);
+    V4<T> J = sh.near[warp][e];
+    int2 inf = sh.ninfo[warp][e];
+    if (lane >= cnt) {
+      J = dummy;
+      inf = make_int2(0, 0);
+    }
+    L.template pairs<NU, true>(pc, J, (inf.y >> 24) - 1, inf.x, inf.y & 0xffffff, myrec,
+                               nrec);
+    nhead += cnt;
+  };
+  jl_sweep<T, SELF>(a, ci, u, lane, sh.items[warp],
+                    [&](bool pass, bool near, const V4<T> &J, int jslot, int jcode,
+                        int selfk, int) {
+    const unsigned mf = __ballot_sync(0xffffffffu, pass && !near);
+    const unsigned mn = __ballot_sync(0xffffffffu, pass && near);
+    if (pass && !near) sh.far[warp][(ftail + __popc(mf & lt)) & (kRing - 1)] = J;
+    if (pass && near) {
+      const int e = (ntail + __popc(mn & lt)) & (kRing - 1);
+      sh.near[warp][e] = J;
+      sh.ninfo[warp][e] = make_int2(jslot, jcode | ((selfk + 1) << 24));
+    }
+    ftail += __popc(mf);
+    ntail += __popc(mn);
+    __syncwarp();
+    if (ftail - fhead >= 32) far_step(32);
+    if (ntail - nhead >= 32) near_step(32);
+    __syncwarp();
+  });
+  if (ftail != fhead) far_step((int)(ftail - fhead));
+  if (ntail != nhead) near_step((int)(ntail - nhead));
+
+  // lanes' partial sums: lane l ends with value l = 8 c + i (c: 0..2 the
+  // negated field components, 3 the potential; i the atom)
+  T v[32];
+  L.values(v);
+  const T vsum = butterfly32(v, lane);
+  const int i = lane & 7, c = lane >> 3;
+  double close = 0.;
+  if constexpr (kMixed) {
+    // close pairs in FP64: the lanes' records regrouped by i atom (counts
+    // of the 8 atoms packed in the bytes of a 64-bit word, scanned over
+    // lanes), then lane (i, sub = lane >> 3) sums every 4th record of atom
+    // i, and the four subs are added in a fixed order
+    unsigned long long cnt = 0;
+    for (int t = 0; t < nrec; ++t) cnt += 1ull << (8 * (myrec[t].y >> 24));
+    unsigned long long incl = cnt;
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, dd);
+      if (lane >= dd) incl += y;
+    }
+    const unsigned long long tot = __shfl_sync(0xffffffffu, incl, 31);
+    double cf[4] = {0., 0., 0., 0.};
+    if (tot) {
+      const unsigned long long base = tot * 0x0101010101010100ull;  // exclusive byte prefix
+      unsigned long long pos = base + (incl - cnt);
+      for (int t = 0; t < nrec; ++t) {
+        const int ia = myrec[t].y >> 24;
+        const int at = (int)((pos >> (8 * ia)) & 255);
+        pos += 1ull << (8 * ia);
+        sh.grp[warp][at] = myrec[t];
+      }
+      __syncwarp();
+      const int sub = lane >> 3;
+      const int gb = (int)((base >> (8 * i)) & 255), gn = (int)((tot >> (8 * i)) & 255);
+      if (gn > sub) {
+        const V4<double> ai64 = a.cpos64[u * 8 + i];
+        for (int t = sub; t < gn; t += 4) {
+          const int2 r = sh.grp[warp][gb + t];
+          const int jslot = r.x, code = r.y & 0xffffff;
+          const int o = code >> 8, k = (code & 255) - 128;
+          const ColumnOffset &co = a.coloff[o];
+          const int dzc = __float_as_int(a.ubox[2 * (jslot >> 3)].c.w) + k * a.nc2 - ci.czf;
+          close_pair64<NU>(pc, ai64, a.cpos64[jslot], co.base[0] + dzc * a.cz[0],
+                           co.base[1] + dzc * a.cz[1], co.base[2] + dzc * a.cz[2], cf[0],
+                           cf[1], cf[2], cf[3]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        cf[q] += __shfl_xor_sync(0xffffffffu, cf[q], 8);
+        cf[q] += __shfl_xor_sync(0xffffffffu, cf[q], 16);
+      }
+    }
+    // lane l = 8 c + i takes atom i's FP64 close sum of component c
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double x = __shfl_sync(0xffffffffu, cf[q], i);
+      if (q == c) close = x;
+    }
+  }
+  if (i >= ci.n) return;
+  T r;
+  if (c < 3) {
+    double qi;
+    if constexpr (kMixed) qi = a.cpos64[u * 8 + i].w;
+    else qi = (double)a.cpos[u * 8 + i].w;
+    r = (T)(qi * (close - (double)vsum));
+  } else {
+    r = (T)((double)vsum + close);
+  }
+  reinterpret_cast<T *>(&a.out[ci.first + i])[c] = r;
+}
+
+template <int NU, bool SELF>
+__global__ void __launch_bounds__(kWarps * 32)
+k_pair_jl_f32(PairClusterArgs<float> a, PairConsts<float> pc) {
+  pair_jl<float, NU, SELF>(a, pc);
+}
+
+template <int NU, bool SELF>
+__global__ void __launch_bounds__(kWarps * 32)
+k_pair_jl_f64(PairClusterArgs<double> a, PairConsts<double> pc) {
+  pair_jl<double, NU, SELF>(a, pc);
+}
+
+// ---- adjoint short-range pass on the same sweep (mixed form) ----
+// Per atom k, d = r_j - r_k (the short-range terms of dL/dq_k and dL/dr_k,
+// as k_adjoint.cu's k_adj_pair computes them):
+//   E_k = sum_j q_j g1 d,  psi_k = sum_j q_j g1 (Fbar_j . d),
+//   h_k = sum_j q_j [g1 (Fbar_j - Fbar_k) + g2 d (d . (Fbar_j - Fbar_k))],
+//   g1 = -1/r^3 - (2/a0^3) tau'(s),  g2 = 3/r^5 - (4/a0^5) tau''(s).
+// Lanes over j atoms with the 8 i atoms (position and Fbar) in registers,
+// packed FP32 as in the forward; the atom itself skipped at every image
+// that reaches it (entries of the i-cluster take the checked path).
+template <int NU>
+struct AdjLane {
+  float2 nix[4], niy[4], niz[4], nfx[4], nfy[4], nfz[4];  // -position, -Fbar
+  float2 ex[4], ey[4], ez[4], ps[4], hx[4], hy[4], hz[4];
+  template <bool SELFCHECK>
+  __device__ __forceinline__ void pairs(const PairConsts<float> &pc, const V4<float> &J,
+                                        const V4<float> &F, int selfk) {
+    const float2 jx = make_float2(J.x, J.x), jy = make_float2(J.y, J.y),
+                 jz = make_float2(J.z, J.z);
+    const float2 Fx = make_float2(F.x, F.x), Fy = make_float2(F.y, F.y),
+                 Fz = make_float2(F.z, F.z);
+    const float c2 = 2.f * pc.two_inv_a03 * pc.inv_a02;  // 4 / a0^5
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      const float2 dx = __fadd2_rn(jx, nix[p]);
+      const float2 dy = __fadd2_rn(jy, niy[p]);
+      const float2 dz = __fadd2_rn(jz, niz[p]);
+      float2 r2 = __fmul2_rn(dx, dx);
+      r2 = __ffma2_rn(dy, dy, r2);
+      r2 = __ffma2_rn(dz, dz, r2);
+      bool h0 = r2.x < pc.a02, h1 = r2.y < pc.a02;
+      if constexpr (SELFCHECK) {
+        if (selfk == 2 * p) h0 = false;
+        if (selfk == 2 * p + 1) h1 = false;
+      }
+      const float2 rr = make_float2(h0 ? r2.x : pc.a02, h1 ? r2.y : pc.a02);
+      const float2 qj = make_float2(h0 ? J.w : 0.f, h1 ? J.w : 0.f);
+      const float2 s = __ffma2_rn(rr, make_float2(pc.inv_a02, pc.inv_a02),
+                                  make_float2(-1.f, -1.f));
+      // tau'(s) and tau''(s)/2 by independent Horner chains
+      float2 p1 = make_float2((NU - 1) * pc.tau[NU - 1], (NU - 1) * pc.tau[NU - 1]);
+      const float h2 = 0.5f * (NU - 1) * (NU - 2) * pc.tau[NU - 1];
+      float2 p2 = make_float2(h2, h2);
+#pragma unroll
+      for (int m = NU - 2; m >= 1; --m) {
+        p1 = __ffma2_rn(s, p1, make_float2(m * pc.tau[m], m * pc.tau[m]));
+        if (m >= 2) {
+          const float cm = 0.5f * m * (m - 1) * pc.tau[m];
+          p2 = __ffma2_rn(s, p2, make_float2(cm, cm));
+        }
+      }
+      const float2 rinv = make_float2(rsqrtf(rr.x), rsqrtf(rr.y));
+      const float2 rinv2 = __fmul2_rn(rinv, rinv);
+      const float2 rinv3 = __fmul2_rn(rinv2, rinv);
+      // g1 = -(rinv3 + p1 2/a0^3); g2 = 3 rinv3 rinv2 - 2 p2 (4/a0^5)
+      const float2 g1 = __fmul2_rn(
+          __ffma2_rn(p1, make_float2(pc.two_inv_a03, pc.two_inv_a03), rinv3),
+          make_float2(-1.f, -1.f));
+      const float2 g2 = __ffma2_rn(p2, make_float2(-2.f * c2, -2.f * c2),
+                                   __fmul2_rn(__fmul2_rn(rinv3, rinv2), make_float2(3.f, 3.f)));
+      const float2 w1 = __fmul2_rn(qj, g1);
+      ex[p] = __ffma2_rn(w1, dx, ex[p]);
+      ey[p] = __ffma2_rn(w1, dy, ey[p]);
+      ez[p] = __ffma2_rn(w1, dz, ez[p]);
+      float2 fd = __fmul2_rn(Fx, dx);
+      fd = __ffma2_rn(Fy, dy, fd);
+      fd = __ffma2_rn(Fz, dz, fd);
+      ps[p] = __ffma2_rn(w1, fd, ps[p]);
+      const float2 Dx = __fadd2_rn(Fx, nfx[p]), Dy = __fadd2_rn(Fy, nfy[p]),
+                   Dz = __fadd2_rn(Fz, nfz[p]);
+      float2 dD = __fmul2_rn(dx, Dx);
+      dD = __ffma2_rn(dy, Dy, dD);
+      dD = __ffma2_rn(dz, Dz, dD);
+      const float2 w2 = __fmul2_rn(__fmul2_rn(qj, g2), dD);
+      hx[p] = __ffma2_rn(w2, dx, __ffma2_rn(w1, Dx, hx[p]));
+      hy[p] = __ffma2_rn(w2, dy, __ffma2_rn(w1, Dy, hy[p]));
+      hz[p] = __ffma2_rn(w2, dz, __ffma2_rn(w1, Dz, hz[p]));
+    }
+  }
+};
+
+struct AdjShared {
+  JlItems items[kWarps];
+  V4<float> far[kWarps][kRing][2], self[kWarps][kRing][2];
+};
+
+template <int NU, bool SELF>
+__global__ void __launch_bounds__(kWarps * 32)
+k_adj_pair_jl(PairClusterArgs<float> a, PairConsts<float> pc, const V4<float> *__restrict__ fbs,
+              V4<float> *__restrict__ out_a, V4<float> *__restrict__ out_b) {
+  __shared__ AdjShared sh;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int u = blockIdx.x * kWarps + warp;
+  if (u >= a.maxcl || u >= a.clstart[a.ncol]) return;  // whole warp
+  const ClusterInfo ci = a.info[u];
+  const unsigned lt = (1u << lane) - 1u;
+  AdjLane<NU> L;
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    V4<float> a0 = a.cpos[u * 8 + 2 * p], a1 = a.cpos[u * 8 + 2 * p + 1];
+    V4<float> f0{0.f, 0.f, 0.f, 0.f}, f1 = f0;
+    if (2 * p < ci.n) f0 = fbs[ci.first + 2 * p];
+    else a0.x = a0.y = a0.z = -kFar;
+    if (2 * p + 1 < ci.n) f1 = fbs[ci.first + 2 * p + 1];
+    else a1.x = a1.y = a1.z = -kFar;
+    L.nix[p] = make_float2(-a0.x, -a1.x);
+    L.niy[p] = make_float2(-a0.y, -a1.y);
+    L.niz[p] = make_float2(-a0.z, -a1.z);
+    L.nfx[p] = make_float2(-f0.x, -f1.x);
+    L.nfy[p] = make_float2(-f0.y, -f1.y);
+    L.nfz[p] = make_float2(-f0.z, -f1.z);
+    L.ex[p] = L.ey[p] = L.ez[p] = L.ps[p] = L.hx[p] = L.hy[p] = L.hz[p] =
+        make_float2(0.f, 0.f);
+  }
+  unsigned fhead = 0, ftail = 0, shead = 0, stail = 0;
+  const V4<float> dummy{kFar, kFar, kFar, 0.f};
+  auto far_step = [&](int cnt) {
+    const int e = (fhead + lane) & (kRing - 1);
+    V4<float> J = sh.far[warp][e][0], F = sh.far[warp][e][1];
+    if (lane >= cnt) J = dummy;
+    L.template pairs<false>(pc, J, F, -1);
+    fhead += cnt;
+  };
+  auto self_step = [&](int cnt) {
+    const int e = (shead + lane) & (kRing - 1);
+    V4<float> J = sh.self[warp][e][0], F = sh.self[warp][e][1];
+    if (lane >= cnt) J = dummy;
+    L.template pairs<true>(pc, J, F, __float_as_int(F.w));
+    shead += cnt;
+  };
+  jl_sweep<float, SELF>(a, ci, u, lane, sh.items[warp],
+                        [&](bool pass, bool, const V4<float> &J, int, int, int selfk,
+                            int sorted) {
+    V4<float> F{0.f, 0.f, 0.f, 0.f};
+    if (pass) F = fbs[sorted];
+    F.w = __int_as_float(selfk);
+    const bool own = selfk >= 0;
+    const unsigned mf = __ballot_sync(0xffffffffu, pass && !own);
+    const unsigned ms = __ballot_sync(0xffffffffu, pass && own);
+    if (pass && !own) {
+      const int e = (ftail + __popc(mf & lt)) & (kRing - 1);
+      sh.far[warp][e][0] = J;
+      sh.far[warp][e][1] = F;
+    }
+    if (pass && own) {
+      const int e = (stail + __popc(ms & lt)) & (kRing - 1);
+      sh.self[warp][e][0] = J;
+      sh.self[warp][e][1] = F;
+    }
+    ftail += __popc(mf);
+    stail += __popc(ms);
+    __syncwarp();
+    if (ftail - fhead >= 32) far_step(32);
+    if (stail - shead >= 32) self_step(32);
+    __syncwarp();
+  });
+  if (ftail != fhead) far_step((int)(ftail - fhead));
+  if (stail != shead) self_step((int)(stail - shead));
+
+  const int i = lane & 7, c = lane >> 3;
+  float v[32];
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    v[2 * p] = L.ex[p].x;
+    v[2 * p + 1] = L.ex[p].y;
+    v[8 + 2 * p] = L.ey[p].x;
+    v[8 + 2 * p + 1] = L.ey[p].y;
+    v[16 + 2 * p] = L.ez[p].x;
+    v[16 + 2 * p + 1] = L.ez[p].y;
+    v[24 + 2 * p] = L.ps[p].x;
+    v[24 + 2 * p + 1] = L.ps[p].y;
+  }
+  const float ra = butterfly32(v, lane);
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    v[2 * p] = L.hx[p].x;
+    v[2 * p + 1] = L.hx[p].y;
+    v[8 + 2 * p] = L.hy[p].x;
+    v[8 + 2 * p + 1] = L.hy[p].y;
+    v[16 + 2 * p] = L.hz[p].x;
+    v[16 + 2 * p + 1] = L.hz[p].y;
+    v[24 + 2 * p] = 0.f;
+    v[24 + 2 * p + 1] = 0.f;
+  }
+  const float rb = butterfly32(v, lane);
+  if (i >= ci.n) return;
+  reinterpret_cast<float *>(&out_a[ci.first + i])[c] = ra;
+  reinterpret_cast<float *>(&out_b[ci.first + i])[c] = rb;
+}
+
 // One kernel per precision, for the register budget: FP32 keeps the
 // compiler's own choice (72 registers; an occupancy hint made the packed path
 // slower), FP64 targets 8 CTAs per SM (64 registers, a few spilled words,
@@ -516,14 +1167,25 @@ void launch_nu(cudaStream_t s, const PairClusterArgs<T> &a, const PairConsts<T> 
   const int blocks = std::max(1, (a.maxcl + kWarps - 1) / kWarps);
   if constexpr (sizeof(T) == 4) {
     if (a.self_images)
-      k_pair_clusters_f32<NU, true><<<blocks, kWarps * 32, 0, s>>>(a, pc);
+      k_pair_jl_f32<NU, true><<<blocks, kWarps * 32, 0, s>>>(a, pc);
     else
-      k_pair_clusters_f32<NU, false><<<blocks, kWarps * 32, 0, s>>>(a, pc);
+      k_pair_jl_f32<NU, false><<<blocks, kWarps * 32, 0, s>>>(a, pc);
   } else {
-    if (a.self_images)
+    // FP64 form: the tile kernel, or with MSMPB_PAIR_FP64=jl the j-lane one
+    static const bool jl = [] {
+      const char *v = std::getenv("MSMPB_PAIR_FP64");
+      return v && v[0] == 'j';
+    }();
+    if (jl) {
+      if (a.self_images)
+        k_pair_jl_f64<NU, true><<<blocks, kWarps * 32, 0, s>>>(a, pc);
+      else
+        k_pair_jl_f64<NU, false><<<blocks, kWarps * 32, 0, s>>>(a, pc);
+    } else if (a.self_images) {
       k_pair_clusters_f64<NU, true><<<blocks, kWarps * 32, 0, s>>>(a, pc);
-    else
+    } else {
       k_pair_clusters_f64<NU, false><<<blocks, kWarps * 32, 0, s>>>(a, pc);
+    }
   }
 }
 
@@ -540,6 +1202,30 @@ void launch_cluster_fill(cudaStream_t s, int maxcl, int ncol, int nc2,
   const int blocks = (int)std::max<long>(1, (threads + 255) / 256);
   k_cluster_fill<T><<<blocks, 256, 0, s>>>(maxcl, ncol, nc2, start, clstart, pcs, src64,
                                            cz[0], cz[1], cz[2], cpos, cpos64, info, ubox);
+}
+
+template <typename T>
+bool adj_pair_clusters_supported() { return sizeof(T) == 4; }
+
+template <typename T>
+void launch_adj_pair_clusters(cudaStream_t s, const PairClusterArgs<T> &a,
+                              const PairConsts<T> &pc, const V4<T> *fbs, V4<T> *out_a,
+                              V4<T> *out_b) {
+  if constexpr (sizeof(T) == 4) {
+    const int blocks = std::max(1, (a.maxcl + kWarps - 1) / kWarps);
+#define MSM_ADJ_JL(NUV)                                                                 \
+  if (a.self_images)                                                                    \
+    k_adj_pair_jl<NUV, true><<<blocks, kWarps * 32, 0, s>>>(a, pc, fbs, out_a, out_b);  \
+  else                                                                                  \
+    k_adj_pair_jl<NUV, false><<<blocks, kWarps * 32, 0, s>>>(a, pc, fbs, out_a, out_b)
+    switch (pc.nu) {
+      case 4: MSM_ADJ_JL(4); break;
+      case 6: MSM_ADJ_JL(6); break;
+      case 8: MSM_ADJ_JL(8); break;
+      default: MSM_ADJ_JL(10); break;
+    }
+#undef MSM_ADJ_JL
+  }
 }
 
 template <typename T>
@@ -564,6 +1250,14 @@ template void launch_cluster_fill<double>(cudaStream_t, int, int, int, const int
                                           ClusterInfo *, UnitBox *);
 template void launch_pair_clusters<float>(cudaStream_t, const PairClusterArgs<float> &,
                                           const PairConsts<float> &);
+template bool adj_pair_clusters_supported<float>();
+template bool adj_pair_clusters_supported<double>();
+template void launch_adj_pair_clusters<float>(cudaStream_t, const PairClusterArgs<float> &,
+                                              const PairConsts<float> &, const V4<float> *,
+                                              V4<float> *, V4<float> *);
+template void launch_adj_pair_clusters<double>(cudaStream_t, const PairClusterArgs<double> &,
+                                               const PairConsts<double> &, const V4<double> *,
+                                               V4<double> *, V4<double> *);
 template void launch_pair_clusters<double>(cudaStream_t, const PairClusterArgs<double> &,
                                            const PairConsts<double> &);
 

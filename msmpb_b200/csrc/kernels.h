@@ -195,6 +195,15 @@ void launch_cluster_fill(cudaStream_t s, int maxcl, int ncol, int nc2,
 template <typename T>
 void launch_pair_clusters(cudaStream_t s, const PairClusterArgs<T> &a,
                           const PairConsts<T> &pc);
+// adjoint short-range pass on the cluster sweep (mixed form; the FP64 form
+// uses launch_adj_pair): fbs = Fbar in pair-cell order, out_a = (E, psi),
+// out_b = (h, 0) per sorted atom, as launch_adj_pair
+template <typename T>
+bool adj_pair_clusters_supported();
+template <typename T>
+void launch_adj_pair_clusters(cudaStream_t s, const PairClusterArgs<T> &a,
+                              const PairConsts<T> &pc, const V4<T> *fbs, V4<T> *out_a,
+                              V4<T> *out_b);
 
 // ---- grid transfers (k_grid.cu) ----
 // variant 0: tile scatter with a fold (scratch: anterp_scratch_elems
