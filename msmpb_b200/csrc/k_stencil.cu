@@ -35,14 +35,33 @@ inline int blocks_for(long n) {
 }
 
 // Row pitch of a shared slice: the nz R + S - 1 values a row needs, in whole
-// 16-byte units, and an odd number of them. Lanes of one row read 16-byte
-// units R values apart; an odd pitch puts the next row's lanes on the
-// banks in between, so 16-byte row reads by up to 4 lanes per row are free
-// of bank conflicts.
-__host__ __device__ inline int slice_pitch(int nz, int R, int S, int V) {
-  int units = (nz * R + S - 1 + V - 1) / V;
-  if (units % 2 == 0) ++units;
-  return units * V;
+// 16-byte units, padded so that the 16-byte row reads are free of bank
+// conflicts. Thread (tz, ty) = tid (tz fastest) reads unit ty p + tz R/V (+v)
+// of the slice; a 16-byte load is served 8 lanes at a time, one wavefront
+// when their units fall in 8 different 16-byte bank groups (unit mod 8). The
+// smallest pitch p that gives that for the CTA's first 128 threads is taken
+// (else the one with the fewest conflicts).
+inline int slice_pitch(int nz, int R, int S, int V) {
+  const int base = (nz * R + S - 1 + V - 1) / V;
+  const int step = R / V;
+  int best = base, best_c = 1 << 30;
+  for (int p = base; p < base + 8; ++p) {
+    int conflicts = 0;
+    for (int g = 0; g < 128; g += 8) {
+      int used = 0;
+      for (int l = g; l < g + 8; ++l) {
+        const int bank = ((l / nz) * p + (l % nz) * step) & 7;
+        if (used & (1 << bank)) ++conflicts;
+        used |= 1 << bank;
+      }
+    }
+    if (conflicts < best_c) {
+      best_c = conflicts;
+      best = p;
+      if (!conflicts) break;
+    }
+  }
+  return best * V;
 }
 
 template <typename T>
@@ -86,7 +105,7 @@ k_stencil_simple(StencilShape sh, const T *__restrict__ p,
     }
     acc.add(pl);
   }
-  e[idx] += w * acc.value();
+  e[idx] = (sh.store ? T(0) : e[idx]) + w * acc.value();
 }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
@@ -101,14 +120,16 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// Copies input plane `plane` of the tile into the shared slice (rows of W).
+// Copies input plane `plane` of the tile into the shared slice: H rows of
+// the WC values the sweep reads (WC <= the row pitch W; the pitch's padding
+// columns are never read, and copying them could run past the padded grid).
 template <typename T>
 __device__ __forceinline__ void stage_plane(const T *__restrict__ P,
                                             const StencilShape &sh, int plane,
-                                            int y0, int z0, int H, int W,
+                                            int y0, int z0, int H, int W, int WC,
                                             T *slice) {
   constexpr int V = 16 / sizeof(T);
-  const int wv = W / V;
+  const int wv = WC / V;
   const int nthreads = blockDim.x * blockDim.y;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const T *src = P + ((long)plane * sh.P[1] + y0) * sh.P[2] + z0;
@@ -142,7 +163,7 @@ template <typename T, int S, int R, int TX>
 __global__ void __launch_bounds__(kThreads)
 k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
                 const T *__restrict__ kh, T w, T *__restrict__ e,
-                int ntx, int chunk, T *__restrict__ part) {
+                int ntx, int chunk, T *__restrict__ part, int W) {
   constexpr int V = 16 / sizeof(T);
   constexpr int SP = (S + V - 1) / V * V;        // tap row pitch
   constexpr int RL = R + S - 1;                  // row values per thread
@@ -157,7 +178,7 @@ k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
   const int i_lo = kc * chunk, i_hi = min(S0, i_lo + chunk);
   const int z0 = blockIdx.x * NZ * R, y0 = blockIdx.y * TY, x0 = xt * TX;
   const int H = TY + S1 - 1;
-  const int W = slice_pitch(NZ, R, S, V);
+  const int WC = (NZ - 1) * R + RLV;  // values a row's threads read
   const int slice_elems = H * W + V;  // +V: tail reads of the last row
   const int tap_elems = S1 * SP;
   T *buf0 = smem, *buf1 = smem + slice_elems;
@@ -171,12 +192,12 @@ k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
 
   const int nplanes = TX + (i_hi - i_lo) - 1;
   const int p0 = x0 + i_lo;  // first input plane
-  stage_plane(P, sh, p0, y0, z0, H, W, buf0);
+  stage_plane(P, sh, p0, y0, z0, H, W, WC, buf0);
   stage_taps(kh, i_lo, tap_elems, ring + (i_lo % NRING) * tap_elems);
   cp_async_commit();
   for (int pi = 0; pi < nplanes; ++pi) {
     if (pi + 1 < nplanes) {
-      stage_plane(P, sh, p0 + pi + 1, y0, z0, H, W, (pi & 1) ? buf0 : buf1);
+      stage_plane(P, sh, p0 + pi + 1, y0, z0, H, W, WC, (pi & 1) ? buf0 : buf1);
       const int inext = i_lo + pi + 1;
       if (inext < i_hi)
         stage_taps(kh, inext, tap_elems, ring + (inext % NRING) * tap_elems);
@@ -251,7 +272,7 @@ k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
       if (part)
         part[kc * mtot + row0 + z] = acc[xo][r];
       else
-        e[row0 + z] += w * acc[xo][r];
+        e[row0 + z] = (sh.store ? T(0) : e[row0 + z]) + w * acc[xo][r];
     }
   }
 }
@@ -272,7 +293,7 @@ k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
 template <typename T, int S, int R>
 __global__ void __launch_bounds__(kThreads)
 k_stencil_fold(StencilShape sh, const T *__restrict__ P, const T *__restrict__ kf,
-               T w, T *__restrict__ e, int chunk, T *__restrict__ part) {
+               T w, T *__restrict__ e, int chunk, T *__restrict__ part, int W) {
   constexpr int V = 16 / sizeof(T);
   constexpr int SP = (S + V - 1) / V * V;
   constexpr int RL = R + S - 1;
@@ -287,7 +308,7 @@ k_stencil_fold(StencilShape sh, const T *__restrict__ P, const T *__restrict__ k
   const int i_lo = kc * chunk, i_hi = min(c0 + 1, i_lo + chunk);
   const int z0 = blockIdx.x * NZ * R, y0 = blockIdx.y * TY;
   const int H = TY + S1 - 1;
-  const int W = slice_pitch(NZ, R, S, V);
+  const int WC = (NZ - 1) * R + RLV;  // values a row's threads read
   const int slice = H * W + V;
   const int tap_elems = (c1 + 1) * SP;
   // shared layout: A slices of stages 0 and 1, one B slice, tap blocks of
@@ -299,8 +320,8 @@ k_stencil_fold(StencilShape sh, const T *__restrict__ P, const T *__restrict__ k
 #pragma unroll
   for (int r = 0; r < R; ++r) acc[r] = T(0);
   auto stage = [&](int i, int s) {
-    stage_plane(P, sh, x + c0 + i, y0, z0, H, W, smem + s * slice);
-    if (i > 0) stage_plane(P, sh, x + c0 - i, y0, z0, H, W, Bsl);
+    stage_plane(P, sh, x + c0 + i, y0, z0, H, W, WC, smem + s * slice);
+    if (i > 0) stage_plane(P, sh, x + c0 - i, y0, z0, H, W, WC, Bsl);
     stage_taps(kf + (long)i * tap_elems, 0, tap_elems, smem + 3 * slice + s * tap_elems);
   };
   if (i_lo < i_hi) {
@@ -408,30 +429,40 @@ k_stencil_fold(StencilShape sh, const T *__restrict__ P, const T *__restrict__ k
     if (part)
       part[kc * mtot + row0 + z] = acc[r];
     else
-      e[row0 + z] += w * acc[r];
+      e[row0 + z] = (sh.store ? T(0) : e[row0 + z]) + w * acc[r];
   }
 }
 
-// e += w * sum_k part[k], chunks added in index order
+// e (+)= w * sum_k part[k], chunks added in index order
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
 k_split_reduce(long n, int nsplit, const T *__restrict__ part, T w,
-               T *__restrict__ e) {
+               T *__restrict__ e, int store) {
   long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
   T s = part[idx];
   for (int k = 1; k < nsplit; ++k) s += part[k * n + idx];
-  e[idx] += w * s;
+  e[idx] = (store ? T(0) : e[idx]) + w * s;
 }
 
+// R: z outputs per thread; RALT: the folded sweep's alternative for widths
+// of at least kMinSAlt taps (more outputs per loaded row: the folded sweep
+// reads two rows per tap row, and shared-memory bandwidth, not the FMA pipe,
+// bounds it at the default R)
 template <typename T> struct TileDefaults;
-template <> struct TileDefaults<float> { static constexpr int R = 8, TX = 4; };
-template <> struct TileDefaults<double> { static constexpr int R = 4, TX = 4; };
+template <> struct TileDefaults<float> { static constexpr int R = 8, TX = 4, RALT = 12; };
+template <> struct TileDefaults<double> { static constexpr int R = 4, TX = 4, RALT = 8; };
+constexpr int kMinSAlt = 9;
+
+int tile_r_of(const StencilTile &tl, bool fp64) {
+  const int d = fp64 ? TileDefaults<double>::R : TileDefaults<float>::R;
+  return tl.r > 0 ? tl.r : d;
+}
 
 // shared memory of the folded sweep: two A slices, one B slice, two tap blocks
 template <typename T>
 size_t fold_smem_bytes(const StencilShape &sh, const StencilTile &tl) {
-  constexpr int R = TileDefaults<T>::R;
+  const int R = tile_r_of(tl, sizeof(T) == 8);
   constexpr int V = 16 / sizeof(T);
   const int H = tl.ty + sh.S[1] - 1;
   const int W = slice_pitch(tl.nz, R, sh.S[2], V);
@@ -457,17 +488,17 @@ void launch_tiled(cudaStream_t s, const StencilShape &sh, const StencilTile &tl,
             ntx * nsplit);
   (void)khz;  // the tiled kernel reads rows of the padded pitch
   k_stencil_tiled<T, S, R, TX><<<grid, block, smem, s>>>(
-      sh, p, kh, w, e, ntx, chunk, nsplit > 1 ? part : nullptr);
+      sh, p, kh, w, e, ntx, chunk, nsplit > 1 ? part : nullptr, W);
   if (nsplit > 1) {
     const long n = (long)sh.M[0] * sh.M[1] * sh.M[2];
-    k_split_reduce<T><<<blocks_for(n), kThreads, 0, s>>>(n, nsplit, part, w, e);
+    k_split_reduce<T><<<blocks_for(n), kThreads, 0, s>>>(n, nsplit, part, w, e, sh.store);
   }
 }
 
-template <typename T, int S>
-void launch_fold(cudaStream_t s, const StencilShape &sh, const StencilTile &tl,
-                 const T *p, const T *kf, T w, T *e, T *part) {
-  constexpr int R = TileDefaults<T>::R;
+template <typename T, int S, int R>
+void launch_fold_r(cudaStream_t s, const StencilShape &sh, const StencilTile &tl,
+                   const T *p, const T *kf, T w, T *e, T *part) {
+  constexpr int V = 16 / sizeof(T);
   const int nI = sh.S[0] / 2 + 1;
   const int nsplit = std::max(1, tl.nsplit);
   const int chunk = (nI + nsplit - 1) / nsplit;
@@ -475,29 +506,48 @@ void launch_fold(cudaStream_t s, const StencilShape &sh, const StencilTile &tl,
   dim3 grid((sh.M[2] + tl.nz * R - 1) / (tl.nz * R), (sh.M[1] + tl.ty - 1) / tl.ty,
             sh.M[0] * nsplit);
   k_stencil_fold<T, S, R><<<grid, block, fold_smem_bytes<T>(sh, tl), s>>>(
-      sh, p, kf, w, e, chunk, nsplit > 1 ? part : nullptr);
+      sh, p, kf, w, e, chunk, nsplit > 1 ? part : nullptr, slice_pitch(tl.nz, R, S, V));
   if (nsplit > 1) {
     const long n = (long)sh.M[0] * sh.M[1] * sh.M[2];
-    k_split_reduce<T><<<blocks_for(n), kThreads, 0, s>>>(n, nsplit, part, w, e);
+    k_split_reduce<T><<<blocks_for(n), kThreads, 0, s>>>(n, nsplit, part, w, e, sh.store);
   }
+}
+
+template <typename T, int S>
+void launch_fold(cudaStream_t s, const StencilShape &sh, const StencilTile &tl,
+                 const T *p, const T *kf, T w, T *e, T *part) {
+  if constexpr (S >= kMinSAlt) {
+    if (tile_r_of(tl, sizeof(T) == 8) == TileDefaults<T>::RALT) {
+      launch_fold_r<T, S, TileDefaults<T>::RALT>(s, sh, tl, p, kf, w, e, part);
+      return;
+    }
+  }
+  launch_fold_r<T, S, TileDefaults<T>::R>(s, sh, tl, p, kf, w, e, part);
 }
 
 // Levels (and plans) that share an instantiation need the largest request:
 // the attribute is per kernel function and per device, so it is only ever
 // raised, and the level granted is kept per device.
+// fold: 0 tiled sweep, 1 folded sweep at the default R, 2 at the alternative
 template <typename T, int S>
-void set_smem_attr(int bytes, bool fold) {
+void set_smem_attr(int bytes, int fold) {
   constexpr int R = TileDefaults<T>::R, TX = TileDefaults<T>::TX;
   static std::mutex mu;
-  static int current[kMaxDevices][2];
+  static int current[kMaxDevices][3];
   const int dev = device_slot();
   std::lock_guard<std::mutex> lock(mu);
   if (dev >= 0 && bytes <= std::max(current[dev][fold], 48 * 1024)) return;
-  const cudaError_t err =
-      fold ? cudaFuncSetAttribute(k_stencil_fold<T, S, R>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)
-           : cudaFuncSetAttribute(k_stencil_tiled<T, S, R, TX>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaError_t err = cudaErrorInvalidValue;
+  if (fold == 0) {
+    err = cudaFuncSetAttribute(k_stencil_tiled<T, S, R, TX>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  } else if (fold == 1) {
+    err = cudaFuncSetAttribute(k_stencil_fold<T, S, R>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  } else if constexpr (S >= kMinSAlt) {
+    err = cudaFuncSetAttribute(k_stencil_fold<T, S, TileDefaults<T>::RALT>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  }
   if (err == cudaSuccess && dev >= 0) current[dev][fold] = bytes;
 }
 
@@ -507,6 +557,13 @@ void set_smem_attr(int bytes, bool fold) {
   X(27) X(28) X(29) X(30) X(31) X(32) X(33)
 
 }  // namespace
+
+int stencil_tile_r(const StencilTile &tile, bool fp64) { return tile_r_of(tile, fp64); }
+
+int stencil_alt_r(const StencilShape &sh, bool fp64) {
+  if (!sh.sym || sh.S[2] < kMinSAlt || sh.S[2] > kMaxTemplatedS) return 0;
+  return fp64 ? TileDefaults<double>::RALT : TileDefaults<float>::RALT;
+}
 
 StencilTile stencil_default_tile(const StencilShape &sh, bool fp64) {
   const int R = fp64 ? TileDefaults<double>::R : TileDefaults<float>::R;
@@ -554,7 +611,7 @@ bool stencil_templated(const StencilShape &sh) {
 
 void stencil_padded_dims(const StencilShape &sh, const StencilTile &tl,
                          bool fp64, int P[3]) {
-  const int R = fp64 ? TileDefaults<double>::R : TileDefaults<float>::R;
+  const int R = tile_r_of(tl, fp64);
   const int V = fp64 ? 2 : 4;
   const int span = tl.nz * R;
   const int mz = (sh.M[2] + span - 1) / span * span;
@@ -569,7 +626,8 @@ void stencil_padded_dims(const StencilShape &sh, const StencilTile &tl,
 template <typename T>
 int stencil_prepare(const StencilShape &sh, const StencilTile &tl) {
   if (!stencil_templated(sh)) return 0;
-  constexpr int R = TileDefaults<T>::R;
+  const int R = tile_r_of(tl, sizeof(T) == 8);
+  if (R != TileDefaults<T>::R && R != stencil_alt_r(sh, sizeof(T) == 8)) return -1;
   constexpr int V = 16 / sizeof(T);
   const int H = tl.ty + sh.S[1] - 1;
   const int W = slice_pitch(tl.nz, R, sh.S[2], V);
@@ -581,7 +639,9 @@ int stencil_prepare(const StencilShape &sh, const StencilTile &tl) {
   if (bytes > 200 * 1024) return -1;
   switch (sh.S[2]) {
 #define X(SS) \
-  case SS: set_smem_attr<T, SS>(bytes, sh.sym != 0); break;
+  case SS:                                                                         \
+    set_smem_attr<T, SS>(bytes, !sh.sym ? 0 : (R == TileDefaults<T>::R ? 1 : 2)); \
+    break;
     MSM_S_CASES(X)
 #undef X
   }

@@ -243,12 +243,19 @@ struct StencilShape {
   int P[3];   // padded input dims (P[2] rounded up for 16-byte rows)
   int sym;    // 1: taps mirror-symmetric in x and y, S0 and S1 odd (folded
               // sweep, taps given as the folded (S0/2+1) x (S1/2+1) rows)
+  int store;  // 1: e = w K q (overwrite); 0: e += w K q
 };
 // CTA tile of the stencil sweep: nz x ty threads, each with tx x R outputs
 struct StencilTile {
   int nz = 0, ty = 0, tx = 0;
   int nsplit = 1;  // CTAs sharing one output tile, each over a run of tap planes
+  int r = 0;       // z outputs per thread of the folded sweep (0: the default)
 };
+// z outputs per thread of a tile (the precision's default unless the tile
+// picks the folded sweep's alternative)
+int stencil_tile_r(const StencilTile &tile, bool fp64);
+// alternative z outputs per thread of the folded sweep for this shape, or 0
+int stencil_alt_r(const StencilShape &sh, bool fp64);
 StencilTile stencil_default_tile(const StencilShape &sh, bool fp64);
 bool stencil_templated(const StencilShape &sh);
 // row pitch of the tap array: S2 rounded up to 16 bytes (rows zero padded)

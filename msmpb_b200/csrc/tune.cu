@@ -5,7 +5,7 @@
 // own buffers and keeps the fastest; smaller levels use the model-based
 // default (stencil_default_tile). Results are cached in a text file, one
 // line per (format, device, precision, grid, stencil):
-//   <format>|<device name>|<fp32|fp64>|M0,M1,M2|S0,S1,S2|<folded|full> nz ty nsplit ms
+//   <format>|<device name>|<fp32|fp64>|M0,M1,M2|S0,S1,S2|<folded|full> nz ty nsplit r ms
 // at $MSMPB_TUNE_CACHE, else $HOME/.cache/msmpb_b200/stencil_tiles.txt. A
 // cached tile is used only after the same checks as a freshly timed one
 // (shape limits, buffer capacities, stencil_prepare); a line that fails them
@@ -30,7 +30,7 @@ std::mutex g_cache_mu;
 
 // Bumped whenever the candidate set or the meaning of a tile changes, so
 // that lines written by another version never match.
-constexpr const char *kCacheFormat = "st2";
+constexpr const char *kCacheFormat = "st3";
 
 std::string cache_path() {
   const char *p = std::getenv("MSMPB_TUNE_CACHE");
@@ -66,12 +66,14 @@ bool cache_lookup(const std::string &key, StencilTile &t) {
   bool found = false;
   while (std::fgets(line, sizeof line, f)) {
     char k[600];
-    int nz, ty, ns;
+    int nz, ty, ns, r;
     double ms;
-    if (std::sscanf(line, "%599s %d %d %d %lf", k, &nz, &ty, &ns, &ms) == 5 && key == k) {
+    if (std::sscanf(line, "%599s %d %d %d %d %lf", k, &nz, &ty, &ns, &r, &ms) == 6 &&
+        key == k) {
       t.nz = nz;
       t.ty = ty;
       t.nsplit = ns;
+      t.r = r;
       found = true;  // the last entry wins
     }
   }
@@ -85,7 +87,7 @@ void cache_store(const std::string &key, const StencilTile &t, double ms) {
   if (path.empty()) return;
   FILE *f = std::fopen(path.c_str(), "a");
   if (!f) return;
-  std::fprintf(f, "%s %d %d %d %.5f\n", key.c_str(), t.nz, t.ty, t.nsplit, ms);
+  std::fprintf(f, "%s %d %d %d %d %.5f\n", key.c_str(), t.nz, t.ty, t.nsplit, t.r, ms);
   std::fclose(f);
 }
 
@@ -100,23 +102,30 @@ std::vector<StencilTile> stencil_candidates(const StencilShape &sh, bool fp64) {
   std::vector<StencilTile> out;
   const StencilTile d = stencil_default_tile(sh, fp64);
   out.push_back(d);
-  const int R = fp64 ? 4 : 8;
-  for (int nz : {d.nz, 2, 3, 4, 6, 8, 9, 12})
-    for (int ty : {4, 8, 12, 16, 24, 32})
-      for (int ns : {1, 2, d.nsplit, 2 * d.nsplit}) {
-        StencilTile t = d;
-        t.nz = nz;
-        t.ty = ty;
-        if (nz * ty > 256 || nz * ty < 32 || ty > sh.M[1]) continue;
-        if (nz * R > sh.M[2] + R - 1 && nz > 1) continue;
-        const int nI = sh.sym ? sh.S[0] / 2 + 1 : sh.S[0];
-        const int chunk = (nI + std::max(1, ns) - 1) / std::max(1, ns);
-        t.nsplit = (nI + chunk - 1) / chunk;
-        bool dup = false;
-        for (auto &u : out)
-          dup |= (u.nz == t.nz && u.ty == t.ty && u.nsplit == t.nsplit);
-        if (!dup) out.push_back(t);
-      }
+  // the precision's default z outputs per thread, and for folded sweeps of
+  // wide stencils the alternative
+  const int alt = stencil_alt_r(sh, fp64);
+  for (int r : {0, alt}) {
+    const int R = r ? r : stencil_tile_r(d, fp64);
+    for (int nz : {d.nz, 2, 3, 4, 6, 8, 9, 12})
+      for (int ty : {4, 8, 12, 16, 24, 32, 36, 48})
+        for (int ns : {1, 2, d.nsplit, 2 * d.nsplit}) {
+          StencilTile t = d;
+          t.nz = nz;
+          t.ty = ty;
+          t.r = r;
+          if (nz * ty > 256 || nz * ty < 32 || ty > sh.M[1]) continue;
+          if (nz * R > sh.M[2] + R - 1 && nz > 1) continue;
+          const int nI = sh.sym ? sh.S[0] / 2 + 1 : sh.S[0];
+          const int chunk = (nI + std::max(1, ns) - 1) / std::max(1, ns);
+          t.nsplit = (nI + chunk - 1) / chunk;
+          bool dup = false;
+          for (auto &u : out)
+            dup |= (u.nz == t.nz && u.ty == t.ty && u.nsplit == t.nsplit && u.r == t.r);
+          if (!dup) out.push_back(t);
+        }
+    if (!alt) break;
+  }
   return out;
 }
 
