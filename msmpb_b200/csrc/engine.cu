@@ -146,7 +146,8 @@ class Plan : public FFDevice {
  private:
   int set_tables(const Tables &t);
   int update_box(const Tables &t, cudaStream_t s, bool stencils_on_device);
-  int enqueue_chain(cudaStream_t s, T *const *qg, T *const *eg, const double *w, bool tm);
+  int enqueue_chain(cudaStream_t s, T *const *qg, T *const *eg, const double *w, bool tm,
+                    bool fork);
   int tune_levels(size_t pad_cap, size_t part_cap);
   int launch_graph(const EvalRequest &r, cudaStream_t s, const double *pos,
                    const double *q, double *force, double *phi, double *edev);
@@ -229,6 +230,13 @@ class Plan : public FFDevice {
   static constexpr bool kMixed = sizeof(T) == 4;
   T *qg_[kMaxLevels + 2] = {}, *eg_[kMaxLevels + 2] = {};
   T *padded_ = nullptr, *part_ = nullptr, *kh_[kMaxLevels + 2] = {};
+  // the levels below the finest in forked evaluations run beside the
+  // level-1 stencil: their own padded copy and split partial sums
+  T *padded2_ = nullptr, *part2_ = nullptr;
+  // forked evaluations: the pair sum and the level-1 stencil on their own
+  // streams (graph branches when captured), joined by events
+  cudaStream_t aux_[2] = {};
+  cudaEvent_t fork_ev_[4] = {};
   T *khf_[kMaxLevels + 2] = {};  // folded taps (symmetric stencils)
   // level stencil taps for the sweep variant in use
   const T *level_taps(int l) const { return sh_[l].sym ? khf_[l] : kh_[l]; }
@@ -288,6 +296,13 @@ Plan<T>::~Plan() {
   for (auto &pr : lev_ev_)
     for (auto &e : pr)
       if (e) cudaEventDestroy(e);
+  for (auto &e : fork_ev_)
+    if (e) cudaEventDestroy(e);
+  for (auto &a : aux_)
+    if (a) {
+      cudaStreamSynchronize(a);
+      cudaStreamDestroy(a);
+    }
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -296,6 +311,8 @@ int Plan<T>::init(const Tables &t, int device) {
   device_ = device;
   MSM_CUDA_TRY(cudaSetDevice(device));
   MSM_CUDA_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  for (auto &a : aux_) MSM_CUDA_TRY(cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking));
+  for (auto &e : fork_ev_) MSM_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   for (auto &e : ev_) MSM_CUDA_TRY(cudaEventCreate(&e));
   for (auto &pr : lev_ev_)
     for (auto &e : pr) MSM_CUDA_TRY(cudaEventCreate(&e));
@@ -326,7 +343,7 @@ int Plan<T>::init(const Tables &t, int device) {
   if (err) return err;
   // stencil shapes; scratch for both sweep variants (a rebuild with a new
   // box can make a stencil lose or gain its mirror symmetry)
-  size_t pad_max = 1, part_max = 1;
+  size_t pad_max = 1, part_max = 1, pad2_max = 1, part2_max = 1;
   for (int l = 1; l < L_; ++l) {
     StencilShape &s = sh_[l];
     for (int k = 0; k < 3; ++k) {
@@ -357,6 +374,30 @@ int Plan<T>::init(const Tables &t, int device) {
         if (c.nsplit > 1)
           part_max = std::max(part_max, (size_t)c.nsplit * s.M[0] * s.M[1] * s.M[2]);
       }
+  }
+  // the same bounds over the levels below the finest only (their stencils
+  // run beside the level-1 stencil in forked evaluations)
+  for (int l = 2; l < L_; ++l) {
+    const StencilShape &s = sh_[l];
+    const bool fp64 = sizeof(T) == 8;
+    std::vector<StencilTile> tiles{tile_[l]};
+    StencilShape alt = s;
+    for (int v = 0; v < 2; ++v) {  // both sweep variants' default tiles
+      alt.sym = v;
+      if (v && (s.S[0] % 2 == 0 || s.S[1] % 2 == 0)) continue;
+      tiles.push_back(stencil_default_tile(alt, fp64));
+    }
+    if (tune_[l])
+      for (const StencilTile &c : stencil_candidates(s, fp64)) tiles.push_back(c);
+    for (const StencilTile &c : tiles) {
+      int P[3];
+      stencil_padded_dims(s, c, fp64, P);
+      if (!stencil_templated(s) || c.nz <= 0)
+        for (int k = 0; k < 3; ++k) P[k] = s.M[k] + s.S[k] - 1;
+      pad2_max = std::max(pad2_max, (size_t)P[0] * P[1] * P[2]);
+      if (c.nsplit > 1)
+        part2_max = std::max(part2_max, (size_t)c.nsplit * s.M[0] * s.M[1] * s.M[2]);
+    }
   }
   const size_t n = N_;
   nq_ = prep_blocks(N_);
@@ -402,6 +443,10 @@ int Plan<T>::init(const Tables &t, int device) {
     a.want(&fold_tab_, fold_tab.size() * sizeof(int));
   }
   a.want(&part_, part_max * sizeof(T));
+  if (L_ > 2) {
+    a.want(&padded2_, std::min(pad2_max, pad_max) * sizeof(T));
+    a.want(&part2_, std::min(part2_max, part_max) * sizeof(T));
+  }
   size_t ntop = (size_t)grid_[L_][0] * grid_[L_][1] * grid_[L_][2];
   a.want(&khat_top_, ntop * sizeof(double));
   a.want(&fft_, ntop * sizeof(double2));
@@ -710,10 +755,31 @@ int Plan<T>::update_box(const Tables &t, cudaStream_t s, bool stencils_on_device
 // The grid operator K: q[1] -> e[1] (restriction, top solve, then from the
 // coarsest level down, prolongation plus the level stencil). Returns the
 // number of kernel launches.
+//
+// Forked form (fork = true, every evaluation except the eagerly timed one):
+// the level-1 stencil depends on q[1] alone, so it runs on its own stream
+// (a branch of the captured graph) and stores e[1] = w1 K1 q[1], while the
+// restrictions, the top solve and the levels below run on s (with their own
+// padded copy and partial sums); s then waits for it and adds the
+// prolongation of e[2] into e[1]. The latency-bound small levels hide behind
+// the level-1 stencil, and e[1] gets the same two terms (addition commutes).
 template <typename T>
 int Plan<T>::enqueue_chain(cudaStream_t s, T *const *qg, T *const *eg, const double *w,
-                           bool tm) {
+                           bool tm, bool fork) {
   int nl = 0;
+  fork = fork && L_ > 2 && padded2_ && part2_;
+  if (fork) {
+    cudaStream_t b = aux_[1];
+    cudaEventRecord(fork_ev_[2], s);
+    cudaStreamWaitEvent(b, fork_ev_[2], 0);
+    StencilShape st = sh_[1];
+    st.store = 1;
+    launch_pad<T>(b, st, qg[1], padded_);
+    launch_stencil<T>(b, st, tile_[1], padded_, level_taps(1),
+                      stencil_tap_pitch(st.S[2], !kMixed), (T)w[1], eg[1], part_);
+    cudaEventRecord(fork_ev_[3], b);
+    nl += 1 + stencil_launches(st, tile_[1]);
+  }
   mark(s, kPhaseRestrict, tm);
   for (int l = 1; l < L_; ++l) {
     launch_restrict<T>(s, grid_[l], qg[l], qg[l + 1], J_, nu_);
@@ -723,14 +789,22 @@ int Plan<T>::enqueue_chain(cudaStream_t s, T *const *qg, T *const *eg, const dou
   launch_top_solve<T>(s, grid_[L_], qg[L_], khat_top_, w[L_], fft_, nullptr, eg[L_]);
   nl += top_solve_launches(grid_[L_]);
   for (int l = L_ - 1; l >= 1; --l) {
+    if (fork && l == 1) {
+      cudaStreamWaitEvent(s, fork_ev_[3], 0);
+      launch_prolong_add<T>(s, grid_[1], eg[2], eg[1], J_, nu_);
+      nl += 1;
+      break;
+    }
+    T *pad = fork ? padded2_ : padded_;
+    T *part = fork ? part2_ : part_;
     mark(s, kPhaseProlong, tm && l == L_ - 1);
     cudaMemsetAsync(eg[l], 0, (size_t)grid_[l][0] * grid_[l][1] * grid_[l][2] * sizeof(T), s);
     launch_prolong_add<T>(s, grid_[l], eg[l + 1], eg[l], J_, nu_);
     mark(s, kPhaseStencil, tm && l == L_ - 1);
-    launch_pad<T>(s, sh_[l], qg[l], padded_);
+    launch_pad<T>(s, sh_[l], qg[l], pad);
     if (tm) cudaEventRecord(lev_ev_[l][0], s);
-    launch_stencil<T>(s, sh_[l], tile_[l], padded_, level_taps(l),
-                      stencil_tap_pitch(sh_[l].S[2], !kMixed), (T)w[l], eg[l], part_);
+    launch_stencil<T>(s, sh_[l], tile_[l], pad, level_taps(l),
+                      stencil_tap_pitch(sh_[l].S[2], !kMixed), (T)w[l], eg[l], part);
     if (tm) cudaEventRecord(lev_ev_[l][1], s);
     nl += 2 + stencil_launches(sh_[l], tile_[l]);
   }
@@ -796,35 +870,48 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
                        kMixed ? prel64_ : nullptr, kMixed ? psorted64_ : nullptr,
                        GatherSide<T>{gperm_, gfrac_, gcell_, gsorted_, gcs_, ginv_});
   nl += 2 + scan_launches(ncp_) + scan_launches(ncg_) + 3;
+  // Forked form (all but the eagerly timed evaluation): after binning the
+  // short-range branch (cluster build and pair sum) runs on its own stream
+  // beside the grid branch (anterpolation, grid operator, interpolation);
+  // the combine waits for both. Captured, the two are branches of one graph.
+  const bool fork = !tm;
+  cudaStream_t sp = s;
+  if (fork) {
+    cudaEventRecord(fork_ev_[0], s);
+    cudaStreamWaitEvent(aux_[0], fork_ev_[0], 0);
+    sp = aux_[0];
+  }
   if (clusters) {  // cluster build (part of the binning phase)
     const V4<double> *src64 =
         kMixed ? psorted64_ : reinterpret_cast<const V4<double> *>(psorted_);
-    launch_scan(s, clcount_, clstart_, ncol_, scan_tmp_);
-    launch_cluster_fill<T>(s, maxcl_, ncol_, geom_.nc[2], pstart_, clstart_, pcs_,
+    launch_scan(sp, clcount_, clstart_, ncol_, scan_tmp_);
+    launch_cluster_fill<T>(sp, maxcl_, ncol_, geom_.nc[2], pstart_, clstart_, pcs_,
                            src64, cz_, cpos_, cpos64_, cinfo_, cubox_);
   }
   mark(s, kPhasePair, tm);
   if (clusters) {
     const PairClusterArgs<T> ca = cluster_args();
-    launch_pair_clusters<T>(s, ca, pc_);
+    launch_pair_clusters<T>(sp, ca, pc_);
     nl += scan_launches(ncol_) + 1;
   } else if (pair_variant_ == 0 && pair_cells_supported(noff_, N_)) {
-    launch_pair_cells<T>(s, ncp_, psorted_, psorted64_, pstart_, geom_, off_d_,
+    launch_pair_cells<T>(sp, ncp_, psorted_, psorted64_, pstart_, geom_, off_d_,
                          noff_, pc_, pout_, err_d_);
   } else {
-    launch_pair<T>(s, N_, psorted_, psorted64_, pcs_, pstart_, geom_, off_d_,
+    launch_pair<T>(sp, N_, psorted_, psorted64_, pcs_, pstart_, geom_, off_d_,
                    noff_, pc_, pout_);
   }
   nl += 1;
+  if (fork) cudaEventRecord(fork_ev_[1], sp);
   mark(s, kPhaseAnterp, tm);
   launch_anterpolate<T>(s, grid_[1], gsorted_, gcs_, gstart_, sc_, qg_[1],
                         anterp_variant_, err_d_, N_, anterp_scratch_, fold_tab_);
   nl += (anterp_variant_ == 0 && anterp_scratch_) ? 2 : 1;
-  nl += enqueue_chain(s, qg_, eg_, w, tm);
+  nl += enqueue_chain(s, qg_, eg_, w, tm, fork);
   mark(s, kPhaseInterp, tm);
   launch_grid_dot<T>(s, (size_t)ncg_, qg_[1], eg_[1], grid_parts_, ngrid_);
   launch_interpolate<T>(s, N_, grid_[1], gsorted_, gcs_, eg_[1], sc_, geom_, gout_);
   nl += 2;
+  if (fork) cudaStreamWaitEvent(s, fork_ev_[1], 0);
   mark(s, kPhaseCombine, tm);
   CombineArgs ca;
   ca.N = N_;
@@ -978,7 +1065,7 @@ int Plan<T>::adjoint(const AdjointRequest &r) {
   launch_adj_dipoles<T>(s, N_, gperm_, r.q, r.fbar, geom_, dip_);
   launch_adj_anterpolate<T>(s, grid_[1], gsorted_, gcs_, gstart_, sc_, dip_, qg2_[1],
                             anterp_scratch_, fold_tab_);
-  enqueue_chain(s, qg2_, eg2_, w, false);
+  enqueue_chain(s, qg2_, eg2_, w, false, true);
   launch_adj_interpolate<T>(s, N_, grid_[1], gsorted_, gcs_, gperm_, r.fbar, eg2_[1],
                             eg_[1], sc_, geom_, adj_g_, adj_h_);
   AdjointCombineArgs ca{};

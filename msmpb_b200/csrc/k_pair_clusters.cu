@@ -1075,14 +1075,20 @@ k_adj_pair_jl(PairClusterArgs<float> a, PairConsts<float> pc, const V4<float> *_
   auto far_step = [&](int cnt) {
     const int e = (fhead + lane) & (kRing - 1);
     V4<float> J = sh.far[warp][e][0], F = sh.far[warp][e][1];
-    if (lane >= cnt) J = dummy;
+    if (lane >= cnt) {  // no entry: zero charge and Fbar (stale slots may hold anything)
+      J = dummy;
+      F = V4<float>{0.f, 0.f, 0.f, 0.f};
+    }
     L.template pairs<false>(pc, J, F, -1);
     fhead += cnt;
   };
   auto self_step = [&](int cnt) {
     const int e = (shead + lane) & (kRing - 1);
     V4<float> J = sh.self[warp][e][0], F = sh.self[warp][e][1];
-    if (lane >= cnt) J = dummy;
+    if (lane >= cnt) {
+      J = dummy;
+      F = V4<float>{0.f, 0.f, 0.f, __int_as_float(-1)};
+    }
     L.template pairs<true>(pc, J, F, __float_as_int(F.w));
     shead += cnt;
   };

@@ -159,15 +159,15 @@ def test_five_levels_headline_depth(precision):
 
 def test_high_accuracy_parameters_match_oracle():
     """The parameters of the bench's high-accuracy reference (the FP64 GPU
-    MSM with order 10, cutoff 12 A, one level, h = 1.0 A, against which the
+    MSM with order 10, cutoff 12 A, one level, h ~ 1.0 A, against which the
     method errors of the headline forms are measured) on a small box: the
     FP64 form against the oracle to 1e-11 (energy) and 1e-10 (forces,
     potentials), so that the reference of those errors is itself pinned."""
     q, pos, edges = systems.water(600, 26.0, 31)
-    kw = dict(cutoff=12.0, order=10, levels=1, top_grid=26)
-    o = Oracle(q, edges, cutoff=12.0, nu=10, levels=1, top_grid=26)
+    kw = dict(cutoff=12.0, order=10, levels=1, top_grid=27)
+    o = Oracle(q, edges, cutoff=12.0, nu=10, levels=1, top_grid=27)
     ff = ForceField(q, pos, edges, **kw, precision="fp64")
-    assert (ff.cutoff, ff.order, ff.levels, ff.top_grid) == (12.0, 10, 1, (26, 26, 26))
+    assert (ff.cutoff, ff.order, ff.levels, ff.top_grid) == (12.0, 10, 1, (27, 27, 27))
     eo, fo, po = o.energy(pos)
     e, f, phi = ff.energy(pos, potentials=True)
     assert abs(e - eo) / abs(eo) < 1e-11
