@@ -255,6 +255,7 @@ class Plan : public FFDevice {
   V4<double> *cpos64_ = nullptr;
   ClusterInfo *cinfo_ = nullptr;
   UnitBox *cubox_ = nullptr;
+  int2 *ulist_ = nullptr, *ulcnt_ = nullptr;  // unit lists (mixed form)
   int *err_d_ = nullptr;
   // graph
   cudaGraphExec_t exec_ = nullptr;
@@ -471,6 +472,10 @@ int Plan<T>::init(const Tables &t, int device) {
   if (kMixed) a.want(&cpos64_, (size_t)maxcl_ * 8 * sizeof(V4<double>));
   a.want(&cinfo_, (size_t)maxcl_ * sizeof(ClusterInfo));
   a.want(&cubox_, (size_t)maxcl_ * 2 * sizeof(UnitBox));
+  if (kMixed) {
+    a.want(&ulist_, (size_t)maxcl_ * kUnitListCap * sizeof(int2));
+    a.want(&ulcnt_, (size_t)maxcl_ * sizeof(int2));
+  }
   a.want(&err_d_, sizeof(int));
   if ((err = a.commit())) return err;
   MSM_CUDA_TRY(cudaMemset(err_d_, 0, sizeof(int)));
@@ -840,6 +845,9 @@ PairClusterArgs<T> Plan<T>::cluster_args() const {
   ca.out = pout_;
   ca.err = err_d_;
   ca.self_images = self_images_ ? 1 : 0;
+  ca.list = ulist_;
+  ca.lcnt = ulcnt_;
+  ca.lcap = kUnitListCap;
   return ca;
 }
 
@@ -891,6 +899,10 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   mark(s, kPhasePair, tm);
   if (clusters) {
     const PairClusterArgs<T> ca = cluster_args();
+    if (ca.list) {
+      launch_pair_list<T>(sp, ca);
+      nl += 1;
+    }
     launch_pair_clusters<T>(sp, ca, pc_);
     nl += scan_launches(ncol_) + 1;
   } else if (pair_variant_ == 0 && pair_cells_supported(noff_, N_)) {

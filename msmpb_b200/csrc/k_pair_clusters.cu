@@ -532,6 +532,65 @@ struct JlShared {
   int2 grp[kWarps][sizeof(T) == 4 ? kGroupCap : 1];
 };
 
+// Item `it` of i-cluster ci's candidates: the column offset o = it / nseg
+// and periodic image k along the column; its run of sorted atoms [A, A + nat)
+// (the cells along the column within K2 of the cluster's cells, for
+// orthorhombic boxes only those the cutoff sphere around the cluster's box
+// reaches through the column's xy gap), the cluster slot s0 of its first
+// atom, its code (o << 8 | k + 128) and the FP64 shift of a j cluster frame
+// at cell 0 of the column into the i-cluster's frame.
+template <typename T>
+__device__ __forceinline__ void jl_item(const PairClusterArgs<T> &a, const ClusterInfo &ci,
+                                        int cx, int cy, int lo, int hi, int klo, int nseg,
+                                        int it, int &A, int &nat, int &s0, int &code,
+                                        double &shx, double &shy, double &shz) {
+  const int o = nseg == 1 ? it : it / nseg;
+  const int k = klo + (it - o * nseg);
+  const ColumnOffset &co = a.coloff[o];
+  int x = cx + co.du, y = cy + co.dv;
+  while (x < 0) x += a.nc0;
+  while (x >= a.nc0) x -= a.nc0;
+  while (y < 0) y += a.nc1;
+  while (y >= a.nc1) y -= a.nc1;
+  int wlo = lo, whi = hi;
+  if (a.ortho) {
+    // the column's slab in the i frame: x in [bx, bx + cw0), y likewise
+    const float bx = (float)co.base[0], by = (float)co.base[1];
+    const float gx =
+        fmaxf(fmaxf(bx - (ci.c.x + ci.h.x), (ci.c.x - ci.h.x) - (bx + a.cw[0])), 0.f);
+    const float gy =
+        fmaxf(fmaxf(by - (ci.c.y + ci.h.y), (ci.c.y - ci.h.y) - (by + a.cw[1])), 0.f);
+    const float rem = a.rbox2 - gx * gx - gy * gy;
+    if (rem <= 0.f) {
+      whi = wlo - 1;
+    } else {
+      const float hw = sqrtf(rem) + 1e-3f;
+      wlo = max(wlo, ci.czf + (int)floorf((ci.c.z - ci.h.z - hw) / a.cw[2]));
+      whi = min(whi, ci.czf + (int)floorf((ci.c.z + ci.h.z + hw) / a.cw[2]));
+    }
+  }
+  const int col = x * a.nc1 + y;
+  const int cb = col * a.nc2;
+  const int c0 = max(wlo, k * a.nc2) - k * a.nc2;
+  const int c1 = min(whi, k * a.nc2 + a.nc2 - 1) - k * a.nc2;
+  nat = 0;
+  s0 = 0;
+  A = 0;
+  if (c0 <= c1) {
+    A = a.start[cb + c0];
+    const int B = a.start[cb + c1 + 1];
+    if (A < B) {
+      nat = B - A;
+      s0 = 8 * a.clstart[col] + (A - a.start[cb]);
+    }
+  }
+  code = (o << 8) | (k + 128);
+  const double dz = (double)(k * a.nc2 - ci.czf);
+  shx = co.base[0] + dz * a.cz[0];
+  shy = co.base[1] + dz * a.cz[1];
+  shz = co.base[2] + dz * a.cz[2];
+}
+
 // The candidate j atoms of i-cluster u for one warp. Phase A: the (column,
 // periodic image) items, 32 at a time, one per lane: each item's run of
 // sorted atoms (the cells along the column within K2 of the cluster's cells,
@@ -557,50 +616,8 @@ __device__ __forceinline__ void jl_sweep(const PairClusterArgs<T> &a, const Clus
     int nat = 0, s0 = 0, A = 0, code = 0;
     double shx = 0., shy = 0., shz = 0.;
     const int it = i0 + lane;
-    if (it < nitems) {
-      const int o = nseg == 1 ? it : it / nseg;
-      const int k = klo + (it - o * nseg);
-      const ColumnOffset &co = a.coloff[o];
-      int x = cx + co.du, y = cy + co.dv;
-      while (x < 0) x += a.nc0;
-      while (x >= a.nc0) x -= a.nc0;
-      while (y < 0) y += a.nc1;
-      while (y >= a.nc1) y -= a.nc1;
-      int wlo = lo, whi = hi;
-      if (a.ortho) {
-        // the column's slab in the i frame: x in [bx, bx + cw0), y likewise
-        const float bx = (float)co.base[0], by = (float)co.base[1];
-        const float gx =
-            fmaxf(fmaxf(bx - (ci.c.x + ci.h.x), (ci.c.x - ci.h.x) - (bx + a.cw[0])), 0.f);
-        const float gy =
-            fmaxf(fmaxf(by - (ci.c.y + ci.h.y), (ci.c.y - ci.h.y) - (by + a.cw[1])), 0.f);
-        const float rem = a.rbox2 - gx * gx - gy * gy;
-        if (rem <= 0.f) {
-          whi = wlo - 1;
-        } else {
-          const float hw = sqrtf(rem) + 1e-3f;
-          wlo = max(wlo, ci.czf + (int)floorf((ci.c.z - ci.h.z - hw) / a.cw[2]));
-          whi = min(whi, ci.czf + (int)floorf((ci.c.z + ci.h.z + hw) / a.cw[2]));
-        }
-      }
-      const int col = x * a.nc1 + y;
-      const int cb = col * a.nc2;
-      const int c0 = max(wlo, k * a.nc2) - k * a.nc2;
-      const int c1 = min(whi, k * a.nc2 + a.nc2 - 1) - k * a.nc2;
-      if (c0 <= c1) {
-        A = a.start[cb + c0];
-        const int B = a.start[cb + c1 + 1];
-        if (A < B) {
-          nat = B - A;
-          s0 = 8 * a.clstart[col] + (A - a.start[cb]);
-        }
-      }
-      code = (o << 8) | (k + 128);
-      const double dz = (double)(k * a.nc2 - ci.czf);
-      shx = co.base[0] + dz * a.cz[0];
-      shy = co.base[1] + dz * a.cz[1];
-      shz = co.base[2] + dz * a.cz[2];
-    }
+    if (it < nitems)
+      jl_item(a, ci, cx, cy, lo, hi, klo, nseg, it, A, nat, s0, code, shx, shy, shz);
     int incl = nat;
 #pragma unroll
     for (int dd = 1; dd < 32; dd <<= 1) {
@@ -649,6 +666,101 @@ __device__ __forceinline__ void jl_sweep(const PairClusterArgs<T> &a, const Clus
       batch(pass, near, J, jslot, jcode, selfk, sorted);
     }
   }
+}
+
+// ---- unit lists: the candidate search of the pair kernels, ahead of them ----
+//
+// One warp per i-cluster, few registers (many warps per SM hide the
+// latencies of the search): the items of jl_item, their atom runs widened to
+// whole units (half clusters, 4 slots; the widening adds atoms of the same
+// column and image outside the window, i.e. beyond the cutoff, and dummy
+// slots, all of which the pair kernels' cutoff test rejects), and every unit
+// box-tested against the i-cluster's box, 32 at a time. Passing units are
+// written as {unit, code} in a fixed order (item, then unit): far ones from
+// the front of the cluster's region, near ones (box within the close
+// distance, or a unit of the cluster itself) from the back.
+struct ListItems {
+  int off[32], u0[32], code[32];
+  double shift[32][3];
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kWarps * 32)
+k_pair_list(PairClusterArgs<T> a) {
+  __shared__ ListItems sh[kWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int u = blockIdx.x * kWarps + warp;
+  if (u >= a.maxcl || u >= a.clstart[a.ncol]) return;  // whole warp
+  const ClusterInfo ci = a.info[u];
+  const unsigned lt = (1u << lane) - 1u;
+  int2 *reg = a.list + (size_t)u * a.lcap;
+  int nf = 0, nn = 0;
+  const int cx = ci.col / a.nc1, cy = ci.col - cx * a.nc1;
+  const int lo = ci.czf - a.K2, hi = ci.czl + a.K2;
+  const int klo = floor_div(lo, a.nc2);
+  const int nseg = floor_div(hi, a.nc2) - klo + 1;
+  const int nitems = a.ncoloff * nseg;
+  ListItems &it_sh = sh[warp];
+  for (int i0 = 0; i0 < nitems; i0 += 32) {
+    int A = 0, nat = 0, s0 = 0, code = 0, nun = 0, u0 = 0;
+    double shx = 0., shy = 0., shz = 0.;
+    const int it = i0 + lane;
+    if (it < nitems) {
+      jl_item(a, ci, cx, cy, lo, hi, klo, nseg, it, A, nat, s0, code, shx, shy, shz);
+      if (nat > 0) {
+        u0 = s0 >> 2;
+        nun = ((s0 + nat - 1) >> 2) - u0 + 1;
+      }
+    }
+    int incl = nun;
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, dd);
+      if (lane >= dd) incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    it_sh.off[lane] = incl - nun;
+    it_sh.u0[lane] = u0;
+    it_sh.code[lane] = code;
+    it_sh.shift[lane][0] = shx;
+    it_sh.shift[lane][1] = shy;
+    it_sh.shift[lane][2] = shz;
+    __syncwarp();
+    for (int b0 = 0; b0 < total; b0 += 32) {
+      const int c = b0 + lane;
+      bool pass = false, near = false;
+      int unit = 0, ucode = 0;
+      if (c < total) {
+        int j = 0;  // last item starting at or before c
+#pragma unroll
+        for (int step = 16; step; step >>= 1)
+          if (it_sh.off[j + step] <= c) j += step;
+        unit = it_sh.u0[j] + (c - it_sh.off[j]);
+        ucode = it_sh.code[j];
+        const UnitBox ub = a.ubox[unit];
+        const double czj = (double)__float_as_int(ub.c.w);
+        const float sx = (float)(it_sh.shift[j][0] + czj * a.cz[0]);
+        const float sy = (float)(it_sh.shift[j][1] + czj * a.cz[1]);
+        const float sz = (float)(it_sh.shift[j][2] + czj * a.cz[2]);
+        pass = box_near(ci.c, ci.h, ub.c, ub.h, sx, sy, sz, a.rbox2);
+        near = box_near(ci.c, ci.h, ub.c, ub.h, sx, sy, sz, a.rnear2) || (unit >> 1) == u;
+      }
+      const unsigned mf = __ballot_sync(0xffffffffu, pass && !near);
+      const unsigned mn = __ballot_sync(0xffffffffu, pass && near);
+      if (pass && !near) {
+        const int e = nf + __popc(mf & lt);
+        if (e < a.lcap) reg[e] = make_int2(unit, ucode);
+      }
+      if (pass && near) {
+        const int e = nn + __popc(mn & lt);
+        if (e < a.lcap) reg[a.lcap - 1 - e] = make_int2(unit, ucode);
+      }
+      nf += __popc(mf);
+      nn += __popc(mn);
+    }
+    __syncwarp();
+  }
+  if (lane == 0) a.lcnt[u] = make_int2(nf, nn);
 }
 
 // lanes' 32 partial sums -> lane l holds the total of value l (fixed order)
@@ -811,6 +923,22 @@ struct JlLane<double> {
   }
 };
 
+// Atom q of list unit `unit` (item `code`), shifted into the frame of the
+// i-cluster ci: FP32 cluster-frame position plus the FP64 shift of its
+// cluster's frame, rounded once.
+template <typename T>
+__device__ __forceinline__ V4<T> list_atom(const PairClusterArgs<T> &a, const ClusterInfo &ci,
+                                           int unit, int code, int q) {
+  V4<T> J = a.cpos[4 * unit + q];
+  const int o = code >> 8, k = (code & 255) - 128;
+  const ColumnOffset &co = a.coloff[o];
+  const int dzc = __float_as_int(a.ubox[unit].c.w) + k * a.nc2 - ci.czf;
+  J.x += (T)(co.base[0] + dzc * a.cz[0]);
+  J.y += (T)(co.base[1] + dzc * a.cz[1]);
+  J.z += (T)(co.base[2] + dzc * a.cz[2]);
+  return J;
+}
+
 template <typename T, int NU, bool SELF>
 __device__ __forceinline__ void pair_jl(const PairClusterArgs<T> &a, const PairConsts<T> &pc) {
   constexpr bool kMixed = sizeof(T) == 4;
@@ -851,6 +979,42 @@ __device__ __forceinline__ void pair_jl(const PairClusterArgs<T> &a, const PairC
                                nrec);
     nhead += cnt;
   };
+  // the cluster's unit list (built by k_pair_list), 8 units = 32 atoms per
+  // step, far units the lean way, near units checked; a cluster whose list
+  // overflowed its region sweeps its candidates here instead
+  bool sweep = true;
+  if (a.list) {
+    const int2 cnt = a.lcnt[u];
+    if (cnt.x + cnt.y <= a.lcap) {
+      sweep = false;
+      const int2 *reg = a.list + (size_t)u * a.lcap;
+      for (int e0 = 0; e0 < cnt.x; e0 += 8) {
+        const int e = e0 + (lane >> 2);
+        V4<T> J = dummy;
+        if (e < cnt.x) {
+          const int2 en = reg[e];
+          J = list_atom(a, ci, en.x, en.y, lane & 3);
+        }
+        L.template pairs<NU, false>(pc, J, -1, 0, 0, myrec, nrec);
+      }
+      for (int e0 = 0; e0 < cnt.y; e0 += 8) {
+        const int e = e0 + (lane >> 2);
+        V4<T> J = dummy;
+        int jslot = 0, jcode = 0, selfk = -1;
+        if (e < cnt.y) {
+          const int2 en = reg[a.lcap - 1 - e];
+          jslot = 4 * en.x + (lane & 3);
+          jcode = en.y;
+          J = list_atom(a, ci, en.x, en.y, lane & 3);
+          if ((jslot >> 3) == u &&
+              (SELF || ((jcode >> 8) == a.ozero && (jcode & 255) == 128)))
+            selfk = jslot & 7;
+        }
+        L.template pairs<NU, true>(pc, J, selfk, jslot, jcode, myrec, nrec);
+      }
+    }
+  }
+  if (sweep) {
   jl_sweep<T, SELF>(a, ci, u, lane, sh.items[warp],
                     [&](bool pass, bool near, const V4<T> &J, int jslot, int jcode,
                         int selfk, int) {
@@ -871,6 +1035,7 @@ __device__ __forceinline__ void pair_jl(const PairClusterArgs<T> &a, const PairC
   });
   if (ftail != fhead) far_step((int)(ftail - fhead));
   if (ntail != nhead) near_step((int)(ntail - nhead));
+  }
 
   // lanes' partial sums: lane l ends with value l = 8 c + i (c: 0..2 the
   // negated field components, 3 the potential; i the atom)
@@ -1092,6 +1257,37 @@ k_adj_pair_jl(PairClusterArgs<float> a, PairConsts<float> pc, const V4<float> *_
     L.template pairs<true>(pc, J, F, __float_as_int(F.w));
     shead += cnt;
   };
+  bool sweep = true;
+  if (a.list) {  // the forward's unit list, as in pair_jl
+    const int2 cnt = a.lcnt[u];
+    if (cnt.x + cnt.y <= a.lcap) {
+      sweep = false;
+      const int2 *reg = a.list + (size_t)u * a.lcap;
+      for (int half = 0; half < 2; ++half) {
+        const int n = half ? cnt.y : cnt.x;
+        for (int e0 = 0; e0 < n; e0 += 8) {
+          const int e = e0 + (lane >> 2);
+          V4<float> J = dummy, F{0.f, 0.f, 0.f, 0.f};
+          int selfk = -1;
+          if (e < n) {
+            const int2 en = half ? reg[a.lcap - 1 - e] : reg[e];
+            const int jslot = 4 * en.x + (lane & 3);
+            J = list_atom(a, ci, en.x, en.y, lane & 3);
+            const ClusterInfo &cj = a.info[jslot >> 3];
+            if ((jslot & 7) < cj.n) F = fbs[cj.first + (jslot & 7)];
+            if ((jslot >> 3) == u &&
+                (SELF || ((en.y >> 8) == a.ozero && (en.y & 255) == 128)))
+              selfk = jslot & 7;
+          }
+          if (half)
+            L.template pairs<true>(pc, J, F, selfk);
+          else
+            L.template pairs<false>(pc, J, F, -1);
+        }
+      }
+    }
+  }
+  if (sweep) {
   jl_sweep<float, SELF>(a, ci, u, lane, sh.items[warp],
                         [&](bool pass, bool, const V4<float> &J, int, int, int selfk,
                             int sorted) {
@@ -1120,6 +1316,7 @@ k_adj_pair_jl(PairClusterArgs<float> a, PairConsts<float> pc, const V4<float> *_
   });
   if (ftail != fhead) far_step((int)(ftail - fhead));
   if (stail != shead) self_step((int)(stail - shead));
+  }
 
   const int i = lane & 7, c = lane >> 3;
   float v[32];
@@ -1211,6 +1408,12 @@ void launch_cluster_fill(cudaStream_t s, int maxcl, int ncol, int nc2,
 }
 
 template <typename T>
+void launch_pair_list(cudaStream_t s, const PairClusterArgs<T> &a) {
+  const int blocks = std::max(1, (a.maxcl + kWarps - 1) / kWarps);
+  k_pair_list<T><<<blocks, kWarps * 32, 0, s>>>(a);
+}
+
+template <typename T>
 bool adj_pair_clusters_supported() { return sizeof(T) == 4; }
 
 template <typename T>
@@ -1256,6 +1459,8 @@ template void launch_cluster_fill<double>(cudaStream_t, int, int, int, const int
                                           ClusterInfo *, UnitBox *);
 template void launch_pair_clusters<float>(cudaStream_t, const PairClusterArgs<float> &,
                                           const PairConsts<float> &);
+template void launch_pair_list<float>(cudaStream_t, const PairClusterArgs<float> &);
+template void launch_pair_list<double>(cudaStream_t, const PairClusterArgs<double> &);
 template bool adj_pair_clusters_supported<float>();
 template bool adj_pair_clusters_supported<double>();
 template void launch_adj_pair_clusters<float>(cudaStream_t, const PairClusterArgs<float> &,
