@@ -270,7 +270,7 @@ class Plan : public FFDevice {
   // adjoint buffers (allocated on first use)
   void *adj_mem_ = nullptr;
   V4<T> *fbs_ = nullptr, *dip_ = nullptr, *adj_a_ = nullptr, *adj_b_ = nullptr,
-        *adj_g_ = nullptr, *adj_h_ = nullptr;
+        *adj_g_ = nullptr, *adj_h_ = nullptr, *fslot_ = nullptr;
   T *qg2_[kMaxLevels + 2] = {}, *eg2_[kMaxLevels + 2] = {};
   // recorded after a device-side rebuild; every later evaluation's stream
   // waits for it (the rebuild may run on another stream)
@@ -1030,7 +1030,7 @@ int Plan<T>::adjoint(const AdjointRequest &r) {
   if (!r.pos || !r.q || !r.fbar) return MSMPB_ERR_ARGUMENT;
   if (!adj_mem_) {
     // six per-atom records and a second set of level grids
-    size_t bytes = 6 * (size_t)N_ * sizeof(V4<T>) + 256 * 6;
+    size_t bytes = 6 * (size_t)N_ * sizeof(V4<T>) + 256 * 7 + 8 * (size_t)maxcl_ * sizeof(V4<T>);
     for (int l = 1; l <= L_; ++l)
       bytes += 2 * ((size_t)grid_[l][0] * grid_[l][1] * grid_[l][2] * sizeof(T) + 256);
     if (cudaMalloc(&adj_mem_, bytes) != cudaSuccess) {
@@ -1046,6 +1046,7 @@ int Plan<T>::adjoint(const AdjointRequest &r) {
     };
     for (V4<T> **b : {&fbs_, &dip_, &adj_a_, &adj_b_, &adj_g_, &adj_h_})
       *b = reinterpret_cast<V4<T> *>(take((size_t)N_ * sizeof(V4<T>)));
+    fslot_ = reinterpret_cast<V4<T> *>(take(8 * (size_t)maxcl_ * sizeof(V4<T>)));
     for (int l = 1; l <= L_; ++l) {
       const size_t g = (size_t)grid_[l][0] * grid_[l][1] * grid_[l][2] * sizeof(T);
       qg2_[l] = reinterpret_cast<T *>(take(g));
@@ -1070,7 +1071,7 @@ int Plan<T>::adjoint(const AdjointRequest &r) {
   launch_adj_gather<T>(s, N_, pperm_, r.fbar, fbs_);
   // the forward just run (or reused) built the clusters of these positions
   if (pair_variant_ == 2 && clusters_ok_ && adj_pair_clusters_supported<T>())
-    launch_adj_pair_clusters<T>(s, cluster_args(), pc_, fbs_, adj_a_, adj_b_);
+    launch_adj_pair_clusters<T>(s, cluster_args(), pc_, fbs_, fslot_, adj_a_, adj_b_);
   else
     launch_adj_pair<T>(s, N_, psorted_, fbs_, pcs_, pstart_, geom_, off_d_, noff_, pc_,
                        adj_a_, adj_b_);

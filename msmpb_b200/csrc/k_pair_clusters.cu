@@ -736,8 +736,9 @@ k_pair_list(PairClusterArgs<T> a) {
         for (int step = 16; step; step >>= 1)
           if (it_sh.off[j + step] <= c) j += step;
         unit = it_sh.u0[j] + (c - it_sh.off[j]);
-        ucode = it_sh.code[j];
         const UnitBox ub = a.ubox[unit];
+        // entry: item code (18 bits) and the first cell of the unit's cluster
+        ucode = it_sh.code[j] | (__float_as_int(ub.c.w) << 18);
         const double czj = (double)__float_as_int(ub.c.w);
         const float sx = (float)(it_sh.shift[j][0] + czj * a.cz[0]);
         const float sy = (float)(it_sh.shift[j][1] + czj * a.cz[1]);
@@ -923,20 +924,19 @@ struct JlLane<double> {
   }
 };
 
-// Atom q of list unit `unit` (item `code`), shifted into the frame of the
-// i-cluster ci: FP32 cluster-frame position plus the FP64 shift of its
-// cluster's frame, rounded once.
+// A list atom (cluster-frame position `raw`) shifted into the frame of the
+// i-cluster ci by the FP64 shift of its cluster's frame (entry y: item code
+// and the cluster's first cell), rounded once.
 template <typename T>
-__device__ __forceinline__ V4<T> list_atom(const PairClusterArgs<T> &a, const ClusterInfo &ci,
-                                           int unit, int code, int q) {
-  V4<T> J = a.cpos[4 * unit + q];
-  const int o = code >> 8, k = (code & 255) - 128;
+__device__ __forceinline__ V4<T> list_shifted(const PairClusterArgs<T> &a, const ClusterInfo &ci,
+                                              V4<T> raw, int y) {
+  const int o = (y >> 8) & 1023, k = (y & 255) - 128;
   const ColumnOffset &co = a.coloff[o];
-  const int dzc = __float_as_int(a.ubox[unit].c.w) + k * a.nc2 - ci.czf;
-  J.x += (T)(co.base[0] + dzc * a.cz[0]);
-  J.y += (T)(co.base[1] + dzc * a.cz[1]);
-  J.z += (T)(co.base[2] + dzc * a.cz[2]);
-  return J;
+  const int dzc = (y >> 18) + k * a.nc2 - ci.czf;
+  raw.x += (T)(co.base[0] + dzc * a.cz[0]);
+  raw.y += (T)(co.base[1] + dzc * a.cz[1]);
+  raw.z += (T)(co.base[2] + dzc * a.cz[2]);
+  return raw;
 }
 
 template <typename T, int NU, bool SELF>
@@ -988,29 +988,34 @@ __device__ __forceinline__ void pair_jl(const PairClusterArgs<T> &a, const PairC
     if (cnt.x + cnt.y <= a.lcap) {
       sweep = false;
       const int2 *reg = a.list + (size_t)u * a.lcap;
-      for (int e0 = 0; e0 < cnt.x; e0 += 8) {
-        const int e = e0 + (lane >> 2);
-        V4<T> J = dummy;
-        if (e < cnt.x) {
-          const int2 en = reg[e];
-          J = list_atom(a, ci, en.x, en.y, lane & 3);
+      // 8 units = 32 atoms per step; the next step's atoms and the entries
+      // of the step after are loaded before this step's pairs, so their
+      // latencies overlap the arithmetic
+      for (int half = 0; half < 2; ++half) {
+        const int n = half ? cnt.y : cnt.x;
+        auto entry = [&](int e) {
+          return e < n ? (half ? reg[a.lcap - 1 - e] : reg[e]) : make_int2(-1, 0);
+        };
+        int2 en1 = entry(lane >> 2), en2 = entry(8 + (lane >> 2));
+        V4<T> raw1 = en1.x >= 0 ? a.cpos[4 * en1.x + (lane & 3)] : dummy;
+        for (int e0 = 0; e0 < n; e0 += 8) {
+          const int2 en = en1;
+          const V4<T> raw = raw1;
+          en1 = en2;
+          raw1 = en1.x >= 0 ? a.cpos[4 * en1.x + (lane & 3)] : dummy;
+          en2 = entry(e0 + 16 + (lane >> 2));
+          const V4<T> J = en.x >= 0 ? list_shifted(a, ci, raw, en.y) : dummy;
+          if (half == 0) {
+            L.template pairs<NU, false>(pc, J, -1, 0, 0, myrec, nrec);
+          } else {
+            const int jslot = 4 * en.x + (lane & 3), jcode = en.y & 0x3ffff;
+            int selfk = -1;
+            if (en.x >= 0 && (jslot >> 3) == u &&
+                (SELF || ((jcode >> 8) == a.ozero && (jcode & 255) == 128)))
+              selfk = jslot & 7;
+            L.template pairs<NU, true>(pc, J, selfk, jslot, jcode, myrec, nrec);
+          }
         }
-        L.template pairs<NU, false>(pc, J, -1, 0, 0, myrec, nrec);
-      }
-      for (int e0 = 0; e0 < cnt.y; e0 += 8) {
-        const int e = e0 + (lane >> 2);
-        V4<T> J = dummy;
-        int jslot = 0, jcode = 0, selfk = -1;
-        if (e < cnt.y) {
-          const int2 en = reg[a.lcap - 1 - e];
-          jslot = 4 * en.x + (lane & 3);
-          jcode = en.y;
-          J = list_atom(a, ci, en.x, en.y, lane & 3);
-          if ((jslot >> 3) == u &&
-              (SELF || ((jcode >> 8) == a.ozero && (jcode & 255) == 128)))
-            selfk = jslot & 7;
-        }
-        L.template pairs<NU, true>(pc, J, selfk, jslot, jcode, myrec, nrec);
       }
     }
   }
@@ -1202,6 +1207,21 @@ struct AdjLane {
   }
 };
 
+// Fbar in cluster-slot order (zero for the dummy slots): one thread per slot
+__global__ void __launch_bounds__(256)
+k_slot_gather(int maxcl, const int *__restrict__ ncl, const ClusterInfo *__restrict__ info,
+              const V4<float> *__restrict__ fbs, V4<float> *__restrict__ fslot) {
+  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= 8L * maxcl) return;
+  const int c = (int)(s >> 3), i = (int)(s & 7);
+  V4<float> f{0.f, 0.f, 0.f, 0.f};
+  if (c < *ncl) {
+    const ClusterInfo &ci = info[c];
+    if (i < ci.n) f = fbs[ci.first + i];
+  }
+  fslot[s] = f;
+}
+
 struct AdjShared {
   JlItems items[kWarps];
   V4<float> far[kWarps][kRing][2], self[kWarps][kRing][2];
@@ -1210,7 +1230,8 @@ struct AdjShared {
 template <int NU, bool SELF>
 __global__ void __launch_bounds__(kWarps * 32)
 k_adj_pair_jl(PairClusterArgs<float> a, PairConsts<float> pc, const V4<float> *__restrict__ fbs,
-              V4<float> *__restrict__ out_a, V4<float> *__restrict__ out_b) {
+              const V4<float> *__restrict__ fslot, V4<float> *__restrict__ out_a,
+              V4<float> *__restrict__ out_b) {
   __shared__ AdjShared sh;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int u = blockIdx.x * kWarps + warp;
@@ -1265,24 +1286,30 @@ k_adj_pair_jl(PairClusterArgs<float> a, PairConsts<float> pc, const V4<float> *_
       const int2 *reg = a.list + (size_t)u * a.lcap;
       for (int half = 0; half < 2; ++half) {
         const int n = half ? cnt.y : cnt.x;
+        auto entry = [&](int e) {
+          return e < n ? (half ? reg[a.lcap - 1 - e] : reg[e]) : make_int2(-1, 0);
+        };
+        int2 en1 = entry(lane >> 2), en2 = entry(8 + (lane >> 2));
+        V4<float> raw1 = en1.x >= 0 ? a.cpos[4 * en1.x + (lane & 3)] : dummy;
+        V4<float> f1 = en1.x >= 0 ? fslot[4 * en1.x + (lane & 3)] : V4<float>{0.f, 0.f, 0.f, 0.f};
         for (int e0 = 0; e0 < n; e0 += 8) {
-          const int e = e0 + (lane >> 2);
-          V4<float> J = dummy, F{0.f, 0.f, 0.f, 0.f};
-          int selfk = -1;
-          if (e < n) {
-            const int2 en = half ? reg[a.lcap - 1 - e] : reg[e];
-            const int jslot = 4 * en.x + (lane & 3);
-            J = list_atom(a, ci, en.x, en.y, lane & 3);
-            const ClusterInfo &cj = a.info[jslot >> 3];
-            if ((jslot & 7) < cj.n) F = fbs[cj.first + (jslot & 7)];
-            if ((jslot >> 3) == u &&
-                (SELF || ((en.y >> 8) == a.ozero && (en.y & 255) == 128)))
-              selfk = jslot & 7;
-          }
-          if (half)
-            L.template pairs<true>(pc, J, F, selfk);
-          else
+          const int2 en = en1;
+          const V4<float> raw = raw1, F = f1;
+          en1 = en2;
+          raw1 = en1.x >= 0 ? a.cpos[4 * en1.x + (lane & 3)] : dummy;
+          f1 = en1.x >= 0 ? fslot[4 * en1.x + (lane & 3)] : V4<float>{0.f, 0.f, 0.f, 0.f};
+          en2 = entry(e0 + 16 + (lane >> 2));
+          const V4<float> J = en.x >= 0 ? list_shifted(a, ci, raw, en.y) : dummy;
+          if (half == 0) {
             L.template pairs<false>(pc, J, F, -1);
+          } else {
+            const int jslot = 4 * en.x + (lane & 3), jcode = en.y & 0x3ffff;
+            int selfk = -1;
+            if (en.x >= 0 && (jslot >> 3) == u &&
+                (SELF || ((jcode >> 8) == a.ozero && (jcode & 255) == 128)))
+              selfk = jslot & 7;
+            L.template pairs<true>(pc, J, F, selfk);
+          }
         }
       }
     }
@@ -1418,15 +1445,18 @@ bool adj_pair_clusters_supported() { return sizeof(T) == 4; }
 
 template <typename T>
 void launch_adj_pair_clusters(cudaStream_t s, const PairClusterArgs<T> &a,
-                              const PairConsts<T> &pc, const V4<T> *fbs, V4<T> *out_a,
-                              V4<T> *out_b) {
+                              const PairConsts<T> &pc, const V4<T> *fbs, V4<T> *fslot,
+                              V4<T> *out_a, V4<T> *out_b) {
   if constexpr (sizeof(T) == 4) {
+    const long slots = 8L * a.maxcl;
+    k_slot_gather<<<(int)std::max<long>(1, (slots + 255) / 256), 256, 0, s>>>(
+        a.maxcl, a.clstart + a.ncol, a.info, fbs, fslot);
     const int blocks = std::max(1, (a.maxcl + kWarps - 1) / kWarps);
 #define MSM_ADJ_JL(NUV)                                                                 \
   if (a.self_images)                                                                    \
-    k_adj_pair_jl<NUV, true><<<blocks, kWarps * 32, 0, s>>>(a, pc, fbs, out_a, out_b);  \
+    k_adj_pair_jl<NUV, true><<<blocks, kWarps * 32, 0, s>>>(a, pc, fbs, fslot, out_a, out_b);  \
   else                                                                                  \
-    k_adj_pair_jl<NUV, false><<<blocks, kWarps * 32, 0, s>>>(a, pc, fbs, out_a, out_b)
+    k_adj_pair_jl<NUV, false><<<blocks, kWarps * 32, 0, s>>>(a, pc, fbs, fslot, out_a, out_b)
     switch (pc.nu) {
       case 4: MSM_ADJ_JL(4); break;
       case 6: MSM_ADJ_JL(6); break;
@@ -1465,10 +1495,10 @@ template bool adj_pair_clusters_supported<float>();
 template bool adj_pair_clusters_supported<double>();
 template void launch_adj_pair_clusters<float>(cudaStream_t, const PairClusterArgs<float> &,
                                               const PairConsts<float> &, const V4<float> *,
-                                              V4<float> *, V4<float> *);
+                                              V4<float> *, V4<float> *, V4<float> *);
 template void launch_adj_pair_clusters<double>(cudaStream_t, const PairClusterArgs<double> &,
                                                const PairConsts<double> &, const V4<double> *,
-                                               V4<double> *, V4<double> *);
+                                               V4<double> *, V4<double> *, V4<double> *);
 template void launch_pair_clusters<double>(cudaStream_t, const PairClusterArgs<double> &,
                                            const PairConsts<double> &);
 

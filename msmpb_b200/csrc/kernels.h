@@ -210,14 +210,15 @@ template <typename T>
 void launch_pair_clusters(cudaStream_t s, const PairClusterArgs<T> &a,
                           const PairConsts<T> &pc);
 // adjoint short-range pass on the cluster sweep (mixed form; the FP64 form
-// uses launch_adj_pair): fbs = Fbar in pair-cell order, out_a = (E, psi),
+// uses launch_adj_pair): fbs = Fbar in pair-cell order, fslot scratch of
+// maxcl x 8 records (Fbar gathered into cluster-slot order), out_a = (E, psi),
 // out_b = (h, 0) per sorted atom, as launch_adj_pair
 template <typename T>
 bool adj_pair_clusters_supported();
 template <typename T>
 void launch_adj_pair_clusters(cudaStream_t s, const PairClusterArgs<T> &a,
-                              const PairConsts<T> &pc, const V4<T> *fbs, V4<T> *out_a,
-                              V4<T> *out_b);
+                              const PairConsts<T> &pc, const V4<T> *fbs, V4<T> *fslot,
+                              V4<T> *out_a, V4<T> *out_b);
 
 // ---- grid transfers (k_grid.cu) ----
 // variant 0: tile scatter with a fold (scratch: anterp_scratch_elems
