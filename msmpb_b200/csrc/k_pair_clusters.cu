@@ -526,6 +526,7 @@ struct JlItems {
 template <typename T>
 struct JlShared {
   JlItems items[kWarps];
+  int rslot[kWarps][256], ry[kWarps][256];  // far-atom ring of the list stream
   V4<T> far[kWarps][kRing], near[kWarps][kRing];
   int2 ninfo[kWarps][kRing];
   int2 rec[kWarps][sizeof(T) == 4 ? 32 * kCloseLane : 1];
@@ -745,6 +746,20 @@ k_pair_list(PairClusterArgs<T> a) {
         const float sz = (float)(it_sh.shift[j][2] + czj * a.cz[2]);
         pass = box_near(ci.c, ci.h, ub.c, ub.h, sx, sy, sz, a.rbox2);
         near = box_near(ci.c, ci.h, ub.c, ub.h, sx, sy, sz, a.rnear2) || (unit >> 1) == u;
+        if (pass && !near) {
+          // far unit: which of its 4 atoms are within the cutoff of the box
+          unsigned m4 = 0;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const V4<T> at = a.cpos[4 * unit + q];
+            const float gx = fmaxf(fabsf((float)at.x + sx - ci.c.x) - ci.h.x, 0.f);
+            const float gy = fmaxf(fabsf((float)at.y + sy - ci.c.y) - ci.h.y, 0.f);
+            const float gz = fmaxf(fabsf((float)at.z + sz - ci.c.z) - ci.h.z, 0.f);
+            if (gx * gx + gy * gy + gz * gz < a.rbox2) m4 |= 1u << q;
+          }
+          ucode |= (int)(m4 << 27);
+          pass = m4 != 0;
+        }
       }
       const unsigned mf = __ballot_sync(0xffffffffu, pass && !near);
       const unsigned mn = __ballot_sync(0xffffffffu, pass && near);
@@ -932,11 +947,63 @@ __device__ __forceinline__ V4<T> list_shifted(const PairClusterArgs<T> &a, const
                                               V4<T> raw, int y) {
   const int o = (y >> 8) & 1023, k = (y & 255) - 128;
   const ColumnOffset &co = a.coloff[o];
-  const int dzc = (y >> 18) + k * a.nc2 - ci.czf;
+  const int dzc = ((y >> 18) & 511) + k * a.nc2 - ci.czf;
   raw.x += (T)(co.base[0] + dzc * a.cz[0]);
   raw.y += (T)(co.base[1] + dzc * a.cz[1]);
   raw.z += (T)(co.base[2] + dzc * a.cz[2]);
   return raw;
+}
+
+// The far atoms of a cluster's unit list, 32 per step: the entries' atom
+// masks are compacted into a per-warp ring of atom slots (32 entries at a
+// time, in list order), and each step's atom loads are issued before the
+// previous step's pairs. `load(slot)` fetches an atom's data, `use(data,
+// y, valid)` evaluates it (every lane, every step; invalid lanes carry none).
+constexpr int kAtomRing = 256;
+template <typename Data, typename Load, typename Use>
+__device__ __forceinline__ void far_atoms(const int2 *reg, int nf, int lane, int *rslot,
+                                          int *ry, Load &&load, Use &&use) {
+  unsigned head = 0, tail = 0;
+  int next_e = 0;
+  auto produce = [&]() {
+    const int e = next_e + lane;
+    const int2 en = e < nf ? reg[e] : make_int2(0, 0);
+    const unsigned m4 = e < nf ? ((unsigned)en.y >> 27) & 15u : 0u;
+    int incl = __popc(m4);
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, dd);
+      if (lane >= dd) incl += y;
+    }
+    const int tot = __shfl_sync(0xffffffffu, incl, 31);
+    int at = tail + incl - __popc(m4);
+    for (unsigned m = m4; m; m &= m - 1) {
+      const int q = __ffs(m) - 1;
+      rslot[at & (kAtomRing - 1)] = 4 * en.x + q;
+      ry[at & (kAtomRing - 1)] = en.y;
+      ++at;
+    }
+    tail += tot;
+    next_e += 32;
+    __syncwarp();
+  };
+  while (tail - head < 64 && next_e < nf) produce();
+  unsigned idx = head + lane;
+  bool v1 = idx < tail;
+  int y1 = v1 ? ry[idx & (kAtomRing - 1)] : 0;
+  Data d1 = load(v1 ? rslot[idx & (kAtomRing - 1)] : -1);
+  while (head < tail) {
+    const bool v = v1;
+    const int y = y1;
+    const Data d = d1;
+    head = min(head + 32, tail);
+    while (tail - head < 64 && next_e < nf) produce();
+    idx = head + lane;
+    v1 = idx < tail;
+    y1 = v1 ? ry[idx & (kAtomRing - 1)] : 0;
+    d1 = load(v1 ? rslot[idx & (kAtomRing - 1)] : -1);
+    use(d, y, v);
+  }
 }
 
 template <typename T, int NU, bool SELF>
@@ -988,14 +1055,19 @@ __device__ __forceinline__ void pair_jl(const PairClusterArgs<T> &a, const PairC
     if (cnt.x + cnt.y <= a.lcap) {
       sweep = false;
       const int2 *reg = a.list + (size_t)u * a.lcap;
-      // 8 units = 32 atoms per step; the next step's atoms and the entries
-      // of the step after are loaded before this step's pairs, so their
-      // latencies overlap the arithmetic
-      for (int half = 0; half < 2; ++half) {
-        const int n = half ? cnt.y : cnt.x;
-        auto entry = [&](int e) {
-          return e < n ? (half ? reg[a.lcap - 1 - e] : reg[e]) : make_int2(-1, 0);
-        };
+      // far atoms (compacted by their masks), 32 per step
+      far_atoms<V4<T>>(
+          reg, cnt.x, lane, sh.rslot[warp], sh.ry[warp],
+          [&](int slot) { return slot >= 0 ? a.cpos[slot] : dummy; },
+          [&](const V4<T> &raw, int y, bool v) {
+            const V4<T> J = v ? list_shifted(a, ci, raw, y) : dummy;
+            L.template pairs<NU, false>(pc, J, -1, 0, 0, myrec, nrec);
+          });
+      // near units, 8 per step (all 4 atoms, checked); the next step's atoms
+      // and the entries of the step after are loaded before this step's pairs
+      {
+        const int n = cnt.y;
+        auto entry = [&](int e) { return e < n ? reg[a.lcap - 1 - e] : make_int2(-1, 0); };
         int2 en1 = entry(lane >> 2), en2 = entry(8 + (lane >> 2));
         V4<T> raw1 = en1.x >= 0 ? a.cpos[4 * en1.x + (lane & 3)] : dummy;
         for (int e0 = 0; e0 < n; e0 += 8) {
@@ -1005,16 +1077,12 @@ __device__ __forceinline__ void pair_jl(const PairClusterArgs<T> &a, const PairC
           raw1 = en1.x >= 0 ? a.cpos[4 * en1.x + (lane & 3)] : dummy;
           en2 = entry(e0 + 16 + (lane >> 2));
           const V4<T> J = en.x >= 0 ? list_shifted(a, ci, raw, en.y) : dummy;
-          if (half == 0) {
-            L.template pairs<NU, false>(pc, J, -1, 0, 0, myrec, nrec);
-          } else {
-            const int jslot = 4 * en.x + (lane & 3), jcode = en.y & 0x3ffff;
-            int selfk = -1;
-            if (en.x >= 0 && (jslot >> 3) == u &&
-                (SELF || ((jcode >> 8) == a.ozero && (jcode & 255) == 128)))
-              selfk = jslot & 7;
-            L.template pairs<NU, true>(pc, J, selfk, jslot, jcode, myrec, nrec);
-          }
+          const int jslot = 4 * en.x + (lane & 3), jcode = en.y & 0x3ffff;
+          int selfk = -1;
+          if (en.x >= 0 && (jslot >> 3) == u &&
+              (SELF || ((jcode >> 8) == a.ozero && (jcode & 255) == 128)))
+            selfk = jslot & 7;
+          L.template pairs<NU, true>(pc, J, selfk, jslot, jcode, myrec, nrec);
         }
       }
     }
@@ -1224,6 +1292,7 @@ k_slot_gather(int maxcl, const int *__restrict__ ncl, const ClusterInfo *__restr
 
 struct AdjShared {
   JlItems items[kWarps];
+  int rslot[kWarps][256], ry[kWarps][256];
   V4<float> far[kWarps][kRing][2], self[kWarps][kRing][2];
 };
 
@@ -1284,33 +1353,42 @@ k_adj_pair_jl(PairClusterArgs<float> a, PairConsts<float> pc, const V4<float> *_
     if (cnt.x + cnt.y <= a.lcap) {
       sweep = false;
       const int2 *reg = a.list + (size_t)u * a.lcap;
-      for (int half = 0; half < 2; ++half) {
-        const int n = half ? cnt.y : cnt.x;
-        auto entry = [&](int e) {
-          return e < n ? (half ? reg[a.lcap - 1 - e] : reg[e]) : make_int2(-1, 0);
-        };
-        int2 en1 = entry(lane >> 2), en2 = entry(8 + (lane >> 2));
-        V4<float> raw1 = en1.x >= 0 ? a.cpos[4 * en1.x + (lane & 3)] : dummy;
-        V4<float> f1 = en1.x >= 0 ? fslot[4 * en1.x + (lane & 3)] : V4<float>{0.f, 0.f, 0.f, 0.f};
-        for (int e0 = 0; e0 < n; e0 += 8) {
-          const int2 en = en1;
-          const V4<float> raw = raw1, F = f1;
-          en1 = en2;
-          raw1 = en1.x >= 0 ? a.cpos[4 * en1.x + (lane & 3)] : dummy;
-          f1 = en1.x >= 0 ? fslot[4 * en1.x + (lane & 3)] : V4<float>{0.f, 0.f, 0.f, 0.f};
-          en2 = entry(e0 + 16 + (lane >> 2));
-          const V4<float> J = en.x >= 0 ? list_shifted(a, ci, raw, en.y) : dummy;
-          if (half == 0) {
-            L.template pairs<false>(pc, J, F, -1);
-          } else {
-            const int jslot = 4 * en.x + (lane & 3), jcode = en.y & 0x3ffff;
-            int selfk = -1;
-            if (en.x >= 0 && (jslot >> 3) == u &&
-                (SELF || ((jcode >> 8) == a.ozero && (jcode & 255) == 128)))
-              selfk = jslot & 7;
-            L.template pairs<true>(pc, J, F, selfk);
-          }
-        }
+      struct AtomF {
+        V4<float> raw, F;
+      };
+      far_atoms<AtomF>(
+          reg, cnt.x, lane, sh.rslot[warp], sh.ry[warp],
+          [&](int slot) {
+            AtomF d{dummy, V4<float>{0.f, 0.f, 0.f, 0.f}};
+            if (slot >= 0) {
+              d.raw = a.cpos[slot];
+              d.F = fslot[slot];
+            }
+            return d;
+          },
+          [&](const AtomF &d, int y, bool v) {
+            const V4<float> J = v ? list_shifted(a, ci, d.raw, y) : dummy;
+            L.template pairs<false>(pc, J, d.F, -1);
+          });
+      const int n = cnt.y;
+      auto entry = [&](int e) { return e < n ? reg[a.lcap - 1 - e] : make_int2(-1, 0); };
+      int2 en1 = entry(lane >> 2), en2 = entry(8 + (lane >> 2));
+      V4<float> raw1 = en1.x >= 0 ? a.cpos[4 * en1.x + (lane & 3)] : dummy;
+      V4<float> f1 = en1.x >= 0 ? fslot[4 * en1.x + (lane & 3)] : V4<float>{0.f, 0.f, 0.f, 0.f};
+      for (int e0 = 0; e0 < n; e0 += 8) {
+        const int2 en = en1;
+        const V4<float> raw = raw1, F = f1;
+        en1 = en2;
+        raw1 = en1.x >= 0 ? a.cpos[4 * en1.x + (lane & 3)] : dummy;
+        f1 = en1.x >= 0 ? fslot[4 * en1.x + (lane & 3)] : V4<float>{0.f, 0.f, 0.f, 0.f};
+        en2 = entry(e0 + 16 + (lane >> 2));
+        const V4<float> J = en.x >= 0 ? list_shifted(a, ci, raw, en.y) : dummy;
+        const int jslot = 4 * en.x + (lane & 3), jcode = en.y & 0x3ffff;
+        int selfk = -1;
+        if (en.x >= 0 && (jslot >> 3) == u &&
+            (SELF || ((jcode >> 8) == a.ozero && (jcode & 255) == 128)))
+          selfk = jslot & 7;
+        L.template pairs<true>(pc, J, F, selfk);
       }
     }
   }
