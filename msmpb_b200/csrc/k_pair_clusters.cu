@@ -514,7 +514,7 @@ __device__ __forceinline__ void pair_clusters(const PairClusterArgs<T> &a,
 // pair is summed once from each side; the lanes' partial sums are combined
 // by a fixed butterfly, so the result does not depend on timing.
 constexpr int kRing = 64;        // entries per queue ring (a warp adds <= 32 at a time)
-constexpr int kCloseLane = 6;    // close-pair records per lane and i-cluster
+constexpr int kCloseLane = 12;   // close-pair records per lane and i-cluster
 constexpr int kGroupCap = 32 * kCloseLane;
 
 // One warp's (column, image) items of the current Phase A batch
@@ -523,14 +523,26 @@ struct JlItems {
   double shift[32][3];
 };
 
+// One warp's buffers: the queues of the sweep and the list streams, which
+// the close pairs regrouped by atom reuse once the warp's pairs are done
+// (each warp aliases only its own buffers)
+template <typename T>
+struct JlWarpBufs {
+  union {
+    struct {
+      int rslot[256], ry[256];  // far-atom ring of the list stream
+      V4<T> far[kRing], near[kRing];
+      int2 ninfo[kRing];
+    };
+    int2 grp[sizeof(T) == 4 ? kGroupCap : 1];
+  };
+  int2 rec[sizeof(T) == 4 ? 32 * kCloseLane : 1];
+};
+
 template <typename T>
 struct JlShared {
   JlItems items[kWarps];
-  int rslot[kWarps][256], ry[kWarps][256];  // far-atom ring of the list stream
-  V4<T> far[kWarps][kRing], near[kWarps][kRing];
-  int2 ninfo[kWarps][kRing];
-  int2 rec[kWarps][sizeof(T) == 4 ? 32 * kCloseLane : 1];
-  int2 grp[kWarps][sizeof(T) == 4 ? kGroupCap : 1];
+  JlWarpBufs<T> w[kWarps];
 };
 
 // Item `it` of i-cluster ci's candidates: the column offset o = it / nseg
@@ -956,8 +968,8 @@ __device__ __forceinline__ V4<T> list_shifted(const PairClusterArgs<T> &a, const
 
 // The far atoms of a cluster's unit list, 32 per step: the entries' atom
 // masks are compacted into a per-warp ring of atom slots (32 entries at a
-// time, in list order), and each step's atom loads are issued before the
-// previous step's pairs. `load(slot)` fetches an atom's data, `use(data,
+// time, in list order, each batch of entries loaded one refill ahead), and
+// each step's atom loads are issued before the previous step's pairs. `load(slot)` fetches an atom's data, `use(data,
 // y, valid)` evaluates it (every lane, every step; invalid lanes carry none).
 constexpr int kAtomRing = 256;
 template <typename Data, typename Load, typename Use>
@@ -965,9 +977,12 @@ __device__ __forceinline__ void far_atoms(const int2 *reg, int nf, int lane, int
                                           int *ry, Load &&load, Use &&use) {
   unsigned head = 0, tail = 0;
   int next_e = 0;
+  // the next 32 entries, loaded one refill ahead (the lists live in DRAM)
+  int2 en_n = lane < nf ? reg[lane] : make_int2(0, 0);
   auto produce = [&]() {
     const int e = next_e + lane;
-    const int2 en = e < nf ? reg[e] : make_int2(0, 0);
+    const int2 en = en_n;
+    en_n = e + 32 < nf ? reg[e + 32] : make_int2(0, 0);
     const unsigned m4 = e < nf ? ((unsigned)en.y >> 27) & 15u : 0u;
     int incl = __popc(m4);
 #pragma unroll
@@ -1023,21 +1038,21 @@ __device__ __forceinline__ void pair_jl(const PairClusterArgs<T> &a, const PairC
     L.set(k, ak);
   }
   L.zero();
-  int2 *myrec = kMixed ? &sh.rec[warp][lane * kCloseLane] : nullptr;
+  int2 *myrec = kMixed ? &sh.w[warp].rec[lane * kCloseLane] : nullptr;
   int nrec = 0;
   unsigned fhead = 0, ftail = 0, nhead = 0, ntail = 0;
   const V4<T> dummy{(T)kFar, (T)kFar, (T)kFar, T(0)};
 
   auto far_step = [&](int cnt) {
-    V4<T> J = sh.far[warp][(fhead + lane) & (kRing - 1)];
+    V4<T> J = sh.w[warp].far[(fhead + lane) & (kRing - 1)];
     if (lane >= cnt) J = dummy;
     L.template pairs<NU, false>(pc, J, -1, 0, 0, myrec, nrec);
     fhead += cnt;
   };
   auto near_step = [&](int cnt) {
     const int e = (nhead + lane) & (kRing - 1);
-    V4<T> J = sh.near[warp][e];
-    int2 inf = sh.ninfo[warp][e];
+    V4<T> J = sh.w[warp].near[e];
+    int2 inf = sh.w[warp].ninfo[e];
     if (lane >= cnt) {
       J = dummy;
       inf = make_int2(0, 0);
@@ -1057,7 +1072,7 @@ __device__ __forceinline__ void pair_jl(const PairClusterArgs<T> &a, const PairC
       const int2 *reg = a.list + (size_t)u * a.lcap;
       // far atoms (compacted by their masks), 32 per step
       far_atoms<V4<T>>(
-          reg, cnt.x, lane, sh.rslot[warp], sh.ry[warp],
+          reg, cnt.x, lane, sh.w[warp].rslot, sh.w[warp].ry,
           [&](int slot) { return slot >= 0 ? a.cpos[slot] : dummy; },
           [&](const V4<T> &raw, int y, bool v) {
             const V4<T> J = v ? list_shifted(a, ci, raw, y) : dummy;
@@ -1093,11 +1108,11 @@ __device__ __forceinline__ void pair_jl(const PairClusterArgs<T> &a, const PairC
                         int selfk, int) {
     const unsigned mf = __ballot_sync(0xffffffffu, pass && !near);
     const unsigned mn = __ballot_sync(0xffffffffu, pass && near);
-    if (pass && !near) sh.far[warp][(ftail + __popc(mf & lt)) & (kRing - 1)] = J;
+    if (pass && !near) sh.w[warp].far[(ftail + __popc(mf & lt)) & (kRing - 1)] = J;
     if (pass && near) {
       const int e = (ntail + __popc(mn & lt)) & (kRing - 1);
-      sh.near[warp][e] = J;
-      sh.ninfo[warp][e] = make_int2(jslot, jcode | ((selfk + 1) << 24));
+      sh.w[warp].near[e] = J;
+      sh.w[warp].ninfo[e] = make_int2(jslot, jcode | ((selfk + 1) << 24));
     }
     ftail += __popc(mf);
     ntail += __popc(mn);
@@ -1119,35 +1134,56 @@ __device__ __forceinline__ void pair_jl(const PairClusterArgs<T> &a, const PairC
   double close = 0.;
   if constexpr (kMixed) {
     // close pairs in FP64: the lanes' records regrouped by i atom (counts
-    // of the 8 atoms packed in the bytes of a 64-bit word, scanned over
-    // lanes), then lane (i, sub = lane >> 3) sums every 4th record of atom
-    // i, and the four subs are added in a fixed order
-    unsigned long long cnt = 0;
-    for (int t = 0; t < nrec; ++t) cnt += 1ull << (8 * (myrec[t].y >> 24));
-    unsigned long long incl = cnt;
+    // of atoms 0-3 and 4-7 packed in the 16-bit fields of two 64-bit words,
+    // scanned over lanes), then lane (i, sub = lane >> 3) sums every 4th
+    // record of atom i, and the four subs are added in a fixed order
+    unsigned long long c0 = 0ull, c1 = 0ull;  // atoms 0-3, 4-7
+    for (int t = 0; t < nrec; ++t) {
+      const int ia = myrec[t].y >> 24;
+      const unsigned long long one = 1ull << (16 * (ia & 3));
+      if (ia < 4) c0 += one; else c1 += one;
+    }
+    unsigned long long i0 = c0, i1 = c1;
 #pragma unroll
     for (int dd = 1; dd < 32; dd <<= 1) {
-      const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, dd);
-      if (lane >= dd) incl += y;
+      const unsigned long long y0 = __shfl_up_sync(0xffffffffu, i0, dd);
+      const unsigned long long y1 = __shfl_up_sync(0xffffffffu, i1, dd);
+      if (lane >= dd) {
+        i0 += y0;
+        i1 += y1;
+      }
     }
-    const unsigned long long tot = __shfl_sync(0xffffffffu, incl, 31);
+    const unsigned long long t0 = __shfl_sync(0xffffffffu, i0, 31);
+    const unsigned long long t1 = __shfl_sync(0xffffffffu, i1, 31);
     double cf[4] = {0., 0., 0., 0.};
-    if (tot) {
-      const unsigned long long base = tot * 0x0101010101010100ull;  // exclusive byte prefix
-      unsigned long long pos = base + (incl - cnt);
+    if (t0 | t1) {
+      // exclusive prefix over atoms: within each word by the multiply, then
+      // the second word offset by the sum of the first (all sums below 2^16)
+      const unsigned long long sum0 = (t0 * 0x0001000100010001ull) >> 48;
+      const unsigned long long b0 = t0 * 0x0001000100010000ull;
+      const unsigned long long b1 = t1 * 0x0001000100010000ull + sum0 * 0x0001000100010001ull;
+      unsigned long long p0 = b0 + (i0 - c0), p1 = b1 + (i1 - c1);
       for (int t = 0; t < nrec; ++t) {
         const int ia = myrec[t].y >> 24;
-        const int at = (int)((pos >> (8 * ia)) & 255);
-        pos += 1ull << (8 * ia);
-        sh.grp[warp][at] = myrec[t];
+        const int sft = 16 * (ia & 3);
+        int at;
+        if (ia < 4) {
+          at = (int)((p0 >> sft) & 0xffff);
+          p0 += 1ull << sft;
+        } else {
+          at = (int)((p1 >> sft) & 0xffff);
+          p1 += 1ull << sft;
+        }
+        sh.w[warp].grp[at] = myrec[t];
       }
+      const int gb = (int)((((i < 4) ? b0 : b1) >> (16 * (i & 3))) & 0xffff);
+      const int gn = (int)((((i < 4) ? t0 : t1) >> (16 * (i & 3))) & 0xffff);
       __syncwarp();
       const int sub = lane >> 3;
-      const int gb = (int)((base >> (8 * i)) & 255), gn = (int)((tot >> (8 * i)) & 255);
       if (gn > sub) {
         const V4<double> ai64 = a.cpos64[u * 8 + i];
         for (int t = sub; t < gn; t += 4) {
-          const int2 r = sh.grp[warp][gb + t];
+          const int2 r = sh.w[warp].grp[gb + t];
           const int jslot = r.x, code = r.y & 0xffffff;
           const int o = code >> 8, k = (code & 255) - 128;
           const ColumnOffset &co = a.coloff[o];
@@ -1290,10 +1326,13 @@ k_slot_gather(int maxcl, const int *__restrict__ ncl, const ClusterInfo *__restr
   fslot[s] = f;
 }
 
+struct AdjWarpBufs {
+  int rslot[256], ry[256];
+  V4<float> far[kRing][2], self[kRing][2];
+};
 struct AdjShared {
   JlItems items[kWarps];
-  int rslot[kWarps][256], ry[kWarps][256];
-  V4<float> far[kWarps][kRing][2], self[kWarps][kRing][2];
+  AdjWarpBufs w[kWarps];
 };
 
 template <int NU, bool SELF>
@@ -1329,7 +1368,7 @@ k_adj_pair_jl(PairClusterArgs<float> a, PairConsts<float> pc, const V4<float> *_
   const V4<float> dummy{kFar, kFar, kFar, 0.f};
   auto far_step = [&](int cnt) {
     const int e = (fhead + lane) & (kRing - 1);
-    V4<float> J = sh.far[warp][e][0], F = sh.far[warp][e][1];
+    V4<float> J = sh.w[warp].far[e][0], F = sh.w[warp].far[e][1];
     if (lane >= cnt) {  // no entry: zero charge and Fbar (stale slots may hold anything)
       J = dummy;
       F = V4<float>{0.f, 0.f, 0.f, 0.f};
@@ -1339,7 +1378,7 @@ k_adj_pair_jl(PairClusterArgs<float> a, PairConsts<float> pc, const V4<float> *_
   };
   auto self_step = [&](int cnt) {
     const int e = (shead + lane) & (kRing - 1);
-    V4<float> J = sh.self[warp][e][0], F = sh.self[warp][e][1];
+    V4<float> J = sh.w[warp].self[e][0], F = sh.w[warp].self[e][1];
     if (lane >= cnt) {
       J = dummy;
       F = V4<float>{0.f, 0.f, 0.f, __int_as_float(-1)};
@@ -1357,7 +1396,7 @@ k_adj_pair_jl(PairClusterArgs<float> a, PairConsts<float> pc, const V4<float> *_
         V4<float> raw, F;
       };
       far_atoms<AtomF>(
-          reg, cnt.x, lane, sh.rslot[warp], sh.ry[warp],
+          reg, cnt.x, lane, sh.w[warp].rslot, sh.w[warp].ry,
           [&](int slot) {
             AtomF d{dummy, V4<float>{0.f, 0.f, 0.f, 0.f}};
             if (slot >= 0) {
@@ -1404,13 +1443,13 @@ k_adj_pair_jl(PairClusterArgs<float> a, PairConsts<float> pc, const V4<float> *_
     const unsigned ms = __ballot_sync(0xffffffffu, pass && own);
     if (pass && !own) {
       const int e = (ftail + __popc(mf & lt)) & (kRing - 1);
-      sh.far[warp][e][0] = J;
-      sh.far[warp][e][1] = F;
+      sh.w[warp].far[e][0] = J;
+      sh.w[warp].far[e][1] = F;
     }
     if (pass && own) {
       const int e = (stail + __popc(ms & lt)) & (kRing - 1);
-      sh.self[warp][e][0] = J;
-      sh.self[warp][e][1] = F;
+      sh.w[warp].self[e][0] = J;
+      sh.w[warp].self[e][1] = F;
     }
     ftail += __popc(mf);
     stail += __popc(ms);

@@ -157,6 +157,23 @@ def test_five_levels_headline_depth(precision):
     assert abs(0.5 * d["q"] @ phi - e) / scale < te * 10
 
 
+def test_mixed_close_to_fp64_on_dense_water():
+    """The mixed form against the FP64 form on a water box at liquid density
+    (24,000 atoms, order 6, cutoff 9 A, three levels): pairs closer than
+    2.5 A (bonded and overlapping atoms) are summed in FP64 and the rest
+    compensated, so the two forms agree to the FP32 rounding level of the far
+    pairs, far below the method's error (~2e-6 of the force at these
+    parameters): RMS force difference < 3e-7 of the RMS force, energy < 1e-8."""
+    q, pos, edges = systems.water(8000, systems.water_edge(8000), 41)
+    kw = dict(cutoff=9.0, order=6, levels=3, top_grid=10)
+    f64 = ForceField(q, pos, edges, **kw, precision="fp64")
+    mix = ForceField(q, pos, edges, **kw, precision="mixed")
+    e1, f1 = f64.energy(pos)
+    e2, f2 = mix.energy(pos)
+    assert abs(e2 - e1) / abs(e1) < 1e-8
+    assert rel_rms(f2, f1) < 3e-7
+
+
 def test_high_accuracy_parameters_match_oracle():
     """The parameters of the bench's high-accuracy reference (the FP64 GPU
     MSM with order 10, cutoff 12 A, one level, h ~ 1.0 A, against which the
