@@ -472,10 +472,7 @@ int Plan<T>::init(const Tables &t, int device) {
   if (kMixed) a.want(&cpos64_, (size_t)maxcl_ * 8 * sizeof(V4<double>));
   a.want(&cinfo_, (size_t)maxcl_ * sizeof(ClusterInfo));
   a.want(&cubox_, (size_t)maxcl_ * 2 * sizeof(UnitBox));
-  if (kMixed) {
-    a.want(&ulist_, (size_t)maxcl_ * kUnitListCap * sizeof(int2));
-    a.want(&ulcnt_, (size_t)maxcl_ * sizeof(int2));
-  }
+
   a.want(&err_d_, sizeof(int));
   if ((err = a.commit())) return err;
   MSM_CUDA_TRY(cudaMemset(err_d_, 0, sizeof(int)));
@@ -899,10 +896,6 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   mark(s, kPhasePair, tm);
   if (clusters) {
     const PairClusterArgs<T> ca = cluster_args();
-    if (ca.list) {
-      launch_pair_list<T>(sp, ca);
-      nl += 1;
-    }
     launch_pair_clusters<T>(sp, ca, pc_);
     nl += scan_launches(ncol_) + 1;
   } else if (pair_variant_ == 0 && pair_cells_supported(noff_, N_)) {
@@ -1030,7 +1023,11 @@ int Plan<T>::adjoint(const AdjointRequest &r) {
   if (!r.pos || !r.q || !r.fbar) return MSMPB_ERR_ARGUMENT;
   if (!adj_mem_) {
     // six per-atom records and a second set of level grids
-    size_t bytes = 6 * (size_t)N_ * sizeof(V4<T>) + 256 * 7 + 8 * (size_t)maxcl_ * sizeof(V4<T>);
+    // (+ the cluster pass's Fbar in slot order and unit lists, mixed form)
+    const bool lists = kMixed && clusters_ok_;
+    size_t bytes = 6 * (size_t)N_ * sizeof(V4<T>) + 256 * 9 + 8 * (size_t)maxcl_ * sizeof(V4<T>);
+    if (lists)
+      bytes += (size_t)maxcl_ * (kUnitListCap + 1) * sizeof(int2);
     for (int l = 1; l <= L_; ++l)
       bytes += 2 * ((size_t)grid_[l][0] * grid_[l][1] * grid_[l][2] * sizeof(T) + 256);
     if (cudaMalloc(&adj_mem_, bytes) != cudaSuccess) {
@@ -1047,6 +1044,10 @@ int Plan<T>::adjoint(const AdjointRequest &r) {
     for (V4<T> **b : {&fbs_, &dip_, &adj_a_, &adj_b_, &adj_g_, &adj_h_})
       *b = reinterpret_cast<V4<T> *>(take((size_t)N_ * sizeof(V4<T>)));
     fslot_ = reinterpret_cast<V4<T> *>(take(8 * (size_t)maxcl_ * sizeof(V4<T>)));
+    if (lists) {
+      ulist_ = reinterpret_cast<int2 *>(take((size_t)maxcl_ * kUnitListCap * sizeof(int2)));
+      ulcnt_ = reinterpret_cast<int2 *>(take((size_t)maxcl_ * sizeof(int2)));
+    }
     for (int l = 1; l <= L_; ++l) {
       const size_t g = (size_t)grid_[l][0] * grid_[l][1] * grid_[l][2] * sizeof(T);
       qg2_[l] = reinterpret_cast<T *>(take(g));
@@ -1070,8 +1071,11 @@ int Plan<T>::adjoint(const AdjointRequest &r) {
   }
   launch_adj_gather<T>(s, N_, pperm_, r.fbar, fbs_);
   // the forward just run (or reused) built the clusters of these positions
-  if (pair_variant_ == 2 && clusters_ok_ && adj_pair_clusters_supported<T>())
-    launch_adj_pair_clusters<T>(s, cluster_args(), pc_, fbs_, fslot_, adj_a_, adj_b_);
+  if (pair_variant_ == 2 && clusters_ok_ && adj_pair_clusters_supported<T>()) {
+    const PairClusterArgs<T> ca = cluster_args();
+    if (ca.list) launch_pair_list<T>(s, ca);  // the unit lists of these positions
+    launch_adj_pair_clusters<T>(s, ca, pc_, fbs_, fslot_, adj_a_, adj_b_);
+  }
   else
     launch_adj_pair<T>(s, N_, psorted_, fbs_, pcs_, pstart_, geom_, off_d_, noff_, pc_,
                        adj_a_, adj_b_);

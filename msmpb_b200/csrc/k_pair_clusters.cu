@@ -514,35 +514,11 @@ __device__ __forceinline__ void pair_clusters(const PairClusterArgs<T> &a,
 // pair is summed once from each side; the lanes' partial sums are combined
 // by a fixed butterfly, so the result does not depend on timing.
 constexpr int kRing = 64;        // entries per queue ring (a warp adds <= 32 at a time)
-constexpr int kCloseLane = 12;   // close-pair records per lane and i-cluster
-constexpr int kGroupCap = 32 * kCloseLane;
 
 // One warp's (column, image) items of the current Phase A batch
 struct JlItems {
   int off[32], s0[32], a0[32], code[32];
   double shift[32][3];
-};
-
-// One warp's buffers: the queues of the sweep and the list streams, which
-// the close pairs regrouped by atom reuse once the warp's pairs are done
-// (each warp aliases only its own buffers)
-template <typename T>
-struct JlWarpBufs {
-  union {
-    struct {
-      int rslot[256], ry[256];  // far-atom ring of the list stream
-      V4<T> far[kRing], near[kRing];
-      int2 ninfo[kRing];
-    };
-    int2 grp[sizeof(T) == 4 ? kGroupCap : 1];
-  };
-  int2 rec[sizeof(T) == 4 ? 32 * kCloseLane : 1];
-};
-
-template <typename T>
-struct JlShared {
-  JlItems items[kWarps];
-  JlWarpBufs<T> w[kWarps];
 };
 
 // Item `it` of i-cluster ci's candidates: the column offset o = it / nseg
@@ -807,165 +783,6 @@ __device__ __forceinline__ T butterfly32(T (&v)[32], int lane) {
   return v[0];
 }
 
-// One lane's 8 i atoms (negated: d = x_j - x_i) and partial sums: q_j V in
-// p and q_j g d in x/y/z, g = -f = 1/r^3 + 2 tau'(s)/a0^3 (the field is
-// -sum q_j g d). FP32: packed pairs (2p, 2p+1); FP64: scalars.
-template <typename T> struct JlLane;
-
-template <>
-struct JlLane<float> {
-  float2 nix[4], niy[4], niz[4];
-  float2 ax[4], ay[4], az[4], ap[4];
-  __device__ __forceinline__ void set(int k, const V4<float> &a) {
-    float *x = reinterpret_cast<float *>(&nix[k >> 1]) + (k & 1);
-    float *y = reinterpret_cast<float *>(&niy[k >> 1]) + (k & 1);
-    float *z = reinterpret_cast<float *>(&niz[k >> 1]) + (k & 1);
-    *x = -a.x;
-    *y = -a.y;
-    *z = -a.z;
-  }
-  __device__ __forceinline__ void zero() {
-#pragma unroll
-    for (int p = 0; p < 4; ++p) ax[p] = ay[p] = az[p] = ap[p] = make_float2(0.f, 0.f);
-  }
-  __device__ __forceinline__ void values(float (&v)[32]) const {
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      v[2 * p] = ax[p].x;
-      v[2 * p + 1] = ax[p].y;
-      v[8 + 2 * p] = ay[p].x;
-      v[8 + 2 * p + 1] = ay[p].y;
-      v[16 + 2 * p] = az[p].x;
-      v[16 + 2 * p + 1] = az[p].y;
-      v[24 + 2 * p] = ap[p].x;
-      v[24 + 2 * p + 1] = ap[p].y;
-    }
-  }
-  // The 8 pairs of one j atom (position in the i-cluster's frame, charge in
-  // J.w). NEAR: the pair with i atom `selfk` is the atom itself (skipped),
-  // and pairs closer than sqrt(close2) are recorded for the FP64 pass while
-  // the lane's record has room (else summed here).
-  template <int NU, bool NEAR>
-  __device__ __forceinline__ void pairs(const PairConsts<float> &pc, const V4<float> &J,
-                                        int selfk, int jslot, int code, int2 *myrec,
-                                        int &nrec) {
-    const float2 jx = make_float2(J.x, J.x), jy = make_float2(J.y, J.y),
-                 jz = make_float2(J.z, J.z);
-#pragma unroll
-    for (int p = 0; p < 4; ++p) {
-      const float2 dx = __fadd2_rn(jx, nix[p]);
-      const float2 dy = __fadd2_rn(jy, niy[p]);
-      const float2 dz = __fadd2_rn(jz, niz[p]);
-      float2 r2 = __fmul2_rn(dx, dx);
-      r2 = __ffma2_rn(dy, dy, r2);
-      r2 = __ffma2_rn(dz, dz, r2);
-      bool h0 = r2.x < pc.a02, h1 = r2.y < pc.a02;
-      if constexpr (NEAR) {
-        if (selfk == 2 * p) h0 = false;
-        if (selfk == 2 * p + 1) h1 = false;
-        if (h0 && r2.x < pc.close2 && nrec < kCloseLane) {
-          myrec[nrec++] = make_int2(jslot, code | ((2 * p) << 24));
-          h0 = false;
-        }
-        if (h1 && r2.y < pc.close2 && nrec < kCloseLane) {
-          myrec[nrec++] = make_int2(jslot, code | ((2 * p + 1) << 24));
-          h1 = false;
-        }
-      }
-      const float2 rr = make_float2(h0 ? r2.x : pc.a02, h1 ? r2.y : pc.a02);
-      const float2 qj = make_float2(h0 ? J.w : 0.f, h1 ? J.w : 0.f);
-      float2 v, g;
-      if constexpr (NU == 0) {  // PME kernel, packed (pair_fn.cuh)
-        float2 f;
-        pme_radial2(pc, rr, v, f);
-        g = make_float2(-f.x, -f.y);
-      } else {
-        const float2 s = __ffma2_rn(rr, make_float2(pc.inv_a02, pc.inv_a02),
-                                    make_float2(-1.f, -1.f));
-        // tau(s) and tau'(s) by two independent Horner chains
-        float2 ts = make_float2(pc.tau[NU - 1], pc.tau[NU - 1]);
-        float2 t1 = make_float2((NU - 1) * pc.tau[NU - 1], (NU - 1) * pc.tau[NU - 1]);
-#pragma unroll
-        for (int m = NU - 2; m >= 0; --m) {
-          ts = __ffma2_rn(s, ts, make_float2(pc.tau[m], pc.tau[m]));
-          if (m >= 1) t1 = __ffma2_rn(s, t1, make_float2(m * pc.tau[m], m * pc.tau[m]));
-        }
-        const float2 rinv = make_float2(rsqrtf(rr.x), rsqrtf(rr.y));
-        v = __ffma2_rn(ts, make_float2(-pc.inv_a0, -pc.inv_a0), rinv);
-        const float2 rinv3 = __fmul2_rn(__fmul2_rn(rinv, rinv), rinv);
-        g = __ffma2_rn(t1, make_float2(pc.two_inv_a03, pc.two_inv_a03), rinv3);
-      }
-      ap[p] = __ffma2_rn(qj, v, ap[p]);
-      const float2 w = __fmul2_rn(qj, g);
-      ax[p] = __ffma2_rn(w, dx, ax[p]);
-      ay[p] = __ffma2_rn(w, dy, ay[p]);
-      az[p] = __ffma2_rn(w, dz, az[p]);
-    }
-  }
-};
-
-template <>
-struct JlLane<double> {
-  double nix[8], niy[8], niz[8];
-  double ax[8], ay[8], az[8], ap[8];
-  __device__ __forceinline__ void set(int k, const V4<double> &a) {
-    nix[k] = -a.x;
-    niy[k] = -a.y;
-    niz[k] = -a.z;
-  }
-  __device__ __forceinline__ void zero() {
-#pragma unroll
-    for (int k = 0; k < 8; ++k) ax[k] = ay[k] = az[k] = ap[k] = 0.;
-  }
-  __device__ __forceinline__ void values(double (&v)[32]) const {
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      v[k] = ax[k];
-      v[8 + k] = ay[k];
-      v[16 + k] = az[k];
-      v[24 + k] = ap[k];
-    }
-  }
-  // NEAR: only the atom itself is skipped (the FP64 form has no close path)
-  template <int NU, bool NEAR>
-  __device__ __forceinline__ void pairs(const PairConsts<double> &pc, const V4<double> &J,
-                                        int selfk, int, int, int2 *, int &) {
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      const double dx = J.x + nix[k], dy = J.y + niy[k], dz = J.z + niz[k];
-      const double r2 = dx * dx + dy * dy + dz * dz;
-      bool h = r2 < pc.a02;
-      if constexpr (NEAR) {
-        if (selfk == k) h = false;
-      }
-      const double rr = h ? r2 : pc.a02;
-      const double qj = h ? J.w : 0.;
-      double v, f;
-      pair_radial<double, NU>(pc, rr, v, f);
-      ap[k] = fma(qj, v, ap[k]);
-      const double w = -qj * f;
-      ax[k] = fma(w, dx, ax[k]);
-      ay[k] = fma(w, dy, ay[k]);
-      az[k] = fma(w, dz, az[k]);
-    }
-  }
-};
-
-// A list atom (cluster-frame position `raw`) shifted into the frame of the
-// i-cluster ci by the FP64 shift of its cluster's frame (entry y: item code
-// and the cluster's first cell), rounded once.
-template <typename T>
-__device__ __forceinline__ V4<T> list_shifted(const PairClusterArgs<T> &a, const ClusterInfo &ci,
-                                              V4<T> raw, int y) {
-  const int o = (y >> 8) & 1023, k = (y & 255) - 128;
-  const ColumnOffset &co = a.coloff[o];
-  const int dzc = ((y >> 18) & 511) + k * a.nc2 - ci.czf;
-  raw.x += (T)(co.base[0] + dzc * a.cz[0]);
-  raw.y += (T)(co.base[1] + dzc * a.cz[1]);
-  raw.z += (T)(co.base[2] + dzc * a.cz[2]);
-  return raw;
-}
-
 // The far atoms of a cluster's unit list, 32 per step: the entries' atom
 // masks are compacted into a per-warp ring of atom slots (32 entries at a
 // time, in list order, each batch of entries loaded one refill ahead), and
@@ -1021,214 +838,19 @@ __device__ __forceinline__ void far_atoms(const int2 *reg, int nf, int lane, int
   }
 }
 
-template <typename T, int NU, bool SELF>
-__device__ __forceinline__ void pair_jl(const PairClusterArgs<T> &a, const PairConsts<T> &pc) {
-  constexpr bool kMixed = sizeof(T) == 4;
-  __shared__ JlShared<T> sh;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int u = blockIdx.x * kWarps + warp;
-  if (u >= a.maxcl || u >= a.clstart[a.ncol]) return;  // whole warp
-  const ClusterInfo ci = a.info[u];
-  const unsigned lt = (1u << lane) - 1u;
-  JlLane<T> L;
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    V4<T> ak = a.cpos[u * 8 + k];
-    if (k >= ci.n) ak.x = ak.y = ak.z = -(T)kFar;
-    L.set(k, ak);
-  }
-  L.zero();
-  int2 *myrec = kMixed ? &sh.w[warp].rec[lane * kCloseLane] : nullptr;
-  int nrec = 0;
-  unsigned fhead = 0, ftail = 0, nhead = 0, ntail = 0;
-  const V4<T> dummy{(T)kFar, (T)kFar, (T)kFar, T(0)};
-
-  auto far_step = [&](int cnt) {
-    V4<T> J = sh.w[warp].far[(fhead + lane) & (kRing - 1)];
-    if (lane >= cnt) J = dummy;
-    L.template pairs<NU, false>(pc, J, -1, 0, 0, myrec, nrec);
-    fhead += cnt;
-  };
-  auto near_step = [&](int cnt) {
-    const int e = (nhead + lane) & (kRing - 1);
-    V4<T> J = sh.w[warp].near[e];
-    int2 inf = sh.w[warp].ninfo[e];
-    if (lane >= cnt) {
-      J = dummy;
-      inf = make_int2(0, 0);
-    }
-    L.template pairs<NU, true>(pc, J, (inf.y >> 24) - 1, inf.x, inf.y & 0xffffff, myrec,
-                               nrec);
-    nhead += cnt;
-  };
-  // the cluster's unit list (built by k_pair_list), 8 units = 32 atoms per
-  // step, far units the lean way, near units checked; a cluster whose list
-  // overflowed its region sweeps its candidates here instead
-  bool sweep = true;
-  if (a.list) {
-    const int2 cnt = a.lcnt[u];
-    if (cnt.x + cnt.y <= a.lcap) {
-      sweep = false;
-      const int2 *reg = a.list + (size_t)u * a.lcap;
-      // far atoms (compacted by their masks), 32 per step
-      far_atoms<V4<T>>(
-          reg, cnt.x, lane, sh.w[warp].rslot, sh.w[warp].ry,
-          [&](int slot) { return slot >= 0 ? a.cpos[slot] : dummy; },
-          [&](const V4<T> &raw, int y, bool v) {
-            const V4<T> J = v ? list_shifted(a, ci, raw, y) : dummy;
-            L.template pairs<NU, false>(pc, J, -1, 0, 0, myrec, nrec);
-          });
-      // near units, 8 per step (all 4 atoms, checked); the next step's atoms
-      // and the entries of the step after are loaded before this step's pairs
-      {
-        const int n = cnt.y;
-        auto entry = [&](int e) { return e < n ? reg[a.lcap - 1 - e] : make_int2(-1, 0); };
-        int2 en1 = entry(lane >> 2), en2 = entry(8 + (lane >> 2));
-        V4<T> raw1 = en1.x >= 0 ? a.cpos[4 * en1.x + (lane & 3)] : dummy;
-        for (int e0 = 0; e0 < n; e0 += 8) {
-          const int2 en = en1;
-          const V4<T> raw = raw1;
-          en1 = en2;
-          raw1 = en1.x >= 0 ? a.cpos[4 * en1.x + (lane & 3)] : dummy;
-          en2 = entry(e0 + 16 + (lane >> 2));
-          const V4<T> J = en.x >= 0 ? list_shifted(a, ci, raw, en.y) : dummy;
-          const int jslot = 4 * en.x + (lane & 3), jcode = en.y & 0x3ffff;
-          int selfk = -1;
-          if (en.x >= 0 && (jslot >> 3) == u &&
-              (SELF || ((jcode >> 8) == a.ozero && (jcode & 255) == 128)))
-            selfk = jslot & 7;
-          L.template pairs<NU, true>(pc, J, selfk, jslot, jcode, myrec, nrec);
-        }
-      }
-    }
-  }
-  if (sweep) {
-  jl_sweep<T, SELF>(a, ci, u, lane, sh.items[warp],
-                    [&](bool pass, bool near, const V4<T> &J, int jslot, int jcode,
-                        int selfk, int) {
-    const unsigned mf = __ballot_sync(0xffffffffu, pass && !near);
-    const unsigned mn = __ballot_sync(0xffffffffu, pass && near);
-    if (pass && !near) sh.w[warp].far[(ftail + __popc(mf & lt)) & (kRing - 1)] = J;
-    if (pass && near) {
-      const int e = (ntail + __popc(mn & lt)) & (kRing - 1);
-      sh.w[warp].near[e] = J;
-      sh.w[warp].ninfo[e] = make_int2(jslot, jcode | ((selfk + 1) << 24));
-    }
-    ftail += __popc(mf);
-    ntail += __popc(mn);
-    __syncwarp();
-    if (ftail - fhead >= 32) far_step(32);
-    if (ntail - nhead >= 32) near_step(32);
-    __syncwarp();
-  });
-  if (ftail != fhead) far_step((int)(ftail - fhead));
-  if (ntail != nhead) near_step((int)(ntail - nhead));
-  }
-
-  // lanes' partial sums: lane l ends with value l = 8 c + i (c: 0..2 the
-  // negated field components, 3 the potential; i the atom)
-  T v[32];
-  L.values(v);
-  const T vsum = butterfly32(v, lane);
-  const int i = lane & 7, c = lane >> 3;
-  double close = 0.;
-  if constexpr (kMixed) {
-    // close pairs in FP64: the lanes' records regrouped by i atom (counts
-    // of atoms 0-3 and 4-7 packed in the 16-bit fields of two 64-bit words,
-    // scanned over lanes), then lane (i, sub = lane >> 3) sums every 4th
-    // record of atom i, and the four subs are added in a fixed order
-    unsigned long long c0 = 0ull, c1 = 0ull;  // atoms 0-3, 4-7
-    for (int t = 0; t < nrec; ++t) {
-      const int ia = myrec[t].y >> 24;
-      const unsigned long long one = 1ull << (16 * (ia & 3));
-      if (ia < 4) c0 += one; else c1 += one;
-    }
-    unsigned long long i0 = c0, i1 = c1;
-#pragma unroll
-    for (int dd = 1; dd < 32; dd <<= 1) {
-      const unsigned long long y0 = __shfl_up_sync(0xffffffffu, i0, dd);
-      const unsigned long long y1 = __shfl_up_sync(0xffffffffu, i1, dd);
-      if (lane >= dd) {
-        i0 += y0;
-        i1 += y1;
-      }
-    }
-    const unsigned long long t0 = __shfl_sync(0xffffffffu, i0, 31);
-    const unsigned long long t1 = __shfl_sync(0xffffffffu, i1, 31);
-    double cf[4] = {0., 0., 0., 0.};
-    if (t0 | t1) {
-      // exclusive prefix over atoms: within each word by the multiply, then
-      // the second word offset by the sum of the first (all sums below 2^16)
-      const unsigned long long sum0 = (t0 * 0x0001000100010001ull) >> 48;
-      const unsigned long long b0 = t0 * 0x0001000100010000ull;
-      const unsigned long long b1 = t1 * 0x0001000100010000ull + sum0 * 0x0001000100010001ull;
-      unsigned long long p0 = b0 + (i0 - c0), p1 = b1 + (i1 - c1);
-      for (int t = 0; t < nrec; ++t) {
-        const int ia = myrec[t].y >> 24;
-        const int sft = 16 * (ia & 3);
-        int at;
-        if (ia < 4) {
-          at = (int)((p0 >> sft) & 0xffff);
-          p0 += 1ull << sft;
-        } else {
-          at = (int)((p1 >> sft) & 0xffff);
-          p1 += 1ull << sft;
-        }
-        sh.w[warp].grp[at] = myrec[t];
-      }
-      const int gb = (int)((((i < 4) ? b0 : b1) >> (16 * (i & 3))) & 0xffff);
-      const int gn = (int)((((i < 4) ? t0 : t1) >> (16 * (i & 3))) & 0xffff);
-      __syncwarp();
-      const int sub = lane >> 3;
-      if (gn > sub) {
-        const V4<double> ai64 = a.cpos64[u * 8 + i];
-        for (int t = sub; t < gn; t += 4) {
-          const int2 r = sh.w[warp].grp[gb + t];
-          const int jslot = r.x, code = r.y & 0xffffff;
-          const int o = code >> 8, k = (code & 255) - 128;
-          const ColumnOffset &co = a.coloff[o];
-          const int dzc = __float_as_int(a.ubox[2 * (jslot >> 3)].c.w) + k * a.nc2 - ci.czf;
-          close_pair64<NU>(pc, ai64, a.cpos64[jslot], co.base[0] + dzc * a.cz[0],
-                           co.base[1] + dzc * a.cz[1], co.base[2] + dzc * a.cz[2], cf[0],
-                           cf[1], cf[2], cf[3]);
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        cf[q] += __shfl_xor_sync(0xffffffffu, cf[q], 8);
-        cf[q] += __shfl_xor_sync(0xffffffffu, cf[q], 16);
-      }
-    }
-    // lane l = 8 c + i takes atom i's FP64 close sum of component c
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const double x = __shfl_sync(0xffffffffu, cf[q], i);
-      if (q == c) close = x;
-    }
-  }
-  if (i >= ci.n) return;
-  T r;
-  if (c < 3) {
-    double qi;
-    if constexpr (kMixed) qi = a.cpos64[u * 8 + i].w;
-    else qi = (double)a.cpos[u * 8 + i].w;
-    r = (T)(qi * (close - (double)vsum));
-  } else {
-    r = (T)((double)vsum + close);
-  }
-  reinterpret_cast<T *>(&a.out[ci.first + i])[c] = r;
-}
-
-template <int NU, bool SELF>
-__global__ void __launch_bounds__(kWarps * 32)
-k_pair_jl_f32(PairClusterArgs<float> a, PairConsts<float> pc) {
-  pair_jl<float, NU, SELF>(a, pc);
-}
-
-template <int NU, bool SELF>
-__global__ void __launch_bounds__(kWarps * 32)
-k_pair_jl_f64(PairClusterArgs<double> a, PairConsts<double> pc) {
-  pair_jl<double, NU, SELF>(a, pc);
+// A list atom (cluster-frame position `raw`) shifted into the frame of the
+// i-cluster ci by the FP64 shift of its cluster's frame (entry y: item code
+// and the cluster's first cell), rounded once.
+template <typename T>
+__device__ __forceinline__ V4<T> list_shifted(const PairClusterArgs<T> &a, const ClusterInfo &ci,
+                                              V4<T> raw, int y) {
+  const int o = (y >> 8) & 1023, k = (y & 255) - 128;
+  const ColumnOffset &co = a.coloff[o];
+  const int dzc = ((y >> 18) & 511) + k * a.nc2 - ci.czf;
+  raw.x += (T)(co.base[0] + dzc * a.cz[0]);
+  raw.y += (T)(co.base[1] + dzc * a.cz[1]);
+  raw.z += (T)(co.base[2] + dzc * a.cz[2]);
+  return raw;
 }
 
 // ---- adjoint short-range pass on the same sweep (mixed form) ----
@@ -1387,7 +1009,7 @@ k_adj_pair_jl(PairClusterArgs<float> a, PairConsts<float> pc, const V4<float> *_
     shead += cnt;
   };
   bool sweep = true;
-  if (a.list) {  // the forward's unit list, as in pair_jl
+  if (a.list) {  // the cluster's unit list (k_pair_list)
     const int2 cnt = a.lcnt[u];
     if (cnt.x + cnt.y <= a.lcap) {
       sweep = false;
@@ -1514,25 +1136,14 @@ void launch_nu(cudaStream_t s, const PairClusterArgs<T> &a, const PairConsts<T> 
   const int blocks = std::max(1, (a.maxcl + kWarps - 1) / kWarps);
   if constexpr (sizeof(T) == 4) {
     if (a.self_images)
-      k_pair_jl_f32<NU, true><<<blocks, kWarps * 32, 0, s>>>(a, pc);
+      k_pair_clusters_f32<NU, true><<<blocks, kWarps * 32, 0, s>>>(a, pc);
     else
-      k_pair_jl_f32<NU, false><<<blocks, kWarps * 32, 0, s>>>(a, pc);
+      k_pair_clusters_f32<NU, false><<<blocks, kWarps * 32, 0, s>>>(a, pc);
   } else {
-    // FP64 form: the tile kernel, or with MSMPB_PAIR_FP64=jl the j-lane one
-    static const bool jl = [] {
-      const char *v = std::getenv("MSMPB_PAIR_FP64");
-      return v && v[0] == 'j';
-    }();
-    if (jl) {
-      if (a.self_images)
-        k_pair_jl_f64<NU, true><<<blocks, kWarps * 32, 0, s>>>(a, pc);
-      else
-        k_pair_jl_f64<NU, false><<<blocks, kWarps * 32, 0, s>>>(a, pc);
-    } else if (a.self_images) {
+    if (a.self_images)
       k_pair_clusters_f64<NU, true><<<blocks, kWarps * 32, 0, s>>>(a, pc);
-    } else {
+    else
       k_pair_clusters_f64<NU, false><<<blocks, kWarps * 32, 0, s>>>(a, pc);
-    }
   }
 }
 

@@ -184,12 +184,12 @@ struct PairClusterArgs {
   int *err;
   int self_images;            // a lattice vector shorter than a0: an atom's
                               // own images reach its tiles and are skipped
-  // unit lists (mixed form): per i-cluster a region of lcap entries {unit,
-  // item code} of the half-cluster units that pass the box test, far ones
-  // from the front, near ones (within the close distance of the box, or of
-  // the cluster itself) from the back; lcnt = {far, near} counts, which may
-  // exceed lcap (the pair kernels then sweep that cluster's candidates
-  // themselves). Null: no lists.
+  // unit lists (the adjoint's cluster pass, mixed form): per i-cluster a
+  // region of lcap entries {unit, item code | first cell | atom mask} of the
+  // half-cluster units that pass the box test, far ones from the front, near
+  // ones (within the close distance of the box, or of the cluster itself)
+  // from the back; lcnt = {far, near} counts, which may exceed lcap (the
+  // pass then sweeps that cluster's candidates itself). Null: no lists.
   int2 *list;
   int2 *lcnt;
   int lcap;
@@ -197,7 +197,8 @@ struct PairClusterArgs {
 int cluster_capacity(int N, int ncol);
 // entries per i-cluster of the unit lists
 constexpr int kUnitListCap = 512;
-// builds the unit lists of a.list / a.lcnt (one warp per i-cluster)
+// builds the unit lists of a.list / a.lcnt (one warp per i-cluster, few
+// registers; FP32 boxes in both precisions)
 template <typename T>
 void launch_pair_list(cudaStream_t s, const PairClusterArgs<T> &a);
 // src64: FP64 cell-relative positions and charges in sorted order
