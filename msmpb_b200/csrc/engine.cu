@@ -167,12 +167,11 @@ class Plan : public FFDevice {
     if (timing) cudaEventRecord(ev_[phase], s);
   }
   bool debug_sync_ = std::getenv("MSMPB_DEBUG_SYNC") != nullptr;
-  // Pair sum: 2 = clusters (default), MSMPB_PAIR=thread selects one
-  // thread per atom, MSMPB_PAIR=cells the cell-staged kernel with
-  // compacted hits
+  // Pair sum: 2 = clusters (default); 1 = one thread per atom, the form for
+  // geometries the cluster form does not take, which MSMPB_PAIR=thread
+  // selects everywhere
   int pair_variant_ = [] {
     const char *v = std::getenv("MSMPB_PAIR");
-    if (v && v[0] == 'c') return 0;
     if (v && v[0] == 't') return 1;
     return 2;
   }();
@@ -182,11 +181,11 @@ class Plan : public FFDevice {
     const char *v = std::getenv("MSMPB_STENCIL");
     return !(v && v[0] == 'f');
   }();
-  // Anterpolation: tile scatter (default); MSMPB_ANTERP=simple selects one
-  // grid point per thread, MSMPB_ANTERP=gather the slab-staged gather
+  // Anterpolation: tile scatter (default); the slab-staged gather (the form
+  // for grids smaller than the order), which MSMPB_ANTERP=gather selects
+  // everywhere
   int anterp_variant_ = [] {
     const char *v = std::getenv("MSMPB_ANTERP");
-    if (v && v[0] == 's') return 1;
     if (v && v[0] == 'g') return 2;
     return 0;
   }();
@@ -898,9 +897,6 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
     const PairClusterArgs<T> ca = cluster_args();
     launch_pair_clusters<T>(sp, ca, pc_);
     nl += scan_launches(ncol_) + 1;
-  } else if (pair_variant_ == 0 && pair_cells_supported(noff_, N_)) {
-    launch_pair_cells<T>(sp, ncp_, psorted_, psorted64_, pstart_, geom_, off_d_,
-                         noff_, pc_, pout_, err_d_);
   } else {
     launch_pair<T>(sp, N_, psorted_, psorted64_, pcs_, pstart_, geom_, off_d_,
                    noff_, pc_, pout_);

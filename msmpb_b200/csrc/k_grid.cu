@@ -72,39 +72,6 @@ __device__ __forceinline__ T bspline_d2(const SplineConsts<T> &sc, int i, T t, T
   return v;
 }
 
-// Anterpolation as an atomic-free gather: grid point g collects from the
-// atoms of cells g + n, n in [-nu/2, nu/2)^3, in cell order (atoms within a
-// cell ordered by index), so the sum order is fixed.
-template <typename T, int NU>
-__global__ void __launch_bounds__(kThreads)
-k_anterpolate(int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
-              const int *__restrict__ start, SplineConsts<T> sc,
-              T *__restrict__ grid) {
-  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (long)M0 * M1 * M2) return;
-  const int gz = idx % M2, gy = (idx / M2) % M1, gx = idx / ((long)M1 * M2);
-  Acc<T> acc;
-  acc.zero();
-  for (int a = 0; a < NU; ++a) {
-    const int mx = pwrap(gx + a - NU / 2, M0);
-    for (int b = 0; b < NU; ++b) {
-      const int my = pwrap(gy + b - NU / 2, M1);
-      const long col = ((long)mx * M1 + my) * M2;
-      T part = T(0);
-      for (int c = 0; c < NU; ++c) {
-        const int mz = pwrap(gz + c - NU / 2, M2);
-        const int e = start[col + mz + 1];
-        for (int j = start[col + mz]; j < e; ++j) {
-          const V4<T> at = atoms[j];
-          part += at.w * bspline<T, NU>(sc, a, at.x) *
-                  bspline<T, NU>(sc, b, at.y) * bspline<T, NU>(sc, c, at.z);
-        }
-      }
-      acc.add(part);
-    }
-  }
-  grid[idx] = acc.value();
-}
 
 // Anterpolation as a slab-staged gather (the fast path).
 //
@@ -953,12 +920,6 @@ void launch_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
                              sc, scratch, nullptr)));
     MSM_NU_SWITCH(sc.nu, (k_anterp_fold<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
                              M[0], M[1], M[2], nt1, nt2, fold_tab, scratch, grid)));
-    return;
-  }
-  if (variant == 1) {  // one grid point per thread, runtime loops
-    long n = (long)M[0] * M[1] * M[2];
-    MSM_NU_SWITCH(sc.nu, (k_anterpolate<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
-                             M[0], M[1], M[2], atoms, cell_start, sc, grid)));
     return;
   }
   const AnterpTile t = anterp_tile<T>(M, sc.nu, natoms);

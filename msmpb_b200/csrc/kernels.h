@@ -134,14 +134,6 @@ void launch_pair(cudaStream_t s, int N, const V4<T> *pos_sorted,
                  const CellOffset<T> *offsets, int noff,
                  const PairConsts<T> &pc, V4<T> *out);
 
-// cell-staged form with compacted hits (k_pair_cells.cu): one CTA per cell
-bool pair_cells_supported(int noff, long natoms);
-template <typename T>
-void launch_pair_cells(cudaStream_t s, int ncell, const V4<T> *pos_sorted,
-                       const V4<double> *pos64_sorted, const int *cell_start,
-                       const Geometry &g, const CellOffset<T> *offsets, int noff,
-                       const PairConsts<T> &pc, V4<T> *out, int *err);
-
 // cluster form (k_pair_clusters.cu): clusters of 8 z-ordered atoms per
 // pair-cell column, one warp per i-cluster, 8 x 4 pair tiles
 constexpr int kMaxColumnOffsets = 1024;
@@ -224,7 +216,7 @@ void launch_adj_pair_clusters(cudaStream_t s, const PairClusterArgs<T> &a,
 // ---- grid transfers (k_grid.cu) ----
 // variant 0: tile scatter with a fold (scratch: anterp_scratch_elems
 // values; grids smaller than nu along an axis use the slab gather);
-// 1: one grid point per thread (reference form); 2: slab-staged gather
+// otherwise the slab-staged gather
 size_t anterp_scratch_elems(const int M[3], int nu);
 bool anterp_tiles_supported(const int M[3], int nu);
 // per-axis cover table of the fold (5 ints per grid index and axis)

@@ -210,16 +210,16 @@ def test_level_weights(precision):
     assert rel_rms(phi, po) < tp
 
 
-@pytest.mark.parametrize("variant", [("MSMPB_PAIR", "cells"), ("MSMPB_PAIR", "thread"),
-                                     ("MSMPB_ANTERP", "simple"), ("MSMPB_ANTERP", "gather"),
+@pytest.mark.parametrize("variant", [("MSMPB_PAIR", "thread"), ("MSMPB_ANTERP", "gather"),
                                      ("MSMPB_STENCIL", "full")])
 @pytest.mark.parametrize("case", ["spceN900_L3_M6_a8_nu8", "changaN512_L2_M8_a0.25_nu6",
                                   "CsClN16_auto"])
 def test_alternative_kernels(case, variant, monkeypatch):
-    """The alternative kernels (cell-staged pair sum with compacted hits, one
-    thread per atom for the pair sum; one thread per grid point, or the
-    slab-staged gather, for anterpolation; the unfolded level stencil) give
-    the same results as the default ones."""
+    """The fallback kernels, forced everywhere (one thread per atom for the
+    pair sum, the form for geometries the cluster form does not take; the
+    slab-staged gather for anterpolation, the form for grids smaller than the
+    order; the unfolded level stencil, the form for stencils without mirror
+    symmetry) give the same results as the default ones."""
     monkeypatch.setenv(*variant)
     d = load(case)
     for precision in ("fp64", "mixed"):
@@ -231,7 +231,7 @@ def test_alternative_kernels(case, variant, monkeypatch):
         ff.close()
 
 
-@pytest.mark.parametrize("variant", ["clusters", "cells", "thread"])
+@pytest.mark.parametrize("variant", ["clusters", "thread"])
 def test_box_smaller_than_cutoff(variant, monkeypatch):
     """Boxes with a lattice vector shorter than the cutoff: an atom's own
     periodic images lie within a0. The reference sums them once, in the
