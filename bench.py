@@ -396,6 +396,17 @@ def batch_timing(dev, torch, flush, reps=10, warmup=3, precisions=("mixed", "fp6
         out["%s_branches" % k] = b.branches()
         out["%s_kernel_launches" % k] = b.kernel_launches()
         b.close()
+        # the other form beside the chosen one: merged launches (one launch
+        # per kernel over all members) or a graph of per-member launches on
+        # 32 branches
+        other = 32 if out["%s_branches" % k] < 0 else Batch.MERGED
+        if branches == 0:
+            b = Batch(ffs[k], branches=other)
+            name = "merged" if other < 0 else "branch_graph"
+            out["%s_%s_ms" % (k, name)] = timed(lambda: b.energy_device(
+                ptr(pos), ptr(q), ptr(f), ptr(phi), e[k].data_ptr(), sh))
+            out["%s_%s_kernel_launches" % (k, name)] = b.kernel_launches()
+            b.close()
 
         def each(k=k):
             for i, x in enumerate(ffs[k]):

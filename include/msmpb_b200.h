@@ -109,15 +109,24 @@ int FF_rebuild_device(FF *ff, double edges[3][3], void *stream);
  * The batch captures every member's evaluation (the launch sequence of
  * FF_energy_device) into one graph over `branches` parallel branches, so
  * kernels of different systems run side by side on the GPU; members are
- * placed longest-first on the least-loaded branch. branches = 0 lets the
- * first FF_batch_energy_device call pick the count by timing replays of
- * candidate graphs (4, 8, 16, 32, 64 and min(n, 64)); that call synchronises
- * `stream`. At most 64 branches. Returns NULL with *status set (may be
+ * placed longest-first on the least-loaded branch. branches = -K
+ * (FF_BATCH_MERGED = -1) instead merges the members' launches: the members
+ * are dealt over K branches, and on each branch every kernel of the
+ * evaluation runs as ONE launch over all its members that need it (a table
+ * of the members' arguments and block ranges passed as the kernel's
+ * parameter), a few tens of graph nodes per branch whatever the member count
+ * (FF_batch_energy_device returns MSMPB_ERR_UNSUPPORTED if a member's
+ * evaluation has a launch that cannot be merged). branches = 0 lets the
+ * first FF_batch_energy_device call pick the form by timing replays of
+ * candidate graphs (merged on 1, 2 and 4 branches; 4, 8, 16, 32, 64 and
+ * min(n, 64) branches of per-member launches); that call synchronises
+ * `stream`. At most 64 branches either way. Returns NULL with *status set (may be
  * NULL) on an invalid list (NULL or repeated handle, mixed devices:
  * MSMPB_ERR_ARGUMENT; a handle not built: MSMPB_ERR_STATE) or a CUDA
  * failure. The handles must outlive the batch and must not be evaluated
  * while a batch replay that holds them runs. */
 typedef struct FFBatch FFBatch;
+#define FF_BATCH_MERGED (-1)
 FFBatch *FF_batch_new(FF *const *members, int n, int branches, int *status);
 
 /* Evaluates every member, asynchronously on `stream` (a cudaStream_t; NULL
@@ -135,9 +144,9 @@ int FF_batch_energy_device(FFBatch *batch, const double *const *position_d,
                            double *const *force_d, double *const *potential_d,
                            double *energy_d, void *stream);
 
-/* Branches of the current graph (after tuning: the chosen count), kernels
- * it launches, the status of the latest FF_batch_energy_device call; and
- * release. */
+/* Branches of the current graph (after tuning: the chosen count; -K for
+ * the merged form on K branches), kernel nodes it launches, the status
+ * of the latest FF_batch_energy_device call; and release. */
 int FF_batch_branches(const FFBatch *batch);
 int FF_batch_kernel_launches(const FFBatch *batch);
 int FF_batch_last_error(const FFBatch *batch);

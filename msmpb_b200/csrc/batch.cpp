@@ -8,12 +8,27 @@
 // over K parallel branches (fork and join by events during capture), so the
 // hardware scheduler runs kernels of different systems side by side and the
 // host pays one launch per step. Members go to branches longest-first onto
-// the least-loaded branch (LPT on the atom count). K is given, or picked on
-// the first call by timing replays of candidate graphs (the batch autotuner).
+// the least-loaded branch (LPT on the atom count).
+//
+// Merged form (branches = -K, FF_BATCH_MERGED = -1): every member's launch sequence is
+// recorded (launch.cuh) instead of launched, and the launches of the same
+// kernel across members become ONE launch over a table of the members'
+// arguments and block ranges (k_multi): a few tens of graph nodes for any
+// number of systems, each phase one GPU-filling launch. The members are dealt
+// over K branches of the graph whose merged chains overlap; within a branch
+// the sequences are merged per segment
+// (binning; the short-range branch, on its own graph branch; the grid
+// branch; the combine), greedily taking at each step the kernel that is next
+// for the most members. Each member's blocks compute exactly what its own
+// launch computes, so results are bit-identical to FF_energy_device.
+//
+// The form (merged, or K branches) is given, or picked on the first call by
+// timing replays of the candidates (the batch autotuner).
 // The graph is re-captured, and updated in place where its shape allows, when
 // a pointer, a weight or a member's box (FF_rebuild / FF_rebuild_device)
 // changes.
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <numeric>
@@ -40,6 +55,9 @@ struct FFBatch {
   std::vector<long> key_ver;
   int launches = 0;
   int last_error = MSMPB_OK;
+  int merge_ok = -1;  // merged form: -1 untried, 0 a member cannot be merged, 1 fine
+  std::vector<cudaStream_t> mbr;  // merged form: two streams per group
+  std::vector<cudaEvent_t> mev;
 };
 
 namespace {
@@ -133,10 +151,247 @@ int capture(FFBatch *b, int K, const Inputs &in, cudaGraph_t *graph) {
   return MSMPB_OK;
 }
 
-// Captures on K branches and installs the result as b->exec.
+// ---- merged form ----
+// One merged launch: the members (index, their record) that run its kernel
+struct Merged {
+  const msm::LaunchRec *key = nullptr;
+  size_t smem = 0;
+  long nblocks = 0;
+  std::vector<std::pair<int, const msm::LaunchRec *>> members;
+};
+
+// Greedy merge of one segment: lists[i] is member i's launch sequence. At
+// each step one kernel (same merged kernel, block shape and uniform argument)
+// runs for every member whose next launch it is, in groups of at most the
+// kernel's table capacity. Preferred are kernels that no other member still
+// needs later (so members whose sequences diverge, e.g. a three-pass scan
+// against a one-pass one, catch up and merge again), and among those the one
+// that is next for the most members.
+void merge_segment(const std::vector<std::vector<const msm::LaunchRec *>> &lists,
+                   std::vector<Merged> &out) {
+  const int n = (int)lists.size();
+  std::vector<size_t> cur(n, 0);
+  auto same = [](const msm::LaunchRec *a, const msm::LaunchRec *c) {
+    return a->kmulti == c->kmulti && a->block.x == c->block.x && a->block.y == c->block.y &&
+           a->block.z == c->block.z && a->uniform == c->uniform;
+  };
+  // ahead: some member whose next launch is another kernel needs k later
+  auto ahead = [&](const msm::LaunchRec *k) {
+    for (int j = 0; j < n; ++j) {
+      if (cur[j] >= lists[j].size() || same(lists[j][cur[j]], k)) continue;
+      for (size_t t = cur[j] + 1; t < lists[j].size(); ++t)
+        if (same(lists[j][t], k)) return true;
+    }
+    return false;
+  };
+  for (;;) {
+    const msm::LaunchRec *best = nullptr;
+    int best_count = 0;
+    bool best_ahead = true;
+    for (int i = 0; i < n; ++i) {
+      if (cur[i] >= lists[i].size()) continue;
+      const msm::LaunchRec *k = lists[i][cur[i]];
+      if (best && same(best, k)) continue;
+      int count = 0;
+      for (int j = 0; j < n; ++j)
+        if (cur[j] < lists[j].size() && same(lists[j][cur[j]], k)) ++count;
+      const bool a = ahead(k);
+      if (!best || (best_ahead && !a) || (a == best_ahead && count > best_count)) {
+        best_count = count;
+        best = k;
+        best_ahead = a;
+      }
+    }
+    if (!best) return;
+    Merged m;
+    m.key = best;
+    for (int i = 0; i < n; ++i) {
+      if (cur[i] >= lists[i].size() || !same(lists[i][cur[i]], best)) continue;
+      if ((int)m.members.size() == best->tab_max) {
+        out.push_back(std::move(m));
+        m = Merged{};
+        m.key = best;
+      }
+      const msm::LaunchRec *r = lists[i][cur[i]++];
+      m.members.emplace_back(i, r);
+      m.smem = std::max(m.smem, r->smem);
+      m.nblocks += (long)r->grid.x * r->grid.y * r->grid.z;
+    }
+    out.push_back(std::move(m));
+  }
+}
+
+// The kernel parameter of a merged launch (the ParamTab of launch.cuh)
+bool param_table(const Merged &m, std::vector<char> &buf) {
+  const msm::LaunchRec &k = *m.key;
+  buf.assign(k.tab_bytes, 0);
+  if (!k.uniform.empty()) std::memcpy(buf.data() + k.off_u, k.uniform.data(), k.uniform.size());
+  const int nm = (int)m.members.size();
+  std::memcpy(buf.data() + k.off_n, &nm, sizeof(int));
+  long acc = 0;
+  for (int j = 0; j < nm; ++j) {
+    const msm::LaunchRec *r = m.members[j].second;
+    const int f = (int)acc;
+    std::memcpy(buf.data() + k.off_first + sizeof(int) * j, &f, sizeof(int));
+    std::memcpy(buf.data() + k.off_grid + sizeof(uint3) * j, &r->grid, sizeof(uint3));
+    std::memcpy(buf.data() + k.off_packs + k.pack_stride * j, r->pack.data(), r->pack.size());
+    acc += (long)r->grid.x * r->grid.y * r->grid.z;
+  }
+  const int f = (int)acc;
+  std::memcpy(buf.data() + k.off_first + sizeof(int) * nm, &f, sizeof(int));
+  return acc <= 0x7fffffffL;
+}
+
+// Records every member, merges the four segments of each of K branches and
+// captures the merged launches into *graph. MSMPB_ERR_UNSUPPORTED: a member
+// has a launch that cannot be merged (nothing captured).
+int capture_merged(FFBatch *b, int K, const Inputs &in, cudaGraph_t *graph) {
+  const int n = (int)b->ffs.size();
+  *graph = nullptr;
+  std::vector<msm::Recorder> recs(n);
+  for (int i = 0; i < n; ++i) {
+    double w[kW];
+    const int L = std::min(b->ffs[i]->maxLevel, msm::kMaxLevels);
+    for (int l = 0; l <= L; ++l) w[l] = in.weight && in.weight[i] ? in.weight[i][l] : 1.0;
+    msm::EvalRequest r{};
+    r.pos = in.pos[i];
+    r.q = in.q[i];
+    r.host = false;
+    r.weight = w;
+    r.force = in.force ? in.force[i] : nullptr;
+    r.phi = in.phi ? in.phi[i] : nullptr;
+    r.energy_dev = in.energy ? in.energy + i : nullptr;
+    r.timing = false;
+    const int st = msm::engine_record(b->ffs[i]->dev, r, recs[i]);
+    if (st != MSMPB_OK) return st;
+    if (!recs[i].ok) return MSMPB_ERR_UNSUPPORTED;
+  }
+  if (cudaSetDevice(b->device) != cudaSuccess) return MSMPB_ERR_CUDA;
+  // Members over G = K branches of the graph, each branch's members merged:
+  // members sorted by order, precision and size, dealt round-robin, so every
+  // branch holds a like mix; the branches' latency-bound phases (small FFTs,
+  // scans) overlap other branches' compute.
+  const int G = std::max(1, std::min(K, n));
+  std::vector<int> ord(n), gof(n);
+  std::iota(ord.begin(), ord.end(), 0);
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int c) {
+    const FF *x = b->ffs[a], *y = b->ffs[c];
+    if (x->orderAcc != y->orderAcc) return x->orderAcc < y->orderAcc;
+    if (x->precision != y->precision) return x->precision < y->precision;
+    return x->N > y->N;
+  });
+  for (int t = 0; t < n; ++t) gof[ord[t]] = t % G;
+  while ((int)b->mbr.size() < 2 * G) {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return MSMPB_ERR_CUDA;
+    b->mbr.push_back(st);
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return MSMPB_ERR_CUDA;
+    b->mev.push_back(ev);
+  }
+  // segments per group: 0 binning, 1 short-range branch, 2 grid branch, 3 combine
+  std::vector<std::vector<Merged>> ms(4 * G);
+  for (int g = 0; g < G; ++g) {
+    std::vector<std::vector<const msm::LaunchRec *>> seg[4];
+    for (int i = 0; i < n; ++i) {
+      if (gof[i] != g) continue;
+      for (auto &v : seg) v.emplace_back();
+      int state = 0;
+      for (const msm::LaunchRec &r : recs[i].recs) {
+        if (r.kind == msm::LaunchRec::kFork) state = 2;
+        else if (r.kind == msm::LaunchRec::kJoin) state = 3;
+        else if (r.kind == msm::LaunchRec::kKernel)
+          seg[r.branch == 1 ? 1 : state].back().push_back(&r);
+        else return MSMPB_ERR_UNSUPPORTED;
+      }
+    }
+    for (int k = 0; k < 4; ++k) merge_segment(seg[k], ms[4 * g + k]);
+  }
+  // dynamic shared memory limits of the merged kernels
+  // (one limit per kernel: the largest of its merged launches)
+  std::vector<std::pair<const void *, size_t>> smem_max;
+  for (auto &v : ms)
+    for (const Merged &m : v) {
+      auto it = std::find_if(smem_max.begin(), smem_max.end(),
+                             [&](const std::pair<const void *, size_t> &x) {
+                               return x.first == m.key->kmulti;
+                             });
+      if (it == smem_max.end())
+        smem_max.emplace_back(m.key->kmulti, m.smem);
+      else
+        it->second = std::max(it->second, m.smem);
+    }
+  for (const auto &x : smem_max)
+    if (x.second > 48 * 1024) {
+      const cudaError_t ae = msm::multi_smem_attr(x.first, x.second);
+      if (ae != cudaSuccess) {
+        std::fprintf(stderr, "msmpb_b200: merged kernel shared memory %zu: %s\n", x.second,
+                     cudaGetErrorString(ae));
+        return MSMPB_ERR_CUDA;
+      }
+    }
+  std::vector<char> buf;
+  bool fits = true;
+  auto launch_one = [&](const Merged &m, cudaStream_t s) {
+    if (!param_table(m, buf)) fits = false;
+    void *args[] = {buf.data()};
+    const cudaError_t le = cudaLaunchKernel(m.key->kmulti, dim3((unsigned)m.nblocks),
+                                            m.key->block, args, m.smem, s);
+    if (le != cudaSuccess)
+      std::fprintf(stderr,
+                   "msmpb_b200: merged launch failed (%s): %d members, %ld blocks of %u, "
+                   "%zu bytes shared, %zu bytes of parameters\n",
+                   cudaGetErrorString(le), (int)m.members.size(), m.nblocks, m.key->block.x,
+                   m.smem, m.key->tab_bytes);
+    return le;
+  };
+  if (cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return MSMPB_ERR_CUDA;
+  cudaError_t e = cudaEventRecord(b->fork, b->cap);
+  int launches = 0;
+  for (int g = 0; g < G && e == cudaSuccess; ++g) {
+    cudaStream_t main = b->mbr[2 * g], side = b->mbr[2 * g + 1];
+    cudaEvent_t evf = b->mev[2 * g], evj = b->mev[2 * g + 1];
+    e = cudaStreamWaitEvent(main, b->fork, 0);
+    for (const Merged &m : ms[4 * g])
+      if (e == cudaSuccess) e = launch_one(m, main), ++launches;
+    const bool branch = !ms[4 * g + 1].empty();
+    if (branch && e == cudaSuccess) {
+      e = cudaEventRecord(evf, main);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(side, evf, 0);
+      for (const Merged &m : ms[4 * g + 1])
+        if (e == cudaSuccess) e = launch_one(m, side), ++launches;
+      if (e == cudaSuccess) e = cudaEventRecord(evj, side);
+    }
+    for (const Merged &m : ms[4 * g + 2])
+      if (e == cudaSuccess) e = launch_one(m, main), ++launches;
+    if (branch && e == cudaSuccess) e = cudaStreamWaitEvent(main, evj, 0);
+    for (const Merged &m : ms[4 * g + 3])
+      if (e == cudaSuccess) e = launch_one(m, main), ++launches;
+    // the group's end joins the capture stream (reusing its fork event slot)
+    if (e == cudaSuccess) e = cudaEventRecord(evf, main);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->cap, evf, 0);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(b->cap, &g);
+  if (e != cudaSuccess || ce != cudaSuccess || !fits) {
+    if (ce != cudaSuccess)
+      std::fprintf(stderr, "msmpb_b200: merged capture failed: %s\n", cudaGetErrorString(ce));
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return fits ? MSMPB_ERR_CUDA : MSMPB_ERR_UNSUPPORTED;
+  }
+  *graph = g;
+  b->launches = launches;
+  return MSMPB_OK;
+}
+
+// Captures on K branches (K < 0: the merged form on -K branches) and installs
+// the result as b->exec.
 int install(FFBatch *b, int K, const Inputs &in) {
   cudaGraph_t g;
-  int st = capture(b, K, in, &g);
+  int st = K < 0 ? capture_merged(b, -K, in, &g) : capture(b, K, in, &g);
+  if (K < 0) b->merge_ok = st == MSMPB_ERR_UNSUPPORTED ? 0 : 1;
   if (st != MSMPB_OK) return st;
   cudaError_t ie = cudaErrorUnknown;
   if (b->exec && b->branches == K) {
@@ -151,6 +406,8 @@ int install(FFBatch *b, int K, const Inputs &in) {
   }
   cudaGraphDestroy(g);
   if (ie != cudaSuccess) {
+    std::fprintf(stderr, "msmpb_b200: batch graph instantiation failed: %s\n",
+                 cudaGetErrorString(ie));
     b->exec = nullptr;
     cudaGetLastError();
     return MSMPB_ERR_CUDA;
@@ -164,7 +421,10 @@ int launch(FFBatch *b, cudaStream_t s) {
     const int st = msm::engine_begin(f->dev, s);
     if (st != MSMPB_OK) return st;
   }
-  return cudaGraphLaunch(b->exec, s) == cudaSuccess ? MSMPB_OK : MSMPB_ERR_CUDA;
+  const cudaError_t ge = cudaGraphLaunch(b->exec, s);
+  if (ge != cudaSuccess)
+    std::fprintf(stderr, "msmpb_b200: batch graph launch failed: %s\n", cudaGetErrorString(ge));
+  return ge == cudaSuccess ? MSMPB_OK : MSMPB_ERR_CUDA;
 }
 
 // The batch autotuner: replays a graph per candidate branch count on s and
@@ -172,6 +432,9 @@ int launch(FFBatch *b, cudaStream_t s) {
 int tune(FFBatch *b, const Inputs &in, cudaStream_t s) {
   const int n = (int)b->ffs.size();
   std::vector<int> cands;
+  if (b->merge_ok != 0)
+    for (int K : {1, 2, 4})
+      if (K == 1 || K < n) cands.push_back(-K);
   for (int K : {4, 8, 16, 32, 64})
     if (K < n) cands.push_back(K);
   cands.push_back(std::min(n, kMaxBranches));
@@ -185,6 +448,10 @@ int tune(FFBatch *b, const Inputs &in, cudaStream_t s) {
   float best_ms = 1e30f;
   for (int K : cands) {
     st = install(b, K, in);
+    if (K < 0 && st == MSMPB_ERR_UNSUPPORTED) {
+      st = MSMPB_OK;  // a member cannot be merged: branches only
+      continue;
+    }
     if (st != MSMPB_OK) break;
     float t[3];
     if ((st = launch(b, s)) != MSMPB_OK) break;
@@ -217,7 +484,7 @@ FFBatch *FF_batch_new(FF *const *members, int n, int branches, int *status) {
   int dummy;
   int &st = status ? *status : dummy;
   st = MSMPB_ERR_ARGUMENT;
-  if (!members || n <= 0 || branches < 0 || branches > kMaxBranches) return nullptr;
+  if (!members || n <= 0 || branches < -kMaxBranches || branches > kMaxBranches) return nullptr;
   for (int i = 0; i < n; ++i) {
     if (!members[i]) return nullptr;
     if (!members[i]->dev) {  // not built, or no device
@@ -279,7 +546,8 @@ int FF_batch_energy_device(FFBatch *b, const double *const *position_d,
   if (b->requested == 0) {
     st = tune(b, in, s);
   } else if (!b->exec || ptrs != b->key_ptrs || w != b->key_w || ver != b->key_ver) {
-    st = install(b, std::min<int>(b->requested, (int)b->ffs.size()), in);
+    const int n = (int)b->ffs.size();
+    st = install(b, b->requested < 0 ? -std::min(-b->requested, n) : std::min(b->requested, n), in);
   }
   if (st != MSMPB_OK) return fail(b, st);
   b->key_ptrs.swap(ptrs);
@@ -300,6 +568,10 @@ void FF_batch_delete(FFBatch *b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   for (cudaEvent_t e : b->join)
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : b->mev)
+    if (e) cudaEventDestroy(e);
+  for (cudaStream_t s : b->mbr)
+    if (s) cudaStreamDestroy(s);
   for (cudaStream_t s : b->br)
     if (s) cudaStreamDestroy(s);
   if (b->fork) cudaEventDestroy(b->fork);

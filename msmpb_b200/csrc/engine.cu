@@ -41,6 +41,9 @@ struct FFDevice {
   // the launch sequence of one device-pointer evaluation on s, nothing else
   // (no waits, no host work): for capture into a caller's graph
   virtual int enqueue_into(const msm::EvalRequest &r, cudaStream_t s) = 0;
+  // the same launch sequence appended to rec instead of launched (merged
+  // batches, launch.cuh)
+  virtual int record_into(const msm::EvalRequest &r, msm::Recorder &rec) = 0;
   // an evaluation issued outside this plan (a batch replay) is about to run
   // on s: order it after a pending device rebuild and count it
   virtual int begin(cudaStream_t s) = 0;
@@ -53,6 +56,39 @@ struct FFDevice {
 };
 
 namespace msm {
+
+// The recorder of merged batch launches installed on this host thread, if any
+Recorder *&tls_recorder() {
+  static thread_local Recorder *r = nullptr;
+  return r;
+}
+
+// Zeroes `words` 32-bit words at p (the recordable form of the evaluation's
+// cudaMemsetAsync calls, so that a batch can merge them)
+__device__ __forceinline__ void clear_words_body(const BlockCtx &ctx, int *p, long words) {
+  for (long i = (long)ctx.b.x * blockDim.x + threadIdx.x; i < words;
+       i += (long)ctx.g.x * blockDim.x)
+    p[i] = 0;
+}
+struct KClearWords {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) {
+    clear_words_body(c, a...);
+  }
+};
+__global__ void __launch_bounds__(256) k_clear_words(int *p, long words) {
+  clear_words_body(hw_ctx(), p, words);
+}
+
+// cudaMemsetAsync(p, 0, bytes, s); while a batch records, a clear kernel
+// (bytes are whole 32-bit words here)
+cudaError_t zero_async(void *p, size_t bytes, cudaStream_t s) {
+  if (!tls_recorder()) return cudaMemsetAsync(p, 0, bytes, s);
+  const long words = (long)(bytes / 4);
+  const int blocks = (int)std::max<long>(1, std::min<long>((words + 255) / 256, 1024));
+  launch<KClearWords, 256, 8>(s, k_clear_words, blocks, 256, 0, static_cast<int *>(p), words);
+  return cudaSuccess;
+}
 
 // Stamps for engine_version (see Plan::version_).
 long next_version() {
@@ -116,6 +152,18 @@ class Plan : public FFDevice {
   long evaluations() const override { return nevals_; }
   int enqueue_into(const EvalRequest &r, cudaStream_t s) override {
     return enqueue(r, s, r.pos, r.q, r.force, r.phi, r.energy_dev ? r.energy_dev : energy_);
+  }
+  int record_into(const EvalRequest &r, Recorder &rec) override {
+    MSM_CUDA_TRY(cudaSetDevice(device_));
+    rec.aux = aux_[0];
+    Recorder *prev = tls_recorder();
+    tls_recorder() = &rec;
+    EvalRequest rr = r;
+    rr.timing = false;
+    const int st =
+        enqueue(rr, stream_, r.pos, r.q, r.force, r.phi, r.energy_dev ? r.energy_dev : energy_);
+    tls_recorder() = prev;
+    return st;
   }
   int begin(cudaStream_t s) override {
     MSM_CUDA_TRY(cudaSetDevice(device_));
@@ -769,16 +817,21 @@ int Plan<T>::enqueue_chain(cudaStream_t s, T *const *qg, T *const *eg, const dou
                            bool tm, bool fork) {
   int nl = 0;
   fork = fork && L_ > 2 && padded2_ && part2_;
+  // a batch recording keeps the forked order of operations (so results match
+  // the replayed evaluation bit for bit) as one chain: no events
+  const bool rec = tls_recorder() != nullptr;
   if (fork) {
-    cudaStream_t b = aux_[1];
-    cudaEventRecord(fork_ev_[2], s);
-    cudaStreamWaitEvent(b, fork_ev_[2], 0);
+    cudaStream_t b = rec ? s : aux_[1];
+    if (!rec) {
+      cudaEventRecord(fork_ev_[2], s);
+      cudaStreamWaitEvent(b, fork_ev_[2], 0);
+    }
     StencilShape st = sh_[1];
     st.store = 1;
     launch_pad<T>(b, st, qg[1], padded_);
     launch_stencil<T>(b, st, tile_[1], padded_, level_taps(1),
                       stencil_tap_pitch(st.S[2], !kMixed), (T)w[1], eg[1], part_);
-    cudaEventRecord(fork_ev_[3], b);
+    if (!rec) cudaEventRecord(fork_ev_[3], b);
     nl += 1 + stencil_launches(st, tile_[1]);
   }
   mark(s, kPhaseRestrict, tm);
@@ -791,7 +844,7 @@ int Plan<T>::enqueue_chain(cudaStream_t s, T *const *qg, T *const *eg, const dou
   nl += top_solve_launches(grid_[L_]);
   for (int l = L_ - 1; l >= 1; --l) {
     if (fork && l == 1) {
-      cudaStreamWaitEvent(s, fork_ev_[3], 0);
+      if (!rec) cudaStreamWaitEvent(s, fork_ev_[3], 0);
       launch_prolong_add<T>(s, grid_[1], eg[2], eg[1], J_, nu_);
       nl += 1;
       break;
@@ -799,7 +852,7 @@ int Plan<T>::enqueue_chain(cudaStream_t s, T *const *qg, T *const *eg, const dou
     T *pad = fork ? padded2_ : padded_;
     T *part = fork ? part2_ : part_;
     mark(s, kPhaseProlong, tm && l == L_ - 1);
-    cudaMemsetAsync(eg[l], 0, (size_t)grid_[l][0] * grid_[l][1] * grid_[l][2] * sizeof(T), s);
+    zero_async(eg[l], (size_t)grid_[l][0] * grid_[l][1] * grid_[l][2] * sizeof(T), s);
     launch_prolong_add<T>(s, grid_[l], eg[l + 1], eg[l], J_, nu_);
     mark(s, kPhaseStencil, tm && l == L_ - 1);
     launch_pad<T>(s, sh_[l], qg[l], pad);
@@ -857,10 +910,9 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   for (int l = 0; l <= L_; ++l) w[l] = r.weight ? r.weight[l] : 1.0;
   mark(s, kPhaseBin, tm);
   // the four cell counters are consecutive in the arena: one clear
-  cudaMemsetAsync(pcount_, 0,
-                  reinterpret_cast<char *>(gcursor_ + ncg_ + 1) -
-                      reinterpret_cast<char *>(pcount_),
-                  s);
+  zero_async(pcount_,
+             reinterpret_cast<char *>(gcursor_ + ncg_ + 1) - reinterpret_cast<char *>(pcount_),
+             s);
   launch_prep<T>(s, N_, pos, q, geom_, pcell_, gcell_, pcount_, gcount_, prel_,
                  gfrac_, prel64_, err_d_, qparts_);
   launch_qstats_final(s, qparts_, nq_, qstats_);
@@ -878,11 +930,19 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   // short-range branch (cluster build and pair sum) runs on its own stream
   // beside the grid branch (anterpolation, grid operator, interpolation);
   // the combine waits for both. Captured, the two are branches of one graph.
+  // While a batch records, the branch is a pair of markers around the
+  // launches on aux_[0] instead of events.
   const bool fork = !tm;
+  Recorder *rec = tls_recorder();
   cudaStream_t sp = s;
   if (fork) {
-    cudaEventRecord(fork_ev_[0], s);
-    cudaStreamWaitEvent(aux_[0], fork_ev_[0], 0);
+    if (rec) {
+      rec->recs.emplace_back();
+      rec->recs.back().kind = LaunchRec::kFork;
+    } else {
+      cudaEventRecord(fork_ev_[0], s);
+      cudaStreamWaitEvent(aux_[0], fork_ev_[0], 0);
+    }
     sp = aux_[0];
   }
   if (clusters) {  // cluster build (part of the binning phase)
@@ -902,7 +962,7 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
                    noff_, pc_, pout_);
   }
   nl += 1;
-  if (fork) cudaEventRecord(fork_ev_[1], sp);
+  if (fork && !rec) cudaEventRecord(fork_ev_[1], sp);
   mark(s, kPhaseAnterp, tm);
   launch_anterpolate<T>(s, grid_[1], gsorted_, gcs_, gstart_, sc_, qg_[1],
                         anterp_variant_, err_d_, N_, anterp_scratch_, fold_tab_);
@@ -912,7 +972,14 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   launch_grid_dot<T>(s, (size_t)ncg_, qg_[1], eg_[1], grid_parts_, ngrid_);
   launch_interpolate<T>(s, N_, grid_[1], gsorted_, gcs_, eg_[1], sc_, geom_, gout_);
   nl += 2;
-  if (fork) cudaStreamWaitEvent(s, fork_ev_[1], 0);
+  if (fork) {
+    if (rec) {
+      rec->recs.emplace_back();
+      rec->recs.back().kind = LaunchRec::kJoin;
+    } else {
+      cudaStreamWaitEvent(s, fork_ev_[1], 0);
+    }
+  }
   mark(s, kPhaseCombine, tm);
   CombineArgs ca;
   ca.N = N_;
@@ -1247,6 +1314,9 @@ int engine_update_tables(FFDevice *d, const Tables &t) { return d->update(t); }
 int engine_adjoint(FFDevice *d, const AdjointRequest &r) { return d->adjoint(r); }
 int engine_enqueue(FFDevice *d, const EvalRequest &r, cudaStream_t s) {
   return d->enqueue_into(r, s);
+}
+int engine_record(FFDevice *d, const EvalRequest &r, Recorder &rec) {
+  return d->record_into(r, rec);
 }
 int engine_begin(FFDevice *d, cudaStream_t s) { return d->begin(s); }
 long engine_version(FFDevice *d) { return d->version(); }

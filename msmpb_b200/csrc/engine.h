@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include "launch_rec.h"
 #include "msm_host.h"
 
 struct FFDevice;
@@ -73,6 +74,10 @@ int engine_adjoint(FFDevice *d, const AdjointRequest &r);
 // on s after a pending device rebuild and counts it.
 int engine_enqueue(FFDevice *d, const EvalRequest &r, cudaStream_t s);
 int engine_begin(FFDevice *d, cudaStream_t s);
+// Appends the launches engine_enqueue would issue for r to rec (kernels with
+// their arguments, clears as kernels, kFork / kJoin around the short-range
+// branch); rec.ok turns false if a launch cannot be merged.
+int engine_record(FFDevice *d, const EvalRequest &r, Recorder &rec);
 long engine_version(FFDevice *d);
 int engine_device(FFDevice *d);
 long engine_evaluations(FFDevice *d);

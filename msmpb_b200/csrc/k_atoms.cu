@@ -19,13 +19,12 @@ __device__ __forceinline__ double matvec_row(const double *m, int r,
 // offset t = M s - m (code/forcefield1.c:350-357); position relative to the
 // pair cell's origin. Counts atoms per cell.
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_prep(int N, const double *__restrict__ pos, const double *__restrict__ q,
+__device__ __forceinline__ void prep_body(const BlockCtx &ctx, int N, const double *__restrict__ pos, const double *__restrict__ q,
        Geometry g, int *__restrict__ pcell, int *__restrict__ gcell,
        int *__restrict__ pcount, int *__restrict__ gcount,
        V4<T> *__restrict__ prel, V4<T> *__restrict__ gfrac,
        V4<double> *__restrict__ prel64, int *err, double *__restrict__ qparts) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int i = ctx.b.x * blockDim.x + threadIdx.x;
   // this block's sums of q and q^2 (FP64, fixed order), one pair per block
   {
     double a = 0., b = 0.;
@@ -50,8 +49,8 @@ k_prep(int N, const double *__restrict__ pos, const double *__restrict__ q,
         sa += wa[w];
         sb += wb[w];
       }
-      qparts[2 * blockIdx.x] = sa;
-      qparts[2 * blockIdx.x + 1] = sb;
+      qparts[2 * ctx.b.x] = sa;
+      qparts[2 * ctx.b.x + 1] = sb;
     }
   }
   if (i >= N) return;
@@ -109,6 +108,20 @@ k_prep(int N, const double *__restrict__ pos, const double *__restrict__ q,
   b.w = (T)qi;
   gfrac[i] = b;
 }
+template <typename T>
+struct KPrep {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { prep_body<T>(c, a...); }
+};
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_prep(int N, const double *__restrict__ pos, const double *__restrict__ q,
+       Geometry g, int *__restrict__ pcell, int *__restrict__ gcell,
+       int *__restrict__ pcount, int *__restrict__ gcount,
+       V4<T> *__restrict__ prel, V4<T> *__restrict__ gfrac,
+       V4<double> *__restrict__ prel64, int *err, double *__restrict__ qparts) {
+  prep_body<T>(hw_ctx(), N, pos, q, g, pcell, gcell, pcount, gcount, prel, gfrac, prel64, err, qparts);
+}
 
 // ---- exclusive scan (three phases) ----
 constexpr int kScanThreads = 512;
@@ -140,10 +153,9 @@ __device__ int block_exclusive_scan(int v, int *sh, int *total) {
   return before;
 }
 
-__global__ void __launch_bounds__(kScanThreads)
-k_scan_reduce(const int *__restrict__ in, int n, int *__restrict__ bsum) {
+__device__ __forceinline__ void scan_reduce_body(const BlockCtx &ctx, const int *__restrict__ in, int n, int *__restrict__ bsum) {
   __shared__ int sh[32];
-  int base = blockIdx.x * kScanTile;
+  int base = ctx.b.x * kScanTile;
   int v = 0;
   for (int k = 0; k < kScanItems; ++k) {
     int idx = base + threadIdx.x * kScanItems + k;
@@ -151,11 +163,18 @@ k_scan_reduce(const int *__restrict__ in, int n, int *__restrict__ bsum) {
   }
   int total;
   block_exclusive_scan(v, sh, &total);
-  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+  if (threadIdx.x == 0) bsum[ctx.b.x] = total;
+}
+struct KScanReduce {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { scan_reduce_body(c, a...); }
+};
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_reduce(const int *__restrict__ in, int n, int *__restrict__ bsum) {
+  scan_reduce_body(hw_ctx(), in, n, bsum);
 }
 
-__global__ void __launch_bounds__(kScanThreads)
-k_scan_top(int *bsum, int nb) {
+__device__ __forceinline__ void scan_top_body(const BlockCtx &ctx, int *bsum, int nb) {
   __shared__ int sh[32];
   int carry = 0;
   for (int base = 0; base < nb; base += kScanThreads) {
@@ -168,13 +187,20 @@ k_scan_top(int *bsum, int nb) {
   }
   if (threadIdx.x == 0) bsum[nb] = carry;
 }
+struct KScanTop {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { scan_top_body(c, a...); }
+};
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_top(int *bsum, int nb) {
+  scan_top_body(hw_ctx(), bsum, nb);
+}
 
 // Short arrays (small systems, column counts): one block walks the tiles in
 // order with a running carry, one launch instead of three.
 constexpr int kScanSingleMax = 4 * kScanTile;
 
-__global__ void __launch_bounds__(kScanThreads)
-k_scan_single(const int *__restrict__ in, int n, int *__restrict__ out) {
+__device__ __forceinline__ void scan_single_body(const BlockCtx &ctx, const int *__restrict__ in, int n, int *__restrict__ out) {
   __shared__ int sh[32];
   int carry = 0;
   for (int base = 0; base < n; base += kScanTile) {
@@ -196,12 +222,19 @@ k_scan_single(const int *__restrict__ in, int n, int *__restrict__ out) {
   }
   if (threadIdx.x == 0) out[n] = carry;
 }
-
+struct KScanSingle {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { scan_single_body(c, a...); }
+};
 __global__ void __launch_bounds__(kScanThreads)
-k_scan_apply(const int *__restrict__ in, int n, const int *__restrict__ bsum,
+k_scan_single(const int *__restrict__ in, int n, int *__restrict__ out) {
+  scan_single_body(hw_ctx(), in, n, out);
+}
+
+__device__ __forceinline__ void scan_apply_body(const BlockCtx &ctx, const int *__restrict__ in, int n, const int *__restrict__ bsum,
              int nb, int *__restrict__ out) {
   __shared__ int sh[32];
-  int base = blockIdx.x * kScanTile;
+  int base = ctx.b.x * kScanTile;
   int vals[kScanItems];
   int v = 0;
   for (int k = 0; k < kScanItems; ++k) {
@@ -209,13 +242,22 @@ k_scan_apply(const int *__restrict__ in, int n, const int *__restrict__ bsum,
     vals[k] = idx < n ? in[idx] : 0;
     v += vals[k];
   }
-  int ex = block_exclusive_scan(v, sh, nullptr) + bsum[blockIdx.x];
+  int ex = block_exclusive_scan(v, sh, nullptr) + bsum[ctx.b.x];
   for (int k = 0; k < kScanItems; ++k) {
     int idx = base + threadIdx.x * kScanItems + k;
     if (idx < n) out[idx] = ex;
     ex += vals[k];
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = bsum[nb];
+  if (ctx.b.x == 0 && threadIdx.x == 0) out[n] = bsum[nb];
+}
+struct KScanApply {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { scan_apply_body(c, a...); }
+};
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_apply(const int *__restrict__ in, int n, const int *__restrict__ bsum,
+             int nb, int *__restrict__ out) {
+  scan_apply_body(hw_ctx(), in, n, bsum, nb, out);
 }
 
 // Both cell scatters of the binning in one launch: threads [0, N) place the
@@ -227,9 +269,8 @@ struct ScatterSide {
   int *cursor, *perm;
 };
 
-__global__ void __launch_bounds__(kThreads)
-k_scatter2(int N, ScatterSide p, ScatterSide g, int ncol, int nc2, int *__restrict__ clcount) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void scatter2_body(const BlockCtx &ctx, int N, ScatterSide p, ScatterSide g, int ncol, int nc2, int *__restrict__ clcount) {
+  int i = ctx.b.x * blockDim.x + threadIdx.x;
   if (i >= 2 * N) {
     const int c = i - 2 * N;
     if (c < ncol) clcount[c] = (p.start[(c + 1) * nc2] - p.start[c * nc2] + 7) >> 3;
@@ -240,6 +281,14 @@ k_scatter2(int N, ScatterSide p, ScatterSide g, int ncol, int nc2, int *__restri
   const int c = d.cell[i];
   const int slot = d.start[c] + atomicAdd(d.cursor + c, 1);
   d.perm[slot] = i;
+}
+struct KScatter2 {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { scatter2_body(c, a...); }
+};
+__global__ void __launch_bounds__(kThreads)
+k_scatter2(int N, ScatterSide p, ScatterSide g, int ncol, int nc2, int *__restrict__ clcount) {
+  scatter2_body(hw_ctx(), N, p, g, ncol, nc2, clcount);
 }
 
 // Orders one grid cell's atoms by atom index, which makes every later
@@ -297,24 +346,34 @@ __device__ void sort_cell_by_z(int b, int e, int *__restrict__ perm,
 // Both per-cell sorts in one launch: threads [0, ncp) sort pair cells along
 // z, threads [ncp, ncp + ncg) sort grid cells by atom index.
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_sort_cells(int ncp, const int *__restrict__ pstart, int *__restrict__ pperm,
+__device__ __forceinline__ void sort_cells_body(const BlockCtx &ctx, int ncp, const int *__restrict__ pstart, int *__restrict__ pperm,
              const V4<T> *__restrict__ key, int ncg, const int *__restrict__ gstart,
              int *__restrict__ gperm) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = ctx.b.x * blockDim.x + threadIdx.x;
   if (c < ncp)
     sort_cell_by_z<T>(pstart[c], pstart[c + 1], pperm, key);
   else if (c < ncp + ncg)
     sort_cell_by_index(gstart[c - ncp], gstart[c - ncp + 1], gperm);
 }
+template <typename T>
+struct KSortCells {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { sort_cells_body<T>(c, a...); }
+};
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_sort_cells(int ncp, const int *__restrict__ pstart, int *__restrict__ pperm,
+             const V4<T> *__restrict__ key, int ncg, const int *__restrict__ gstart,
+             int *__restrict__ gperm) {
+  sort_cells_body<T>(hw_ctx(), ncp, pstart, pperm, key, ncg, gstart, gperm);
+}
 
 // Both gathers into sorted order in one launch (and the FP64 copy of the
 // pair-cell records in the mixed form): slot k takes atom perm[k].
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_gather2(int N, GatherSide<T> p, const V4<double> *__restrict__ src64,
+__device__ __forceinline__ void gather2_body(const BlockCtx &ctx, int N, GatherSide<T> p, const V4<double> *__restrict__ src64,
           V4<double> *__restrict__ dst64, GatherSide<T> g) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = ctx.b.x * blockDim.x + threadIdx.x;
   if (k >= N) return;
   int i = p.perm[k];
   p.dst[k] = p.src[i];
@@ -326,19 +385,29 @@ k_gather2(int N, GatherSide<T> p, const V4<double> *__restrict__ src64,
   g.cell_sorted[k] = g.cell[i];
   g.inv[i] = k;
 }
+template <typename T>
+struct KGather2 {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { gather2_body<T>(c, a...); }
+};
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_gather2(int N, GatherSide<T> p, const V4<double> *__restrict__ src64,
+          V4<double> *__restrict__ dst64, GatherSide<T> g) {
+  gather2_body<T>(hw_ctx(), N, p, src64, dst64, g);
+}
 
 
 // Per atom in input order: F_i = w0 F_short + q_i E_i and
 // phi_i = w0 (q_i c1 - Q c2 - q_i gamma0/a0 + phi_short) + phi_long.
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_combine(CombineArgs a, const int *__restrict__ pinv,
+__device__ __forceinline__ void combine_body(const BlockCtx &ctx, CombineArgs a, const int *__restrict__ pinv,
           const int *__restrict__ ginv, const V4<T> *__restrict__ pout,
           const V4<T> *__restrict__ gout) {
   __shared__ double red[kThreads];
   const double qsum = a.qstats[0];  // reduced by k_qstats_final
   double e = 0.;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int i = ctx.b.x * blockDim.x + threadIdx.x;
   if (i < a.N) {
     double qi = a.q[i];
     V4<T> ps = pout[pinv[i]];
@@ -360,7 +429,19 @@ k_combine(CombineArgs a, const int *__restrict__ pinv,
     if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) a.epart[blockIdx.x] = red[0];
+  if (threadIdx.x == 0) a.epart[ctx.b.x] = red[0];
+}
+template <typename T>
+struct KCombine {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { combine_body<T>(c, a...); }
+};
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_combine(CombineArgs a, const int *__restrict__ pinv,
+          const int *__restrict__ ginv, const V4<T> *__restrict__ pout,
+          const V4<T> *__restrict__ gout) {
+  combine_body<T>(hw_ctx(), a, pinv, ginv, pout, gout);
 }
 
 __device__ double block_sum(const double *v, int n, double *sh) {
@@ -377,7 +458,7 @@ __device__ double block_sum(const double *v, int n, double *sh) {
   return r;
 }
 
-__global__ void __launch_bounds__(kThreads) k_qstats_final(const double *qparts, int n,
+__device__ __forceinline__ void qstats_final_body(const BlockCtx &ctx, const double *qparts, int n,
                                                            double *qstats) {
   __shared__ double sh[kThreads];
   double a = 0., b = 0.;
@@ -404,10 +485,19 @@ __global__ void __launch_bounds__(kThreads) k_qstats_final(const double *qparts,
     qstats[1] = sh[0];
   }
 }
+struct KQstatsFinal {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { qstats_final_body(c, a...); }
+};
+__global__ void __launch_bounds__(kThreads)
+k_qstats_final(const double *qparts, int n,
+                                                           double *qstats) {
+  qstats_final_body(hw_ctx(), qparts, n, qstats);
+}
 
 // U = w0 (Q2 c1/2 - Q^2 c2/2 - Q2 gamma0/(2 a0)) + w0 sum q phi_s / 2
 //     + q^1 . e^1 / 2      (code/forcefield1.c:114-137, :195-219)
-__global__ void __launch_bounds__(kThreads) k_energy_total(EnergyArgs a) {
+__device__ __forceinline__ void energy_total_body(const BlockCtx &ctx, EnergyArgs a) {
   __shared__ double sh[kThreads];
   double qs = a.qstats[0], q2 = a.qstats[1];
   double us = block_sum(a.short_parts, a.nshort, sh);
@@ -417,6 +507,14 @@ __global__ void __launch_bounds__(kThreads) k_energy_total(EnergyArgs a) {
                 0.5 * q2 * a.gamma0_over_a0;
     a.energy[0] = a.w0 * uc + us + 0.5 * a.grid_scale * ug;
   }
+}
+struct KEnergyTotal {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { energy_total_body(c, a...); }
+};
+__global__ void __launch_bounds__(kThreads)
+k_energy_total(EnergyArgs a) {
+  energy_total_body(hw_ctx(), a);
 }
 
 inline int blocks_for(long n, int threads) {
@@ -430,15 +528,14 @@ void launch_prep(cudaStream_t s, int N, const double *pos, const double *q,
                  const Geometry &g, int *pcell, int *gcell, int *pcount,
                  int *gcount, V4<T> *prel, V4<T> *gfrac, V4<double> *prel64,
                  int *err, double *qparts) {
-  k_prep<T><<<blocks_for(N, kThreads), kThreads, 0, s>>>(
-      N, pos, q, g, pcell, gcell, pcount, gcount, prel, gfrac, prel64, err, qparts);
+  launch<KPrep<T>, kThreads, 6>(s, k_prep<T>, blocks_for(N, kThreads), kThreads, 0, N, pos, q, g, pcell, gcell, pcount, gcount, prel, gfrac, prel64, err, qparts);
 }
 
 int prep_blocks(int N) { return (int)blocks_for(N, kThreads); }
 
 void launch_qstats_final(cudaStream_t s, const double *qparts, int nqparts,
                          double *qstats) {
-  k_qstats_final<<<1, kThreads, 0, s>>>(qparts, nqparts, qstats);
+  launch<KQstatsFinal, kThreads, 1>(s, k_qstats_final, 1, kThreads, 0, qparts, nqparts, qstats);
 }
 
 size_t scan_temp_ints(int n) { return (size_t)(n / kScanTile + 2); }
@@ -447,34 +544,32 @@ int scan_launches(int n) { return n <= kScanSingleMax ? 1 : 3; }
 
 void launch_scan(cudaStream_t s, const int *in, int *out, int n, int *tmp) {
   if (n <= kScanSingleMax) {
-    k_scan_single<<<1, kScanThreads, 0, s>>>(in, n, out);
+    launch<KScanSingle, kScanThreads, 4>(s, k_scan_single, 1, kScanThreads, 0, in, n, out);
     return;
   }
   int nb = std::max(1, (n + kScanTile - 1) / kScanTile);
-  k_scan_reduce<<<nb, kScanThreads, 0, s>>>(in, n, tmp);
-  k_scan_top<<<1, kScanThreads, 0, s>>>(tmp, nb);
-  k_scan_apply<<<nb, kScanThreads, 0, s>>>(in, n, tmp, nb, out);
+  launch<KScanReduce, kScanThreads, 4>(s, k_scan_reduce, nb, kScanThreads, 0, in, n, tmp);
+  launch<KScanTop, kScanThreads, 4>(s, k_scan_top, 1, kScanThreads, 0, tmp, nb);
+  launch<KScanApply, kScanThreads, 4>(s, k_scan_apply, nb, kScanThreads, 0, in, n, tmp, nb, out);
 }
 
 void launch_bin_scatter(cudaStream_t s, int N, const int *pcell, const int *pstart,
                         int *pcursor, int *pperm, const int *gcell, const int *gstart,
                         int *gcursor, int *gperm, int ncol, int nc2, int *clcount) {
-  k_scatter2<<<blocks_for(2L * N + ncol, kThreads), kThreads, 0, s>>>(
-      N, ScatterSide{pcell, pstart, pcursor, pperm}, ScatterSide{gcell, gstart, gcursor, gperm},
+  launch<KScatter2, kThreads, 8>(s, k_scatter2, blocks_for(2L * N + ncol, kThreads), kThreads, 0, N, ScatterSide{pcell, pstart, pcursor, pperm}, ScatterSide{gcell, gstart, gcursor, gperm},
       ncol, nc2, clcount);
 }
 
 template <typename T>
 void launch_bin_sort(cudaStream_t s, int ncp, const int *pstart, int *pperm, const V4<T> *key,
                      int ncg, const int *gstart, int *gperm) {
-  k_sort_cells<T><<<blocks_for((long)ncp + ncg, kThreads), kThreads, 0, s>>>(
-      ncp, pstart, pperm, key, ncg, gstart, gperm);
+  launch<KSortCells<T>, kThreads, 8>(s, k_sort_cells<T>, blocks_for((long)ncp + ncg, kThreads), kThreads, 0, ncp, pstart, pperm, key, ncg, gstart, gperm);
 }
 
 template <typename T>
 void launch_bin_gather(cudaStream_t s, int N, const GatherSide<T> &p,
                        const V4<double> *src64, V4<double> *dst64, const GatherSide<T> &g) {
-  k_gather2<T><<<blocks_for(N, kThreads), kThreads, 0, s>>>(N, p, src64, dst64, g);
+  launch<KGather2<T>, kThreads, 8>(s, k_gather2<T>, blocks_for(N, kThreads), kThreads, 0, N, p, src64, dst64, g);
 }
 
 int combine_blocks(int N) { return blocks_for(N, kThreads); }
@@ -483,11 +578,11 @@ template <typename T>
 void launch_combine(cudaStream_t s, const CombineArgs &a, const int *pinv,
                     const int *ginv, const V4<T> *pout, const V4<T> *gout,
                     int nblocks) {
-  k_combine<T><<<nblocks, kThreads, 0, s>>>(a, pinv, ginv, pout, gout);
+  launch<KCombine<T>, kThreads, 8>(s, k_combine<T>, nblocks, kThreads, 0, a, pinv, ginv, pout, gout);
 }
 
 void launch_energy_total(cudaStream_t s, const EnergyArgs &a) {
-  k_energy_total<<<1, kThreads, 0, s>>>(a);
+  launch<KEnergyTotal, kThreads, 1>(s, k_energy_total, 1, kThreads, 0, a);
 }
 
 #define MSM_INST_ATOMS(T)                                                     \

@@ -195,15 +195,14 @@ size_t xlines_smem(int M0) { return (2 * (size_t)kXLines * M0 + M0) * sizeof(dou
 // inverse = 0: real q (this plane) -> forward z, forward y -> complex buf
 // inverse = 1: complex buf -> inverse y, inverse z -> real e (scaled)
 template <typename T>
-__global__ void __launch_bounds__(kPlaneThreads)
-k_fft_plane(FftAxis ay, FftAxis az, int inverse, const T *__restrict__ rin, double2 *buf,
+__device__ __forceinline__ void fft_plane_body(const BlockCtx &ctx, FftAxis ay, FftAxis az, int inverse, const T *__restrict__ rin, double2 *buf,
             T *__restrict__ rout, double scale) {
   extern __shared__ double2 smem[];
   const int M1 = ay.n, M2 = az.n, P = plane_pitch(M2);
   double2 *a = smem, *b = smem + M1 * P, *Wy = smem + 2 * M1 * P, *Wz = Wy + M1;
   root_table(M1, Wy);
   root_table(M2, Wz);
-  const long base = (long)blockIdx.x * M1 * M2;
+  const long base = (long)ctx.b.x * M1 * M2;
   for (int t = threadIdx.x; t < M1 * M2; t += blockDim.x) {
     const int y = t / M2, z = t % M2;
     a[y * P + z] = inverse ? buf[base + t] : make_double2((double)rin[base + t], 0.);
@@ -228,15 +227,25 @@ k_fft_plane(FftAxis ay, FftAxis az, int inverse, const T *__restrict__ rin, doub
       buf[base + t] = v;
   }
 }
+template <typename T>
+struct KFftPlane {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { fft_plane_body<T>(c, a...); }
+};
+template <typename T>
+__global__ void __launch_bounds__(kPlaneThreads)
+k_fft_plane(FftAxis ay, FftAxis az, int inverse, const T *__restrict__ rin, double2 *buf,
+            T *__restrict__ rout, double scale) {
+  fft_plane_body<T>(hw_ctx(), ay, az, inverse, rin, buf, rout, scale);
+}
 
 // Forward x, times w * khat, inverse x on kXLines adjacent x-lines
-__global__ void __launch_bounds__(kPlaneThreads)
-k_fft_xlines(FftAxis ax, int nlines, const double *__restrict__ khat, double w, double2 *buf) {
+__device__ __forceinline__ void fft_xlines_body(const BlockCtx &ctx, FftAxis ax, int nlines, const double *__restrict__ khat, double w, double2 *buf) {
   extern __shared__ double2 smem[];
   const int n = ax.n, L = kXLines;
   double2 *a = smem, *b = smem + L * n, *W = smem + 2 * L * n;
   root_table(n, W);
-  const int line0 = blockIdx.x * L;
+  const int line0 = ctx.b.x * L;
   for (int t = threadIdx.x; t < L * n; t += blockDim.x) {
     const int l = t % L, e = t / L, g = line0 + l;
     a[e * L + l] = g < nlines ? buf[(long)e * nlines + g] : make_double2(0., 0.);
@@ -256,6 +265,14 @@ k_fft_xlines(FftAxis ax, int nlines, const double *__restrict__ khat, double w, 
     const int l = t % L, e = t / L, g = line0 + l;
     if (g < nlines) buf[(long)e * nlines + g] = res[e * L + l];
   }
+}
+struct KFftXlines {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { fft_xlines_body(c, a...); }
+};
+__global__ void __launch_bounds__(kPlaneThreads)
+k_fft_xlines(FftAxis ax, int nlines, const double *__restrict__ khat, double w, double2 *buf) {
+  fft_xlines_body(hw_ctx(), ax, nlines, khat, w, buf);
 }
 
 // Larger grids: one launch per axis pass. A CTA transforms L lines of
@@ -287,15 +304,14 @@ size_t line_smem(int n, const LineShape &ls) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kPlaneThreads)
-k_fft_lines(FftAxis ax, int nlines, int inner, LineShape ls, int mode, const T *__restrict__ rin,
+__device__ __forceinline__ void fft_lines_body(const BlockCtx &ctx, FftAxis ax, int nlines, int inner, LineShape ls, int mode, const T *__restrict__ rin,
             double2 *buf, const double *__restrict__ khat, double w, T *__restrict__ rout,
             double scale) {
   extern __shared__ double2 smem[];
   const int n = ax.n, L = ls.L, LP = ls.LP;
   double2 *a = smem, *b = smem + LP * n, *W = smem + 2 * LP * n;
   root_table(n, W);
-  const int line0 = blockIdx.x * L;
+  const int line0 = ctx.b.x * L;
   const bool rows = inner == 1;
   auto gaddr = [&](int g, int e) -> long {
     return (long)(g / inner) * ((long)n * inner) + g % inner + (long)e * inner;
@@ -334,6 +350,18 @@ k_fft_lines(FftAxis ax, int nlines, int inner, LineShape ls, int mode, const T *
       buf[gi] = v;
   }
 }
+template <typename T>
+struct KFftLines {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { fft_lines_body<T>(c, a...); }
+};
+template <typename T>
+__global__ void __launch_bounds__(kPlaneThreads)
+k_fft_lines(FftAxis ax, int nlines, int inner, LineShape ls, int mode, const T *__restrict__ rin,
+            double2 *buf, const double *__restrict__ khat, double w, T *__restrict__ rout,
+            double scale) {
+  fft_lines_body<T>(hw_ctx(), ax, nlines, inner, ls, mode, rin, buf, khat, w, rout, scale);
+}
 
 template <typename T>
 void line_pass(cudaStream_t s, int n, int nlines, int inner, int mode, const T *rin,
@@ -341,7 +369,7 @@ void line_pass(cudaStream_t s, int n, int nlines, int inner, int mode, const T *
   const FftAxis ax = make_axis(n);
   const LineShape ls = line_shape(n, inner);
   const int blocks = (nlines + ls.L - 1) / ls.L;
-  k_fft_lines<T><<<blocks, kPlaneThreads, line_smem(n, ls), s>>>(ax, nlines, inner, ls, mode, rin,
+  launch<KFftLines<T>, kPlaneThreads, 2>(s, k_fft_lines<T>, blocks, kPlaneThreads, line_smem(n, ls), ax, nlines, inner, ls, mode, rin,
                                                                 buf, khat, w, rout, scale);
 }
 
@@ -398,10 +426,10 @@ void launch_top_solve(cudaStream_t s, const int M[3], const T *q,
     const FftAxis ax = make_axis(M0), ay = make_axis(M1), az = make_axis(M2);
     const size_t ps = plane_smem(M), xs = xlines_smem(M0);
     const int nl = M1 * M2;
-    k_fft_plane<T><<<M0, kPlaneThreads, ps, s>>>(ay, az, 0, q, buf0, nullptr, 0.);
-    k_fft_xlines<<<(nl + kXLines - 1) / kXLines, kPlaneThreads, xs, s>>>(ax, nl, khat, weight,
+    launch<KFftPlane<T>, kPlaneThreads, 2>(s, k_fft_plane<T>, M0, kPlaneThreads, ps, ay, az, 0, q, buf0, nullptr, 0.);
+    launch<KFftXlines, kPlaneThreads, 2>(s, k_fft_xlines, (nl + kXLines - 1) / kXLines, kPlaneThreads, xs, ax, nl, khat, weight,
                                                                          buf0);
-    k_fft_plane<T><<<M0, kPlaneThreads, ps, s>>>(ay, az, 1, nullptr, buf0, e, scale);
+    launch<KFftPlane<T>, kPlaneThreads, 2>(s, k_fft_plane<T>, M0, kPlaneThreads, ps, ay, az, 1, nullptr, buf0, e, scale);
     return;
   }
   line_pass<T>(s, M2, M0 * M1, 1, 1, q, buf0, nullptr, 0., nullptr, 0.);

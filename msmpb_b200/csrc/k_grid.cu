@@ -87,8 +87,7 @@ __device__ __forceinline__ T bspline_d2(const SplineConsts<T> &sc, int i, T t, T
 // order: no atomics, deterministic sums. Slabs whose atoms exceed the
 // staging capacity are processed in row chunks.
 template <typename T, int NU, int BX>
-__global__ void __launch_bounds__(512)
-k_anterpolate_slab(int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
+__device__ __forceinline__ void anterpolate_slab_body(const BlockCtx &ctx, int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
                    const int *__restrict__ start, SplineConsts<T> sc, int cap,
                    T *__restrict__ grid, int *err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -96,7 +95,7 @@ k_anterpolate_slab(int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
   const int tz = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * BZ + tz, nth = BZ * BY;
   const int EY = BY + NU - 1, EZ = BZ + NU - 1, ncell = EY * EZ;
-  const int x0 = blockIdx.z * BX, y0 = blockIdx.y * BY, z0 = blockIdx.x * BZ;
+  const int x0 = ctx.b.z * BX, y0 = ctx.b.y * BY, z0 = ctx.b.x * BZ;
   // shared layout: pre[ncell+1] | hz[cap] | wx[NU][cap] | wy[NU][cap] | wz[NU][cap]
   int *pre = reinterpret_cast<int *>(smem_raw);
   int *shz = pre + ((ncell + 1 + 3) & ~3);
@@ -211,6 +210,18 @@ k_anterpolate_slab(int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
     if (x < M0) grid[((long)x * M1 + y) * M2 + z] = acc[xo];
   }
 }
+template <typename T, int NU, int BX>
+struct KAnterpolateSlab {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { anterpolate_slab_body<T, NU, BX>(c, a...); }
+};
+template <typename T, int NU, int BX>
+__global__ void __launch_bounds__(512)
+k_anterpolate_slab(int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
+                   const int *__restrict__ start, SplineConsts<T> sc, int cap,
+                   T *__restrict__ grid, int *err) {
+  anterpolate_slab_body<T, NU, BX>(hw_ctx(), M0, M1, M2, atoms, start, sc, cap, grid, err);
+}
 
 // Anterpolation as a tile scatter (the default).
 //
@@ -246,8 +257,7 @@ struct TileGeom {
 // p^x Q'x Qy Qz + p^y Qx Q'y Qz + p^z Qx Qy Q'z. Weight row: P = p^x Q'x, Qx,
 // Qy, Qz, p^y Q'y, p^z Q'z (nu each).
 template <typename T, int NU, bool DIP>
-__global__ void __launch_bounds__(32)
-k_anterp_tiles(int M0, int M1, int M2, int nt1, int nt2, const V4<T> *__restrict__ atoms,
+__device__ __forceinline__ void anterp_tiles_body(const BlockCtx &ctx, int M0, int M1, int M2, int nt1, int nt2, const V4<T> *__restrict__ atoms,
                const int *__restrict__ cell, const int *__restrict__ start,
                SplineConsts<T> sc, T *__restrict__ scratch, const V4<T> *__restrict__ dip) {
   using G = TileGeom<NU>;
@@ -260,7 +270,7 @@ k_anterp_tiles(int M0, int M1, int M2, int nt1, int nt2, const V4<T> *__restrict
   __shared__ int base[32];
   __shared__ int rowbeg[64], rowoff[64];
   const int lane = threadIdx.x;
-  const int tile = blockIdx.x;
+  const int tile = ctx.b.x;
   const int tz = tile % nt2, ty = (tile / nt2) % nt1, tx = tile / (nt2 * nt1);
   const int X0 = tx * kAT, Y0 = ty * kAT, Z0 = tz * kAT;
   const int nx = min(kAT, M0 - X0), ny = min(kAT, M1 - Y0), nz = min(kAT, M2 - Z0);
@@ -414,16 +424,28 @@ k_anterp_tiles(int M0, int M1, int M2, int nt1, int nt2, const V4<T> *__restrict
   T *out = scratch + (long)tile * G::E3;
   for (int i = lane; i < G::E3; i += 32) out[i] = acc[i];
 }
+template <typename T, int NU, bool DIP>
+struct KAnterpTiles {
+  static constexpr int kUniformArg = 8;  // SplineConsts
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { anterp_tiles_body<T, NU, DIP>(c, a...); }
+};
+template <typename T, int NU, bool DIP>
+__global__ void __launch_bounds__(32)
+k_anterp_tiles(int M0, int M1, int M2, int nt1, int nt2, const V4<T> *__restrict__ atoms,
+               const int *__restrict__ cell, const int *__restrict__ start,
+               SplineConsts<T> sc, T *__restrict__ scratch, const V4<T> *__restrict__ dip) {
+  anterp_tiles_body<T, NU, DIP>(hw_ctx(), M0, M1, M2, nt1, nt2, atoms, cell, start, sc, scratch, dip);
+}
 
 // grid[p] = sum over the tiles covering p of their block value at p, in a
 // fixed order. tab (host-built, anterp_fold_table): per axis and point, the
 // count (<= 4) and the (tile, local index) covers packed as tile << 8 | local.
 template <typename T, int NU>
-__global__ void __launch_bounds__(kThreads)
-k_anterp_fold(int M0, int M1, int M2, int nt1, int nt2, const int *__restrict__ tab,
+__device__ __forceinline__ void anterp_fold_body(const BlockCtx &ctx, int M0, int M1, int M2, int nt1, int nt2, const int *__restrict__ tab,
               const T *__restrict__ scratch, T *__restrict__ grid) {
   using G = TileGeom<NU>;
-  const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long idx = (long)ctx.b.x * blockDim.x + threadIdx.x;
   if (idx >= (long)M0 * M1 * M2) return;
   const int p2 = idx % M2, p1 = (idx / M2) % M1, p0 = idx / ((long)M1 * M2);
   const int *t0 = tab + 5 * p0, *t1 = tab + 5 * (M0 + p1), *t2 = tab + 5 * (M0 + M1 + p2);
@@ -443,16 +465,26 @@ k_anterp_fold(int M0, int M1, int M2, int nt1, int nt2, const int *__restrict__ 
   }
   grid[idx] = s;
 }
+template <typename T, int NU>
+struct KAnterpFold {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { anterp_fold_body<T, NU>(c, a...); }
+};
+template <typename T, int NU>
+__global__ void __launch_bounds__(kThreads)
+k_anterp_fold(int M0, int M1, int M2, int nt1, int nt2, const int *__restrict__ tab,
+              const T *__restrict__ scratch, T *__restrict__ grid) {
+  anterp_fold_body<T, NU>(hw_ctx(), M0, M1, M2, nt1, nt2, tab, scratch, grid);
+}
 
 // Field and potential at each atom (code/forcefield1.c:570-607), separable:
 // z sums first, then y, then x. Output E in Cartesian components
 // (E = A^-T (M * grad_u)) and phi_long.
 template <typename T, int NU>
-__global__ void __launch_bounds__(kThreads)
-k_interpolate(int N, int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
+__device__ __forceinline__ void interpolate_body(const BlockCtx &ctx, int N, int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
               const int *__restrict__ cell, const T *__restrict__ grid,
               SplineConsts<T> sc, Geometry g, V4<T> *__restrict__ out) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  int k = ctx.b.x * blockDim.x + threadIdx.x;
   if (k >= N) return;
   const V4<T> at = atoms[k];
   const int c = cell[k];
@@ -503,6 +535,19 @@ k_interpolate(int N, int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
   r.z = (T)(g.Ai[2] * gxv + g.Ai[5] * gyv + g.Ai[8] * gzv);
   r.w = phi + ec;
   out[k] = r;
+}
+template <typename T, int NU>
+struct KInterpolate {
+  static constexpr int kUniformArg = 7;  // SplineConsts
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { interpolate_body<T, NU>(c, a...); }
+};
+template <typename T, int NU>
+__global__ void __launch_bounds__(kThreads)
+k_interpolate(int N, int M0, int M1, int M2, const V4<T> *__restrict__ atoms,
+              const int *__restrict__ cell, const T *__restrict__ grid,
+              SplineConsts<T> sc, Geometry g, V4<T> *__restrict__ out) {
+  interpolate_body<T, NU>(hw_ctx(), N, M0, M1, M2, atoms, cell, grid, sc, g, out);
 }
 
 // Adjoint interpolation, per atom (grid-sorted order): the value psi and
@@ -629,8 +674,7 @@ struct RestrictGeom {
 // q^{l+1}_m = sum_n J_n q^l_{2m+n}, n in [-nu/2, nu/2]^3
 // (code/forcefield1.c:401-477)
 template <typename T, int NU>
-__global__ void __launch_bounds__(kSepThreads)
-k_restrict(int F0, int F1, int F2, const T *__restrict__ fine,
+__device__ __forceinline__ void restrict_body(const BlockCtx &ctx, int F0, int F1, int F2, const T *__restrict__ fine,
            T *__restrict__ coarse, TwoScale js) {
   using Tl = RestrictTile<T>;
   using G = RestrictGeom<T, NU>;
@@ -641,7 +685,7 @@ k_restrict(int F0, int F1, int F2, const T *__restrict__ fine,
   T *t2 = reg;
   const int C0 = F0 / 2, C1 = F1 / 2, C2 = F2 / 2;
   const int nbz = (C2 + CZ - 1) / CZ, nby = (C1 + CY - 1) / CY;
-  const int bz = blockIdx.x % nbz, by = (blockIdx.x / nbz) % nby, bx = blockIdx.x / (nbz * nby);
+  const int bz = ctx.b.x % nbz, by = (ctx.b.x / nbz) % nby, bx = ctx.b.x / (nbz * nby);
   const int x0 = bx * CX, y0 = by * CY, z0 = bz * CZ;
   __shared__ int wrap[RX + RY + RZ];  // periodic indices of the region's planes, rows, columns
   T J[NU + 1];
@@ -687,6 +731,17 @@ k_restrict(int F0, int F1, int F2, const T *__restrict__ fine,
     coarse[((long)x * C1 + y) * C2 + z] = acc;
   }
 }
+template <typename T, int NU>
+struct KRestrict {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { restrict_body<T, NU>(c, a...); }
+};
+template <typename T, int NU>
+__global__ void __launch_bounds__(kSepThreads)
+k_restrict(int F0, int F1, int F2, const T *__restrict__ fine,
+           T *__restrict__ coarse, TwoScale js) {
+  restrict_body<T, NU>(hw_ctx(), F0, F1, F2, fine, coarse, js);
+}
 
 // Prolongation tile: FX x FY x FZ fine points; the coarse region along an
 // axis covers every m with |x - 2m| <= nu/2 for x in the tile
@@ -721,8 +776,7 @@ __device__ __forceinline__ int tap_coarse(int x, int k) {
 // e^l_x += sum over (m, n) with 2m + n = x (mod M) of J_n e^{l+1}_m
 // (transpose of the restriction; code/forcefield1.c:530-567)
 template <typename T, int NU>
-__global__ void __launch_bounds__(kSepThreads)
-k_prolong(int F0, int F1, int F2, const T *__restrict__ coarse,
+__device__ __forceinline__ void prolong_body(const BlockCtx &ctx, int F0, int F1, int F2, const T *__restrict__ coarse,
           T *__restrict__ fine, TwoScale js) {
   using G = ProlongGeom<NU>;
   constexpr int RX = G::RX, RY = G::RY, RZ = G::RZ, lo = G::lo;
@@ -732,7 +786,7 @@ k_prolong(int F0, int F1, int F2, const T *__restrict__ coarse,
   T *t2 = t1 + G::N_T1;
   const int C0 = F0 / 2, C1 = F1 / 2, C2 = F2 / 2;
   const int nbz = (F2 + kPZ - 1) / kPZ, nby = (F1 + kPY - 1) / kPY;
-  const int bz = blockIdx.x % nbz, by = (blockIdx.x / nbz) % nby, bx = blockIdx.x / (nbz * nby);
+  const int bz = ctx.b.x % nbz, by = (ctx.b.x / nbz) % nby, bx = ctx.b.x / (nbz * nby);
   const int x0 = bx * kPX, y0 = by * kPY, z0 = bz * kPZ;
   // coarse region origin along each axis
   const int mx0 = x0 / 2 - lo, my0 = y0 / 2 - lo, mz0 = z0 / 2 - lo;
@@ -788,6 +842,17 @@ k_prolong(int F0, int F1, int F2, const T *__restrict__ coarse,
     fine[((long)x * F1 + y) * F2 + z] += acc;
   }
 }
+template <typename T, int NU>
+struct KProlong {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { prolong_body<T, NU>(c, a...); }
+};
+template <typename T, int NU>
+__global__ void __launch_bounds__(kSepThreads)
+k_prolong(int F0, int F1, int F2, const T *__restrict__ coarse,
+          T *__restrict__ fine, TwoScale js) {
+  prolong_body<T, NU>(hw_ctx(), F0, F1, F2, coarse, fine, js);
+}
 
 template <typename T, int NU>
 constexpr int prolong_smem() {
@@ -796,13 +861,12 @@ constexpr int prolong_smem() {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_grid_dot(long n, const T *__restrict__ a, const T *__restrict__ b,
+__device__ __forceinline__ void grid_dot_body(const BlockCtx &ctx, long n, const T *__restrict__ a, const T *__restrict__ b,
            double *partials) {
   __shared__ double sh[kThreads];
   double acc = 0.;
-  for (long i = (long)blockIdx.x * kThreads + threadIdx.x; i < n;
-       i += (long)gridDim.x * kThreads)
+  for (long i = (long)ctx.b.x * kThreads + threadIdx.x; i < n;
+       i += (long)ctx.g.x * kThreads)
     acc += (double)a[i] * (double)b[i];
   sh[threadIdx.x] = acc;
   __syncthreads();
@@ -810,11 +874,30 @@ k_grid_dot(long n, const T *__restrict__ a, const T *__restrict__ b,
     if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) partials[blockIdx.x] = sh[0];
+  if (threadIdx.x == 0) partials[ctx.b.x] = sh[0];
+}
+template <typename T>
+struct KGridDot {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { grid_dot_body<T>(c, a...); }
+};
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_grid_dot(long n, const T *__restrict__ a, const T *__restrict__ b,
+           double *partials) {
+  grid_dot_body<T>(hw_ctx(), n, a, b, partials);
 }
 
 inline int blocks_for(long n) {
   return (int)std::max<long>(1, (n + kThreads - 1) / kThreads);
+}
+
+// Blocks per SM the merged launches of these kernels are compiled for: the
+// plain kernels' own occupancy at their register counts (their arguments then
+// stay in the constant bank rather than in registers)
+template <typename T, int NU>
+constexpr int interp_multi_blocks() {
+  return sizeof(T) == 4 ? (NU <= 6 ? 3 : NU == 8 ? 2 : 1) : (NU <= 6 ? 2 : 1);
 }
 
 #define MSM_NU_SWITCH(nu, CALL)     \
@@ -914,20 +997,16 @@ void launch_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
               nt2 = (M[2] + kAT - 1) / kAT;
     const int ntiles = nt0 * nt1 * nt2;
     const long n = (long)M[0] * M[1] * M[2];
-    MSM_NU_SWITCH(sc.nu, (k_anterp_tiles<T, NU, false><<<ntiles, 32,
-                                                         TileGeom<NU>::E3 * sizeof(T), s>>>(
-                             M[0], M[1], M[2], nt1, nt2, atoms, cell_sorted, cell_start,
+    MSM_NU_SWITCH(sc.nu, (launch<KAnterpTiles<T, NU, false>, 32, 1>(s, k_anterp_tiles<T, NU, false>, ntiles, 32, TileGeom<NU>::E3 * sizeof(T), M[0], M[1], M[2], nt1, nt2, atoms, cell_sorted, cell_start,
                              sc, scratch, nullptr)));
-    MSM_NU_SWITCH(sc.nu, (k_anterp_fold<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
-                             M[0], M[1], M[2], nt1, nt2, fold_tab, scratch, grid)));
+    MSM_NU_SWITCH(sc.nu, (launch<KAnterpFold<T, NU>, kThreads, 8>(s, k_anterp_fold<T, NU>, blocks_for(n), kThreads, 0, M[0], M[1], M[2], nt1, nt2, fold_tab, scratch, grid)));
     return;
   }
   const AnterpTile t = anterp_tile<T>(M, sc.nu, natoms);
   dim3 block(t.bz, t.by);
   dim3 g((M[2] + t.bz - 1) / t.bz, (M[1] + t.by - 1) / t.by,
          (M[0] + kAnterpBX - 1) / kAnterpBX);
-  MSM_NU_SWITCH(sc.nu, (k_anterpolate_slab<T, NU, kAnterpBX><<<g, block, t.smem, s>>>(
-                           M[0], M[1], M[2], atoms, cell_start, sc, t.cap, grid, err)));
+  MSM_NU_SWITCH(sc.nu, (launch<KAnterpolateSlab<T, NU, kAnterpBX>, 512, 1>(s, k_anterpolate_slab<T, NU, kAnterpBX>, g, block, t.smem, M[0], M[1], M[2], atoms, cell_start, sc, t.cap, grid, err)));
 }
 
 template <typename T>
@@ -963,12 +1042,9 @@ void launch_adj_anterpolate(cudaStream_t s, const int M[3], const V4<T> *atoms,
   const int nt0 = (M[0] + kAT - 1) / kAT, nt1 = (M[1] + kAT - 1) / kAT,
             nt2 = (M[2] + kAT - 1) / kAT;
   const long n = (long)M[0] * M[1] * M[2];
-  MSM_NU_SWITCH(sc.nu, (k_anterp_tiles<T, NU, true><<<nt0 * nt1 * nt2, 32,
-                                                      TileGeom<NU>::E3 * sizeof(T), s>>>(
-                           M[0], M[1], M[2], nt1, nt2, atoms, cell_sorted, cell_start, sc,
+  MSM_NU_SWITCH(sc.nu, (launch<KAnterpTiles<T, NU, true>, 32, 1>(s, k_anterp_tiles<T, NU, true>, nt0 * nt1 * nt2, 32, TileGeom<NU>::E3 * sizeof(T), M[0], M[1], M[2], nt1, nt2, atoms, cell_sorted, cell_start, sc,
                            scratch, dip)));
-  MSM_NU_SWITCH(sc.nu, (k_anterp_fold<T, NU><<<blocks_for(n), kThreads, 0, s>>>(
-                           M[0], M[1], M[2], nt1, nt2, fold_tab, scratch, grid)));
+  MSM_NU_SWITCH(sc.nu, (launch<KAnterpFold<T, NU>, kThreads, 8>(s, k_anterp_fold<T, NU>, blocks_for(n), kThreads, 0, M[0], M[1], M[2], nt1, nt2, fold_tab, scratch, grid)));
 }
 
 template <typename T>
@@ -986,8 +1062,7 @@ void launch_interpolate(cudaStream_t s, int N, const int M[3],
                         const V4<T> *atoms, const int *cell_sorted,
                         const T *grid, const SplineConsts<T> &sc,
                         const Geometry &g, V4<T> *out) {
-  MSM_NU_SWITCH(sc.nu, (k_interpolate<T, NU><<<blocks_for(N), kThreads, 0, s>>>(
-                           N, M[0], M[1], M[2], atoms, cell_sorted, grid, sc, g, out)));
+  MSM_NU_SWITCH(sc.nu, (launch<KInterpolate<T, NU>, kThreads, interp_multi_blocks<T, NU>()>(s, k_interpolate<T, NU>, blocks_for(N), kThreads, 0, N, M[0], M[1], M[2], atoms, cell_sorted, grid, sc, g, out)));
 }
 
 template <typename T>
@@ -999,8 +1074,7 @@ void launch_restrict(cudaStream_t s, const int Mf[3], const T *fine,
   const int C0 = Mf[0] / 2, C1 = Mf[1] / 2, C2 = Mf[2] / 2;
   const int blocks = ((C0 + Tl::CX - 1) / Tl::CX) * ((C1 + Tl::CY - 1) / Tl::CY) *
                      ((C2 + Tl::CZ - 1) / Tl::CZ);
-  MSM_NU_SWITCH(nu, (k_restrict<T, NU><<<blocks, kSepThreads, RestrictGeom<T, NU>::SMEM, s>>>(
-                        Mf[0], Mf[1], Mf[2], fine, coarse, js)));
+  MSM_NU_SWITCH(nu, (launch<KRestrict<T, NU>, kSepThreads, 1>(s, k_restrict<T, NU>, blocks, kSepThreads, RestrictGeom<T, NU>::SMEM, Mf[0], Mf[1], Mf[2], fine, coarse, js)));
 }
 
 template <typename T>
@@ -1010,8 +1084,7 @@ void launch_prolong_add(cudaStream_t s, const int Mf[3], const T *coarse,
   for (int i = 0; i <= nu; ++i) js.J[i] = J[i];
   const int blocks = ((Mf[0] + kPX - 1) / kPX) * ((Mf[1] + kPY - 1) / kPY) *
                      ((Mf[2] + kPZ - 1) / kPZ);
-  MSM_NU_SWITCH(nu, (k_prolong<T, NU><<<blocks, kSepThreads, prolong_smem<T, NU>(), s>>>(
-                        Mf[0], Mf[1], Mf[2], coarse, fine, js)));
+  MSM_NU_SWITCH(nu, (launch<KProlong<T, NU>, kSepThreads, 1>(s, k_prolong<T, NU>, blocks, kSepThreads, prolong_smem<T, NU>(), Mf[0], Mf[1], Mf[2], coarse, fine, js)));
 }
 
 int grid_dot_blocks(size_t n) {
@@ -1021,7 +1094,7 @@ int grid_dot_blocks(size_t n) {
 template <typename T>
 void launch_grid_dot(cudaStream_t s, size_t n, const T *a, const T *b,
                      double *partials, int nparts) {
-  k_grid_dot<T><<<nparts, kThreads, 0, s>>>((long)n, a, b, partials);
+  launch<KGridDot<T>, kThreads, 8>(s, k_grid_dot<T>, nparts, kThreads, 0, (long)n, a, b, partials);
 }
 
 #define MSM_INST_GRID(T)                                                       \

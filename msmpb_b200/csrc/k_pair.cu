@@ -28,12 +28,11 @@ namespace {
 constexpr int kPairThreads = 128;
 
 template <typename T, int NU, bool COMPENSATE, bool CLOSE>
-__global__ void __launch_bounds__(kPairThreads)
-k_pair(int N, const V4<T> *__restrict__ ps, const V4<double> *__restrict__ ps64,
+__device__ __forceinline__ void pair_body(const BlockCtx &ctx, int N, const V4<T> *__restrict__ ps, const V4<double> *__restrict__ ps64,
        const int *__restrict__ pcs, const int *__restrict__ start, int nc0,
        int nc1, int nc2, const CellOffset<T> *__restrict__ off, int noff,
        PairConsts<T> pc, V4<T> *__restrict__ out) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  int k = ctx.b.x * blockDim.x + threadIdx.x;
   if (k >= N) return;
   const V4<T> ai = ps[k];
   V4<double> ai64;
@@ -141,6 +140,19 @@ k_pair(int N, const V4<T> *__restrict__ ps, const V4<double> *__restrict__ ps64,
   }
   out[k] = r;
 }
+template <typename T, int NU, bool COMPENSATE, bool CLOSE>
+struct KPair {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { pair_body<T, NU, COMPENSATE, CLOSE>(c, a...); }
+};
+template <typename T, int NU, bool COMPENSATE, bool CLOSE>
+__global__ void __launch_bounds__(kPairThreads)
+k_pair(int N, const V4<T> *__restrict__ ps, const V4<double> *__restrict__ ps64,
+       const int *__restrict__ pcs, const int *__restrict__ start, int nc0,
+       int nc1, int nc2, const CellOffset<T> *__restrict__ off, int noff,
+       PairConsts<T> pc, V4<T> *__restrict__ out) {
+  pair_body<T, NU, COMPENSATE, CLOSE>(hw_ctx(), N, ps, ps64, pcs, start, nc0, nc1, nc2, off, noff, pc, out);
+}
 
 template <typename T, int NU>
 void launch_nu(cudaStream_t s, int N, const V4<T> *ps, const V4<double> *ps64,
@@ -150,8 +162,7 @@ void launch_nu(cudaStream_t s, int N, const V4<T> *ps, const V4<double> *ps64,
   int blocks = (N + kPairThreads - 1) / kPairThreads;
   if (blocks < 1) blocks = 1;
   constexpr bool kMixed = sizeof(T) == 4;
-  k_pair<T, NU, kMixed, kMixed><<<blocks, kPairThreads, 0, s>>>(
-      N, ps, ps64, pcs, start, g.nc[0], g.nc[1], g.nc[2], off, noff, pc, out);
+  launch<KPair<T, NU, kMixed, kMixed>, kPairThreads, sizeof(T) == 4 ? 6 : 8>(s, k_pair<T, NU, kMixed, kMixed>, blocks, kPairThreads, 0, N, ps, ps64, pcs, start, g.nc[0], g.nc[1], g.nc[2], off, noff, pc, out);
 }
 
 }  // namespace

@@ -50,13 +50,12 @@ __device__ __forceinline__ int floor_div(int a, int n) {
 
 // ---- cluster build: 8 threads per cluster ----
 template <typename T>
-__global__ void __launch_bounds__(256)
-k_cluster_fill(int maxcl, int ncol, int nc2, const int *__restrict__ start,
+__device__ __forceinline__ void cluster_fill_body(const BlockCtx &ctx, int maxcl, int ncol, int nc2, const int *__restrict__ start,
                const int *__restrict__ clstart, const int *__restrict__ pcs,
                const V4<double> *__restrict__ src64, double cz0, double cz1,
                double cz2, V4<T> *__restrict__ cpos, V4<double> *__restrict__ cpos64,
                ClusterInfo *__restrict__ info, UnitBox *__restrict__ ubox) {
-  const long s = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long s = (long)ctx.b.x * blockDim.x + threadIdx.x;
   const int u = (int)(s >> 3), l = (int)(s & 7);
   const int total = clstart[ncol];
   const bool valid = u < maxcl && u < total;
@@ -137,6 +136,20 @@ k_cluster_fill(int maxcl, int ncol, int nc2, const int *__restrict__ start,
                        0.5f * (hi[2] - lo[2]), 0.f);
     info[u] = ci;
   }
+}
+template <typename T>
+struct KClusterFill {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { cluster_fill_body<T>(c, a...); }
+};
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_cluster_fill(int maxcl, int ncol, int nc2, const int *__restrict__ start,
+               const int *__restrict__ clstart, const int *__restrict__ pcs,
+               const V4<double> *__restrict__ src64, double cz0, double cz1,
+               double cz2, V4<T> *__restrict__ cpos, V4<double> *__restrict__ cpos64,
+               ClusterInfo *__restrict__ info, UnitBox *__restrict__ ubox) {
+  cluster_fill_body<T>(hw_ctx(), maxcl, ncol, nc2, start, clstart, pcs, src64, cz0, cz1, cz2, cpos, cpos64, info, ubox);
 }
 
 template <typename T, int NU>
@@ -275,7 +288,7 @@ __device__ __forceinline__ void tile2(const PairConsts<float> &pc, const V4<floa
 }
 
 template <typename T, int NU, bool MIXED, bool SELF>
-__device__ __forceinline__ void pair_clusters(const PairClusterArgs<T> &a,
+__device__ __forceinline__ void pair_clusters(const BlockCtx &ctx, const PairClusterArgs<T> &a,
                                               const PairConsts<T> &pc) {
   // passing units of the current batch: their 4 atoms shifted into the
   // i-cluster's frame, the unit index and the (column, image) code
@@ -289,7 +302,7 @@ __device__ __forceinline__ void pair_clusters(const PairClusterArgs<T> &a,
   __shared__ int item_off[kWarps][32], item_u0[kWarps][32], item_code[kWarps][32];
   __shared__ int2 closeq[MIXED ? kWarps : 1][MIXED ? 32 * kCloseCap : 1];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int u = blockIdx.x * kWarps + warp;
+  const int u = ctx.b.x * kWarps + warp;
   if (u >= a.maxcl || u >= a.clstart[a.ncol]) return;  // whole warp
   const ClusterInfo ci = a.info[u];
   const int ii = lane & 7, jq = lane >> 3;
@@ -1120,15 +1133,35 @@ k_adj_pair_jl(PairClusterArgs<float> a, PairConsts<float> pc, const V4<float> *_
 // slower), FP64 targets 8 CTAs per SM (64 registers, a few spilled words,
 // faster than its unhinted 72). Both measured on the 1M-atom water box.
 template <int NU, bool SELF>
+__device__ __forceinline__ void pair_clusters_f32_body(const BlockCtx &ctx, PairClusterArgs<float> a, PairConsts<float> pc) {
+  pair_clusters<float, NU, true, SELF>(ctx, a, pc);
+}
+template <int NU, bool SELF>
+struct KPairClustersF32 {
+  static constexpr int kUniformArg = 1;  // PairConsts
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { pair_clusters_f32_body<NU, SELF>(c, a...); }
+};
+template <int NU, bool SELF>
 __global__ void __launch_bounds__(kWarps * 32)
 k_pair_clusters_f32(PairClusterArgs<float> a, PairConsts<float> pc) {
-  pair_clusters<float, NU, true, SELF>(a, pc);
+  pair_clusters_f32_body<NU, SELF>(hw_ctx(), a, pc);
 }
 
 template <int NU, bool SELF>
+__device__ __forceinline__ void pair_clusters_f64_body(const BlockCtx &ctx, PairClusterArgs<double> a, PairConsts<double> pc) {
+  pair_clusters<double, NU, false, SELF>(ctx, a, pc);
+}
+template <int NU, bool SELF>
+struct KPairClustersF64 {
+  static constexpr int kUniformArg = 1;  // PairConsts
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { pair_clusters_f64_body<NU, SELF>(c, a...); }
+};
+template <int NU, bool SELF>
 __global__ void __launch_bounds__(kWarps * 32, 8)
 k_pair_clusters_f64(PairClusterArgs<double> a, PairConsts<double> pc) {
-  pair_clusters<double, NU, false, SELF>(a, pc);
+  pair_clusters_f64_body<NU, SELF>(hw_ctx(), a, pc);
 }
 
 template <typename T, int NU>
@@ -1136,14 +1169,14 @@ void launch_nu(cudaStream_t s, const PairClusterArgs<T> &a, const PairConsts<T> 
   const int blocks = std::max(1, (a.maxcl + kWarps - 1) / kWarps);
   if constexpr (sizeof(T) == 4) {
     if (a.self_images)
-      k_pair_clusters_f32<NU, true><<<blocks, kWarps * 32, 0, s>>>(a, pc);
+      launch<KPairClustersF32<NU, true>, kWarps * 32, 7>(s, k_pair_clusters_f32<NU, true>, blocks, kWarps * 32, 0, a, pc);
     else
-      k_pair_clusters_f32<NU, false><<<blocks, kWarps * 32, 0, s>>>(a, pc);
+      launch<KPairClustersF32<NU, false>, kWarps * 32, 7>(s, k_pair_clusters_f32<NU, false>, blocks, kWarps * 32, 0, a, pc);
   } else {
     if (a.self_images)
-      k_pair_clusters_f64<NU, true><<<blocks, kWarps * 32, 0, s>>>(a, pc);
+      launch<KPairClustersF64<NU, true>, kWarps * 32, 8>(s, k_pair_clusters_f64<NU, true>, blocks, kWarps * 32, 0, a, pc);
     else
-      k_pair_clusters_f64<NU, false><<<blocks, kWarps * 32, 0, s>>>(a, pc);
+      launch<KPairClustersF64<NU, false>, kWarps * 32, 8>(s, k_pair_clusters_f64<NU, false>, blocks, kWarps * 32, 0, a, pc);
   }
 }
 
@@ -1158,7 +1191,7 @@ void launch_cluster_fill(cudaStream_t s, int maxcl, int ncol, int nc2,
                          V4<double> *cpos64, ClusterInfo *info, UnitBox *ubox) {
   const long threads = 8L * maxcl;
   const int blocks = (int)std::max<long>(1, (threads + 255) / 256);
-  k_cluster_fill<T><<<blocks, 256, 0, s>>>(maxcl, ncol, nc2, start, clstart, pcs, src64,
+  launch<KClusterFill<T>, 256, 5>(s, k_cluster_fill<T>, blocks, 256, 0, maxcl, ncol, nc2, start, clstart, pcs, src64,
                                            cz[0], cz[1], cz[2], cpos, cpos64, info, ubox);
 }
 

@@ -65,29 +65,37 @@ inline int slice_pitch(int nz, int R, int S, int V) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_pad(StencilShape sh, const T *__restrict__ q, T *__restrict__ p) {
-  // one padded row (a, b) per blockIdx.(z, y); threads along it
-  const int a = blockIdx.z, b = blockIdx.y;
+__device__ __forceinline__ void pad_body(const BlockCtx &ctx, StencilShape sh, const T *__restrict__ q, T *__restrict__ p) {
+  // one padded row (a, b) per ctx.b.(z, y); threads along it
+  const int a = ctx.b.z, b = ctx.b.y;
   const int x = pwrap(a - sh.S[0] / 2, sh.M[0]);
   const int y = pwrap(b - sh.S[1] / 2, sh.M[1]);
   const T *src = q + ((long)x * sh.M[1] + y) * sh.M[2];
   T *dst = p + ((long)a * sh.P[1] + b) * sh.P[2];
   const int h = sh.S[2] / 2, M2 = sh.M[2];
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < sh.P[2]; c += gridDim.x * blockDim.x) {
+  for (int c = ctx.b.x * blockDim.x + threadIdx.x; c < sh.P[2]; c += ctx.g.x * blockDim.x) {
     int z = c - h;
     if (z < 0 || z >= M2) z = pwrap(z, M2);
     dst[c] = src[z];
   }
 }
+template <typename T>
+struct KPad {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { pad_body<T>(c, a...); }
+};
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_pad(StencilShape sh, const T *__restrict__ q, T *__restrict__ p) {
+  pad_body<T>(hw_ctx(), sh, q, p);
+}
 
 // Reference-form sweep: one output per thread, all loops at run time.
 // Used for stencil widths beyond the templated range.
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_stencil_simple(StencilShape sh, const T *__restrict__ p,
+__device__ __forceinline__ void stencil_simple_body(const BlockCtx &ctx, StencilShape sh, const T *__restrict__ p,
                  const T *__restrict__ kh, int khz, T w, T *__restrict__ e) {
-  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long idx = (long)ctx.b.x * blockDim.x + threadIdx.x;
   const long n = (long)sh.M[0] * sh.M[1] * sh.M[2];
   if (idx >= n) return;
   const int z = idx % sh.M[2], y = (idx / sh.M[2]) % sh.M[1],
@@ -106,6 +114,17 @@ k_stencil_simple(StencilShape sh, const T *__restrict__ p,
     acc.add(pl);
   }
   e[idx] = (sh.store ? T(0) : e[idx]) + w * acc.value();
+}
+template <typename T>
+struct KStencilSimple {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { stencil_simple_body<T>(c, a...); }
+};
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_stencil_simple(StencilShape sh, const T *__restrict__ p,
+                 const T *__restrict__ kh, int khz, T w, T *__restrict__ e) {
+  stencil_simple_body<T>(hw_ctx(), sh, p, kh, khz, w, e);
 }
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
@@ -160,8 +179,7 @@ __device__ __forceinline__ void stage_taps(const T *__restrict__ kh, int plane,
 // planes i_lo+pi-TX+1 .. i_lo+pi and prefetches plane i_lo+pi+1 into the one
 // free slot, together with the next input plane.
 template <typename T, int S, int R, int TX>
-__global__ void __launch_bounds__(kThreads)
-k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
+__device__ __forceinline__ void stencil_tiled_body(const BlockCtx &ctx, StencilShape sh, const T *__restrict__ P,
                 const T *__restrict__ kh, T w, T *__restrict__ e,
                 int ntx, int chunk, T *__restrict__ part, int W) {
   constexpr int V = 16 / sizeof(T);
@@ -174,9 +192,9 @@ k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
   const int NZ = blockDim.x, TY = blockDim.y;
   const int tz = threadIdx.x, ty = threadIdx.y;
   const int S0 = sh.S[0], S1 = sh.S[1];
-  const int xt = blockIdx.z % ntx, kc = blockIdx.z / ntx;
+  const int xt = ctx.b.z % ntx, kc = ctx.b.z / ntx;
   const int i_lo = kc * chunk, i_hi = min(S0, i_lo + chunk);
-  const int z0 = blockIdx.x * NZ * R, y0 = blockIdx.y * TY, x0 = xt * TX;
+  const int z0 = ctx.b.x * NZ * R, y0 = ctx.b.y * TY, x0 = xt * TX;
   const int H = TY + S1 - 1;
   const int WC = (NZ - 1) * R + RLV;  // values a row's threads read
   const int slice_elems = H * W + V;  // +V: tail reads of the last row
@@ -276,6 +294,18 @@ k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
     }
   }
 }
+template <typename T, int S, int R, int TX>
+struct KStencilTiled {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { stencil_tiled_body<T, S, R, TX>(c, a...); }
+};
+template <typename T, int S, int R, int TX>
+__global__ void __launch_bounds__(kThreads)
+k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
+                const T *__restrict__ kh, T w, T *__restrict__ e,
+                int ntx, int chunk, T *__restrict__ part, int W) {
+  stencil_tiled_body<T, S, R, TX>(hw_ctx(), sh, P, kh, w, e, ntx, chunk, part, W);
+}
 
 // Folded sweep for stencils that are mirror-symmetric in x and y (every
 // orthorhombic box; S0, S1 odd, centres c0 = S0/2, c1 = S1/2):
@@ -291,8 +321,7 @@ k_stencil_tiled(StencilShape sh, const T *__restrict__ P,
 // i in [k chunk, min(c0+1, (k+1) chunk)), partial sums as in k_stencil_tiled.
 // kf: (c0+1) x (c1+1) rows of SP taps (zero padded).
 template <typename T, int S, int R>
-__global__ void __launch_bounds__(kThreads)
-k_stencil_fold(StencilShape sh, const T *__restrict__ P, const T *__restrict__ kf,
+__device__ __forceinline__ void stencil_fold_body(const BlockCtx &ctx, StencilShape sh, const T *__restrict__ P, const T *__restrict__ kf,
                T w, T *__restrict__ e, int chunk, T *__restrict__ part, int W) {
   constexpr int V = 16 / sizeof(T);
   constexpr int SP = (S + V - 1) / V * V;
@@ -304,9 +333,9 @@ k_stencil_fold(StencilShape sh, const T *__restrict__ P, const T *__restrict__ k
   const int tz = threadIdx.x, ty = threadIdx.y;
   const int nth = NZ * TY, tid = ty * NZ + tz;
   const int S1 = sh.S[1], c0 = sh.S[0] / 2, c1 = S1 / 2;
-  const int x = blockIdx.z % sh.M[0], kc = blockIdx.z / sh.M[0];
+  const int x = ctx.b.z % sh.M[0], kc = ctx.b.z / sh.M[0];
   const int i_lo = kc * chunk, i_hi = min(c0 + 1, i_lo + chunk);
-  const int z0 = blockIdx.x * NZ * R, y0 = blockIdx.y * TY;
+  const int z0 = ctx.b.x * NZ * R, y0 = ctx.b.y * TY;
   const int H = TY + S1 - 1;
   const int WC = (NZ - 1) * R + RLV;  // values a row's threads read
   const int slice = H * W + V;
@@ -432,17 +461,38 @@ k_stencil_fold(StencilShape sh, const T *__restrict__ P, const T *__restrict__ k
       e[row0 + z] = (sh.store ? T(0) : e[row0 + z]) + w * acc[r];
   }
 }
+template <typename T, int S, int R>
+struct KStencilFold {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { stencil_fold_body<T, S, R>(c, a...); }
+};
+template <typename T, int S, int R>
+__global__ void __launch_bounds__(kThreads)
+k_stencil_fold(StencilShape sh, const T *__restrict__ P, const T *__restrict__ kf,
+               T w, T *__restrict__ e, int chunk, T *__restrict__ part, int W) {
+  stencil_fold_body<T, S, R>(hw_ctx(), sh, P, kf, w, e, chunk, part, W);
+}
 
 // e (+)= w * sum_k part[k], chunks added in index order
 template <typename T>
-__global__ void __launch_bounds__(kThreads)
-k_split_reduce(long n, int nsplit, const T *__restrict__ part, T w,
+__device__ __forceinline__ void split_reduce_body(const BlockCtx &ctx, long n, int nsplit, const T *__restrict__ part, T w,
                T *__restrict__ e, int store) {
-  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long idx = (long)ctx.b.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
   T s = part[idx];
   for (int k = 1; k < nsplit; ++k) s += part[k * n + idx];
   e[idx] = (store ? T(0) : e[idx]) + w * s;
+}
+template <typename T>
+struct KSplitReduce {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { split_reduce_body<T>(c, a...); }
+};
+template <typename T>
+__global__ void __launch_bounds__(kThreads)
+k_split_reduce(long n, int nsplit, const T *__restrict__ part, T w,
+               T *__restrict__ e, int store) {
+  split_reduce_body<T>(hw_ctx(), n, nsplit, part, w, e, store);
 }
 
 // R: z outputs per thread; RALT: the folded sweep's alternative for widths
@@ -487,11 +537,10 @@ void launch_tiled(cudaStream_t s, const StencilShape &sh, const StencilTile &tl,
   dim3 grid((sh.M[2] + tl.nz * R - 1) / (tl.nz * R), (sh.M[1] + tl.ty - 1) / tl.ty,
             ntx * nsplit);
   (void)khz;  // the tiled kernel reads rows of the padded pitch
-  k_stencil_tiled<T, S, R, TX><<<grid, block, smem, s>>>(
-      sh, p, kh, w, e, ntx, chunk, nsplit > 1 ? part : nullptr, W);
+  launch<KStencilTiled<T, S, R, TX>, kThreads, sizeof(T) == 4 ? 2 : 1>(s, k_stencil_tiled<T, S, R, TX>, grid, block, smem, sh, p, kh, w, e, ntx, chunk, nsplit > 1 ? part : nullptr, W);
   if (nsplit > 1) {
     const long n = (long)sh.M[0] * sh.M[1] * sh.M[2];
-    k_split_reduce<T><<<blocks_for(n), kThreads, 0, s>>>(n, nsplit, part, w, e, sh.store);
+    launch<KSplitReduce<T>, kThreads, 8>(s, k_split_reduce<T>, blocks_for(n), kThreads, 0, n, nsplit, part, w, e, sh.store);
   }
 }
 
@@ -505,11 +554,10 @@ void launch_fold_r(cudaStream_t s, const StencilShape &sh, const StencilTile &tl
   dim3 block(tl.nz, tl.ty);
   dim3 grid((sh.M[2] + tl.nz * R - 1) / (tl.nz * R), (sh.M[1] + tl.ty - 1) / tl.ty,
             sh.M[0] * nsplit);
-  k_stencil_fold<T, S, R><<<grid, block, fold_smem_bytes<T>(sh, tl), s>>>(
-      sh, p, kf, w, e, chunk, nsplit > 1 ? part : nullptr, slice_pitch(tl.nz, R, S, V));
+  launch<KStencilFold<T, S, R>, kThreads, sizeof(T) == 4 ? 3 : 2>(s, k_stencil_fold<T, S, R>, grid, block, fold_smem_bytes<T>(sh, tl), sh, p, kf, w, e, chunk, nsplit > 1 ? part : nullptr, slice_pitch(tl.nz, R, S, V));
   if (nsplit > 1) {
     const long n = (long)sh.M[0] * sh.M[1] * sh.M[2];
-    k_split_reduce<T><<<blocks_for(n), kThreads, 0, s>>>(n, nsplit, part, w, e, sh.store);
+    launch<KSplitReduce<T>, kThreads, 8>(s, k_split_reduce<T>, blocks_for(n), kThreads, 0, n, nsplit, part, w, e, sh.store);
   }
 }
 
@@ -679,7 +727,7 @@ bool stencil_fold_taps(const double *kh, const int S[3], bool fp64,
 template <typename T>
 void launch_pad(cudaStream_t s, const StencilShape &sh, const T *q, T *p) {
   const dim3 grid((sh.P[2] + kThreads - 1) / kThreads, sh.P[1], sh.P[0]);
-  k_pad<T><<<grid, kThreads, 0, s>>>(sh, q, p);
+  launch<KPad<T>, kThreads, 8>(s, k_pad<T>, grid, kThreads, 0, sh, q, p);
 }
 
 template <typename T>
@@ -687,7 +735,7 @@ void launch_stencil(cudaStream_t s, const StencilShape &sh, const StencilTile &t
                     const T *p, const T *kh, int khz, T w, T *e, T *part) {
   if (!stencil_templated(sh) || tl.nz <= 0) {
     long n = (long)sh.M[0] * sh.M[1] * sh.M[2];
-    k_stencil_simple<T><<<blocks_for(n), kThreads, 0, s>>>(sh, p, kh, khz, w, e);
+    launch<KStencilSimple<T>, kThreads, 1>(s, k_stencil_simple<T>, blocks_for(n), kThreads, 0, sh, p, kh, khz, w, e);
     return;
   }
   switch (sh.S[2]) {

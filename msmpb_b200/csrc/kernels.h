@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "device.cuh"
+#include "launch.cuh"
 
 namespace msm {
 

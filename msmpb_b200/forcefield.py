@@ -243,7 +243,11 @@ class ForceField:
 class Batch:
     """Many built ForceField handles evaluated by one CUDA graph launch
     (FF_batch_new / FF_batch_energy_device). ``branches``: parallel branches
-    of the graph, 0 = tuned on the first evaluation."""
+    of the graph, -K = the members' launches merged into one launch per
+    kernel on each of K branches (``Batch.MERGED`` = -1: one branch), 0 = the
+    form tuned on the first evaluation."""
+
+    MERGED = -1  # FF_BATCH_MERGED
 
     def __init__(self, members, branches=0):
         self._lib = L.load()

@@ -75,7 +75,7 @@ def assert_same_as_single(members, e, f, phi, weights=None):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("branches", [0, 1, 3])
+@pytest.mark.parametrize("branches", [0, 1, 3, Batch.MERGED, -3])
 def test_batch_matches_members(branches):
     members = small_batch()
     b = Batch([m[3] for m in members], branches=branches)
@@ -84,9 +84,54 @@ def test_batch_matches_members(branches):
     if branches:
         assert b.branches() == branches
     else:
-        assert 1 <= b.branches() <= len(members)
-    assert b.kernel_launches() == sum(m[3].kernel_launches() for m in members)
+        assert -4 <= b.branches() <= len(members) and b.branches() != 0
+    if b.branches() < 0:
+        # one launch per kernel of each (order, precision) group's sequence
+        groups = len({(m[3].order, m[3].struct.precision) for m in members})
+        assert b.kernel_launches() <= -b.branches() * groups * max(
+            m[3].kernel_launches() for m in members)
+        assert b.kernel_launches() < sum(m[3].kernel_launches() for m in members)
+    else:
+        assert b.kernel_launches() == sum(m[3].kernel_launches() for m in members)
     assert_same_as_single(members, e, f, phi)
+    b.close()
+
+
+@pytest.mark.gpu
+def test_merged_batch_levels_and_pme():
+    """Merged launches over members of several kinds: one to four levels
+    (level stencils, transfers and the top FFT merged), both precisions and
+    a triclinic box."""
+    members = []
+    for i, (q, pos, edges, kw) in enumerate(
+            systems.ion_batch(6, seed=21, n_min=800, n_max=2500)):
+        kw = dict(kw)
+        kw["levels"] = 1 + i % 4
+        kw["top_grid"] = 6 if i % 4 else 0
+        if not kw["top_grid"]:
+            kw.pop("top_grid")
+        ff = ForceField(q, pos, edges, **kw, precision=("mixed", "fp64")[i % 2])
+        ff.set_timing(False)
+        members.append((q, pos, edges, ff))
+    q, pos, edges, kw = systems.ion_batch(1, seed=22, n_min=900, n_max=900)[0]
+    tri = edges.copy()
+    tri[0, 1] = 0.2 * edges[0, 0]
+    ff = ForceField(q, pos, tri, **kw, precision="mixed")
+    ff.set_timing(False)
+    members.append((q, pos, tri, ff))
+    b = Batch([m[3] for m in members], branches=Batch.MERGED)
+    buf = Buffers(members)
+    e, f, phi = buf.run(b)
+    assert b.branches() == Batch.MERGED
+    assert b.kernel_launches() < sum(m[3].kernel_launches() for m in members)
+    assert_same_as_single(members, e, f, phi)
+    # replays after new weights and a device box change stay bit-identical
+    weights = [[0.75] * (m[3].levels + 1) for m in members]
+    e, f, phi = buf.run(b, weights=weights)
+    assert_same_as_single(members, e, f, phi, weights)
+    members[0][3].rebuild_device(members[0][2] * 0.98, torch.cuda.current_stream().cuda_stream)
+    e, f, phi = buf.run(b, weights=weights)
+    assert_same_as_single(members, e, f, phi, weights)
     b.close()
 
 
@@ -109,9 +154,10 @@ def test_batch_against_oracle():
 
 
 @pytest.mark.gpu
-def test_batch_recaptures_on_change():
+@pytest.mark.parametrize("branches", [2, Batch.MERGED])
+def test_batch_recaptures_on_change(branches):
     members = small_batch(count=6, seed=13)
-    b = Batch([m[3] for m in members], branches=2)
+    b = Batch([m[3] for m in members], branches=branches)
     buf = Buffers(members)
     buf.run(b)
     # new output buffers: the graph is captured again
@@ -143,7 +189,7 @@ def test_batch_recaptures_after_member_engine_replaced():
     call must capture again rather than replay nodes that point into the
     freed engine."""
     members = small_batch(count=4, seed=15)
-    b = Batch([m[3] for m in members], branches=2)
+    b = Batch([m[3] for m in members], branches=Batch.MERGED)
     buf = Buffers(members)
     buf.run(b)
     members[1][3].set_precision("fp64")
@@ -172,6 +218,8 @@ def test_batch_new_argument_checks():
     ff = ForceField(q, pos, edges, order=4, cutoff=8.0)
     arr = (C.POINTER(L.FFStruct) * 1)(ff.ff)
     assert not lib.FF_batch_new(arr, 1, 65, C.byref(st))
+    assert st.value == L.ERR_ARGUMENT
+    assert not lib.FF_batch_new(arr, 1, -65, C.byref(st))
     assert st.value == L.ERR_ARGUMENT
     if not torch.cuda.is_available():  # built on the host, no device plan
         assert not lib.FF_batch_new(arr, 1, 0, C.byref(st))
