@@ -214,6 +214,45 @@ __device__ __forceinline__ void tile(const PairConsts<T> &pc, const V4<T> &ai,
   }
 }
 
+// The two packed pairs' potential and force terms: rr the squared
+// distances (replaced by a02 where the pair is masked), qj the j charges
+// (zero where masked).
+template <int NU>
+__device__ __forceinline__ void tile2_sum(const PairConsts<float> &pc, const float2 &rr,
+                                          const float2 &qj, const float2 &dx, const float2 &dy,
+                                          const float2 &dz, float2 &px, float2 &py, float2 &pz,
+                                          float2 &pp) {
+  if constexpr (NU == 0) {  // PME kernel, packed (pair_fn.cuh)
+    float2 v, f;
+    pme_radial2(pc, rr, v, f);
+    const float2 fs = __fmul2_rn(qj, f);
+    pp = __ffma2_rn(qj, v, pp);
+    px = __ffma2_rn(fs, dx, px);
+    py = __ffma2_rn(fs, dy, py);
+    pz = __ffma2_rn(fs, dz, pz);
+  } else {
+    const float2 s =
+        __ffma2_rn(rr, make_float2(pc.inv_a02, pc.inv_a02), make_float2(-1.f, -1.f));
+    float2 ts = make_float2(pc.tau[NU - 1], pc.tau[NU - 1]), t1 = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int m = NU - 2; m >= 0; --m) {
+      t1 = __ffma2_rn(s, t1, ts);
+      ts = __ffma2_rn(s, ts, make_float2(pc.tau[m], pc.tau[m]));
+    }
+    const float2 rinv = make_float2(rsqrtf(rr.x), rsqrtf(rr.y));
+    const float2 pot =
+        __fmul2_rn(qj, __ffma2_rn(ts, make_float2(-pc.inv_a0, -pc.inv_a0), rinv));
+    const float2 rinv3 = __fmul2_rn(__fmul2_rn(rinv, rinv), rinv);
+    const float2 fs = __fmul2_rn(
+        make_float2(-qj.x, -qj.y),
+        __ffma2_rn(t1, make_float2(pc.two_inv_a03, pc.two_inv_a03), rinv3));
+    pp = __fadd2_rn(pp, pot);
+    px = __ffma2_rn(fs, dx, px);
+    py = __ffma2_rn(fs, dy, py);
+    pz = __ffma2_rn(fs, dz, pz);
+  }
+}
+
 // Two tiles at once in the mixed form (queue entries e, e+1 on the two
 // halves of packed FP32 registers: fma.rn.f32x2 and friends do two FP32
 // operations per instruction, each rounded as the scalar one). X = (x_e,
@@ -234,6 +273,16 @@ __device__ __forceinline__ void tile2(const PairConsts<float> &pc, const V4<floa
   float2 r2 = __fmul2_rn(dx, dx);
   r2 = __ffma2_rn(dy, dy, r2);
   r2 = __ffma2_rn(dz, dz, r2);
+  // Warp-uniform fast path (about four steps in five on water): no lane
+  // holds a close pair (nor the atom itself, r2 = 0 < close2), so every
+  // pair is either summed here or beyond the cutoff, and out-of-range pairs
+  // are masked without per-lane branches (the same values as below).
+  if (!SELF && !__any_sync(0xffffffffu, fminf(r2.x, r2.y) < pc.close2)) {
+    const float2 rr = make_float2(fminf(r2.x, pc.a02), fminf(r2.y, pc.a02));
+    const float2 qj = make_float2(r2.x < pc.a02 ? Y.z : 0.f, r2.y < pc.a02 ? Y.w : 0.f);
+    tile2_sum<NU>(pc, rr, qj, dx, dy, dz, px, py, pz, pp);
+    return;
+  }
   bool h0 = r2.x < pc.a02, h1 = r2.y < pc.a02;
   if constexpr (SELF) {
     if (h0 && qunit[e] * 4 + jq == islot) h0 = false;
@@ -256,35 +305,7 @@ __device__ __forceinline__ void tile2(const PairConsts<float> &pc, const V4<floa
   if (!(h0 || h1)) return;
   const float2 rr = make_float2(h0 ? r2.x : pc.a02, h1 ? r2.y : pc.a02);
   const float2 qj = make_float2(h0 ? Y.z : 0.f, h1 ? Y.w : 0.f);
-  if constexpr (NU == 0) {  // PME kernel, packed (pair_fn.cuh)
-    float2 v, f;
-    pme_radial2(pc, rr, v, f);
-    const float2 fs = __fmul2_rn(qj, f);
-    pp = __ffma2_rn(qj, v, pp);
-    px = __ffma2_rn(fs, dx, px);
-    py = __ffma2_rn(fs, dy, py);
-    pz = __ffma2_rn(fs, dz, pz);
-    return;
-  } else {
-  const float2 s = __ffma2_rn(rr, make_float2(pc.inv_a02, pc.inv_a02), make_float2(-1.f, -1.f));
-  float2 ts = make_float2(pc.tau[NU - 1], pc.tau[NU - 1]), t1 = make_float2(0.f, 0.f);
-#pragma unroll
-  for (int m = NU - 2; m >= 0; --m) {
-    t1 = __ffma2_rn(s, t1, ts);
-    ts = __ffma2_rn(s, ts, make_float2(pc.tau[m], pc.tau[m]));
-  }
-  const float2 rinv = make_float2(rsqrtf(rr.x), rsqrtf(rr.y));
-  const float2 pot =
-      __fmul2_rn(qj, __ffma2_rn(ts, make_float2(-pc.inv_a0, -pc.inv_a0), rinv));
-  const float2 rinv3 = __fmul2_rn(__fmul2_rn(rinv, rinv), rinv);
-  const float2 fs = __fmul2_rn(
-      make_float2(-qj.x, -qj.y),
-      __ffma2_rn(t1, make_float2(pc.two_inv_a03, pc.two_inv_a03), rinv3));
-  pp = __fadd2_rn(pp, pot);
-  px = __ffma2_rn(fs, dx, px);
-  py = __ffma2_rn(fs, dy, py);
-  pz = __ffma2_rn(fs, dz, pz);
-  }
+  tile2_sum<NU>(pc, rr, qj, dx, dy, dz, px, py, pz, pp);
 }
 
 template <typename T, int NU, bool MIXED, bool SELF>
@@ -1128,9 +1149,9 @@ k_adj_pair_jl(PairClusterArgs<float> a, PairConsts<float> pc, const V4<float> *_
   reinterpret_cast<float *>(&out_b[ci.first + i])[c] = rb;
 }
 
-// One kernel per precision, for the register budget: FP32 keeps the
-// compiler's own choice (72 registers; an occupancy hint made the packed path
-// slower), FP64 targets 8 CTAs per SM (64 registers, a few spilled words,
+// One kernel per precision, for the register budget: FP32 targets 7 CTAs per
+// SM (72 registers; unhinted, the fast path of tile2 takes 80 and 6 CTAs, as
+// fast within noise), FP64 8 CTAs per SM (64 registers, a few spilled words,
 // faster than its unhinted 72). Both measured on the 1M-atom water box.
 template <int NU, bool SELF>
 __device__ __forceinline__ void pair_clusters_f32_body(const BlockCtx &ctx, PairClusterArgs<float> a, PairConsts<float> pc) {
@@ -1143,7 +1164,7 @@ struct KPairClustersF32 {
   static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { pair_clusters_f32_body<NU, SELF>(c, a...); }
 };
 template <int NU, bool SELF>
-__global__ void __launch_bounds__(kWarps * 32)
+__global__ void __launch_bounds__(kWarps * 32, 7)
 k_pair_clusters_f32(PairClusterArgs<float> a, PairConsts<float> pc) {
   pair_clusters_f32_body<NU, SELF>(hw_ctx(), a, pc);
 }
