@@ -82,6 +82,40 @@ def test_noalloc_stencil_matches_energy_entry_point():
     ff.close()
 
 
+def _periodic_stencil(q, k):
+    """sum_d k[d] q[(x + d - S//2) mod M] by FFT (circular cross-correlation)."""
+    M, S = q.shape, k.shape
+    K = np.zeros(M)
+    for d0 in range(S[0]):
+        for d1 in range(S[1]):
+            for d2 in range(S[2]):
+                K[(d0 - S[0] // 2) % M[0], (d1 - S[1] // 2) % M[1],
+                  (d2 - S[2] // 2) % M[2]] = k[d0, d1, d2]
+    return np.real(np.fft.ifftn(np.fft.fftn(q) * np.conj(np.fft.fftn(K))))
+
+
+# (grid, stencil): tap planes split over fewer CTAs than the default because
+# the partial sums would not fit beside the padded grid (64^3: 9 chunks cut to
+# 5), no room for partial sums at all (80^3: one chunk), and a stencil wider
+# than the templated sweeps (z width 35: the one-output-per-thread kernel)
+@pytest.mark.parametrize("M,S", [((64, 64, 64), (25, 25, 25)), ((80, 80, 80), (25, 25, 25)),
+                                 ((10, 12, 40), (3, 5, 35))])
+def test_noalloc_stencil_scratch_limits_and_wide_stencil(M, S):
+    rng = np.random.default_rng(sum(M) + sum(S))
+    q = rng.standard_normal(M)
+    k = rng.standard_normal(S)
+    e0 = rng.standard_normal(M)
+    dev = torch.device("cuda:0")
+    q_d, k_d = torch.from_numpy(q).to(dev), torch.from_numpy(k).to(dev)
+    e_d = torch.from_numpy(e0.copy()).to(dev)
+    f = _entry()
+    w = 0.625
+    assert _call(f, M, S, q_d, k_d, w, e_d) == _lib.OK
+    torch.cuda.synchronize()
+    ref = w * _periodic_stencil(q, k)
+    assert rel_rms(e_d.cpu().numpy() - e0, ref) < 1e-12
+
+
 def test_noalloc_stencil_rejects_what_does_not_fit():
     f = _entry()
     dev = torch.device("cuda:0")
