@@ -68,10 +68,45 @@ __device__ __forceinline__ double2 root(const double2 *W, int j, int sign) {
   return sign < 0 ? w : make_double2(w.x, -w.y);
 }
 
+// sign * i * b
+__device__ __forceinline__ double2 times_i(double2 b, int sign) {
+  return make_double2(-sign * b.y, sign * b.x);
+}
+
 template <int R>
 __device__ __forceinline__ void butterfly(double2 (&v)[R], double2 (&y)[R],
                                           const double2 *W, int n, int sign) {
-  if (R == 2) {
+  if constexpr (R == 3) {
+    // y_q = sum_r v_r w^(r q), w = exp(sign 2 pi i / 3) = -1/2 + sign i sqrt(3)/2
+    constexpr double kS3 = 0.86602540378443864676;  // sqrt(3) / 2
+    const double2 t = make_double2(v[1].x + v[2].x, v[1].y + v[2].y);
+    const double2 d = make_double2(kS3 * (v[1].x - v[2].x), kS3 * (v[1].y - v[2].y));
+    const double2 a = make_double2(v[0].x - 0.5 * t.x, v[0].y - 0.5 * t.y);
+    const double2 b = times_i(d, sign);
+    y[0] = make_double2(v[0].x + t.x, v[0].y + t.y);
+    y[1] = make_double2(a.x + b.x, a.y + b.y);
+    y[2] = make_double2(a.x - b.x, a.y - b.y);
+  } else if constexpr (R == 5) {
+    // w^k = cos(2 pi k / 5) + sign i sin(2 pi k / 5); pairs k, 5 - k share the
+    // cosine and differ in the sign of the sine
+    constexpr double kC1 = 0.30901699437494742410;   // cos(2 pi / 5) = (sqrt 5 - 1) / 4
+    constexpr double kC2 = -0.80901699437494742410;  // cos(4 pi / 5) = -(sqrt 5 + 1) / 4
+    constexpr double kS1 = 0.95105651629515357212;   // sin(2 pi / 5)
+    constexpr double kS2 = 0.58778525229247312917;   // sin(4 pi / 5)
+    const double2 t1 = make_double2(v[1].x + v[4].x, v[1].y + v[4].y);
+    const double2 t2 = make_double2(v[2].x + v[3].x, v[2].y + v[3].y);
+    const double2 t3 = make_double2(v[1].x - v[4].x, v[1].y - v[4].y);
+    const double2 t4 = make_double2(v[2].x - v[3].x, v[2].y - v[3].y);
+    const double2 a1 = make_double2(v[0].x + kC1 * t1.x + kC2 * t2.x, v[0].y + kC1 * t1.y + kC2 * t2.y);
+    const double2 a2 = make_double2(v[0].x + kC2 * t1.x + kC1 * t2.x, v[0].y + kC2 * t1.y + kC1 * t2.y);
+    const double2 b1 = times_i(make_double2(kS1 * t3.x + kS2 * t4.x, kS1 * t3.y + kS2 * t4.y), sign);
+    const double2 b2 = times_i(make_double2(kS2 * t3.x - kS1 * t4.x, kS2 * t3.y - kS1 * t4.y), sign);
+    y[0] = make_double2(v[0].x + t1.x + t2.x, v[0].y + t1.y + t2.y);
+    y[1] = make_double2(a1.x + b1.x, a1.y + b1.y);
+    y[4] = make_double2(a1.x - b1.x, a1.y - b1.y);
+    y[2] = make_double2(a2.x + b2.x, a2.y + b2.y);
+    y[3] = make_double2(a2.x - b2.x, a2.y - b2.y);
+  } else if constexpr (R == 2) {
     y[0] = make_double2(v[0].x + v[1].x, v[0].y + v[1].y);
     y[1] = make_double2(v[0].x - v[1].x, v[0].y - v[1].y);
   } else if (R == 4) {
@@ -100,6 +135,28 @@ __device__ __forceinline__ void butterfly(double2 (&v)[R], double2 (&y)[R],
   }
 }
 
+// q = n / d and r = n % d for 0 <= n < 2^24 and d >= 1, from rd = the
+// correctly rounded single-precision 1/d: the product n rd is within one of
+// n / d, so one correction step either way makes it exact (checked for every
+// d < 4097 and a sample up to 2^16 against integer division)
+struct DivD {
+  int d;
+  float rd;
+};
+__device__ __forceinline__ DivD divisor(int d) { return DivD{d, __frcp_rn((float)d)}; }
+__device__ __forceinline__ int divmod(int n, const DivD &D, int &r) {
+  int q = __float2int_rz(__int2float_rn(n) * D.rd);
+  r = n - q * D.d;
+  if (r < 0) {
+    --q;
+    r += D.d;
+  } else if (r >= D.d) {
+    ++q;
+    r -= D.d;
+  }
+  return q;
+}
+
 // One Stockham stage of radix R on nl lines held in shared memory; element e
 // of line l sits at l * ls + e * es in src and dst. line_fast: consecutive
 // threads take consecutive lines (lines adjacent in memory), else
@@ -108,20 +165,25 @@ template <int R>
 __device__ void stage_r(int n, int Ns, int nl, int ls, int es, bool line_fast, int sign,
                         const double2 *W, const double2 *src, double2 *dst) {
   const int m = n / R, ts = n / (Ns * R);
+  const DivD dl = divisor(line_fast ? nl : m), dn = divisor(Ns);
   for (int t = threadIdx.x; t < nl * m; t += blockDim.x) {
-    const int line = line_fast ? t % nl : t / m;
-    const int j = line_fast ? t / nl : t % m;
-    const int k = j % Ns;
+    int rem;
+    const int quo = divmod(t, dl, rem);
+    const int line = line_fast ? rem : quo;
+    const int j = line_fast ? quo : rem;
+    int k;
+    const int jq = divmod(j, dn, k);
     const double2 *s = src + line * ls;
     double2 v[R], y[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const double2 a = s[(j + r * m) * es];
-      v[r] = r == 0 ? a : cmul(a, root(W, (k * r * ts) % n, sign));
+      // k r ts < Ns R ts = n: no wrap
+      v[r] = r == 0 ? a : cmul(a, root(W, k * r * ts, sign));
     }
     butterfly<R>(v, y, W, n, sign);
     double2 *d = dst + line * ls;
-    const int base = (j / Ns) * Ns * R + k;
+    const int base = jq * Ns * R + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) d[(base + r * Ns) * es] = y[r];
   }
@@ -203,8 +265,11 @@ __device__ __forceinline__ void fft_plane_body(const BlockCtx &ctx, FftAxis ay, 
   root_table(M1, Wy);
   root_table(M2, Wz);
   const long base = (long)ctx.b.x * M1 * M2;
+  const DivD d2 = divisor(M2);
+#pragma unroll 4
   for (int t = threadIdx.x; t < M1 * M2; t += blockDim.x) {
-    const int y = t / M2, z = t % M2;
+    int z;
+    const int y = divmod(t, d2, z);
     a[y * P + z] = inverse ? buf[base + t] : make_double2((double)rin[base + t], 0.);
   }
   __syncthreads();
@@ -219,7 +284,8 @@ __device__ __forceinline__ void fft_plane_body(const BlockCtx &ctx, FftAxis ay, 
     res = axis_fft(az, M1, P, 1, false, +1, Wz, res, o);
   }
   for (int t = threadIdx.x; t < M1 * M2; t += blockDim.x) {
-    const int y = t / M2, z = t % M2;
+    int z;
+    const int y = divmod(t, d2, z);
     const double2 v = res[y * P + z];
     if (inverse)
       rout[base + t] = (T)(v.x * scale);
@@ -246,12 +312,14 @@ __device__ __forceinline__ void fft_xlines_body(const BlockCtx &ctx, FftAxis ax,
   double2 *a = smem, *b = smem + L * n, *W = smem + 2 * L * n;
   root_table(n, W);
   const int line0 = ctx.b.x * L;
+#pragma unroll 4
   for (int t = threadIdx.x; t < L * n; t += blockDim.x) {
     const int l = t % L, e = t / L, g = line0 + l;
     a[e * L + l] = g < nlines ? buf[(long)e * nlines + g] : make_double2(0., 0.);
   }
   __syncthreads();
   double2 *res = axis_fft(ax, L, 1, L, true, -1, W, a, b);
+#pragma unroll 4
   for (int t = threadIdx.x; t < L * n; t += blockDim.x) {
     const int l = t % L, e = t / L, g = line0 + l;
     const double kv = g < nlines ? w * khat[(long)e * nlines + g] : 0.;
