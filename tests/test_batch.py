@@ -154,6 +154,31 @@ def test_batch_against_oracle():
 
 
 @pytest.mark.gpu
+def test_merged_batch_fallback_kernels(monkeypatch):
+    """The forms chosen for geometries the default kernels do not take (one
+    thread per atom for the pair sum, the slab-staged anterpolation, the
+    unfolded level stencils), forced everywhere, through merged launches:
+    bit-identical to each member's own evaluation."""
+    for var, val in (("MSMPB_PAIR", "thread"), ("MSMPB_ANTERP", "gather"),
+                     ("MSMPB_STENCIL", "full")):
+        monkeypatch.setenv(var, val)
+    members = []
+    for i, (q, pos, edges, kw) in enumerate(
+            systems.ion_batch(4, seed=23, n_min=800, n_max=2000)):
+        kw = dict(kw, levels=1 + i % 3)
+        if i % 3:
+            kw["top_grid"] = 6
+        ff = ForceField(q, pos, edges, **kw, precision=("mixed", "fp64")[i % 2])
+        ff.set_timing(False)
+        members.append((q, pos, edges, ff))
+    b = Batch([m[3] for m in members], branches=Batch.MERGED)
+    e, f, phi = Buffers(members).run(b)
+    assert b.branches() == Batch.MERGED
+    assert_same_as_single(members, e, f, phi)
+    b.close()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("branches", [2, Batch.MERGED])
 def test_batch_recaptures_on_change(branches):
     members = small_batch(count=6, seed=13)
