@@ -184,14 +184,19 @@ void merge_segment(const std::vector<std::vector<const msm::LaunchRec *>> &lists
     }
     return false;
   };
+  std::vector<const msm::LaunchRec *> seen;  // candidate kernels of this step
   for (;;) {
     const msm::LaunchRec *best = nullptr;
     int best_count = 0;
     bool best_ahead = true;
+    seen.clear();
     for (int i = 0; i < n; ++i) {
       if (cur[i] >= lists[i].size()) continue;
       const msm::LaunchRec *k = lists[i][cur[i]];
-      if (best && same(best, k)) continue;
+      if (std::any_of(seen.begin(), seen.end(),
+                      [&](const msm::LaunchRec *x) { return same(x, k); }))
+        continue;
+      seen.push_back(k);
       int count = 0;
       for (int j = 0; j < n; ++j)
         if (cur[j] < lists[j].size() && same(lists[j][cur[j]], k)) ++count;
