@@ -465,7 +465,7 @@ int Plan<T>::init(const Tables &t, int device) {
   a.want(&gcursor_, (ncg_ + 1) * sizeof(int));
   a.want(&pstart_, (ncp_ + 1) * sizeof(int));
   a.want(&gstart_, (ncg_ + 1) * sizeof(int));
-  a.want(&scan_tmp_, std::max(scan_temp_ints(ncp_), scan_temp_ints(ncg_)) * sizeof(int));
+  a.want(&scan_tmp_, (scan_temp_ints(ncp_) + scan_temp_ints(ncg_)) * sizeof(int));
   for (V4<T> **b : {&prel_, &gfrac_, &psorted_, &gsorted_, &pout_, &gout_})
     a.want(b, n * sizeof(V4<T>));
   if (kMixed) {
@@ -916,8 +916,7 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   launch_prep<T>(s, N_, pos, q, geom_, pcell_, gcell_, pcount_, gcount_, prel_,
                  gfrac_, prel64_, err_d_, qparts_);
   launch_qstats_final(s, qparts_, nq_, qstats_);
-  launch_scan(s, pcount_, pstart_, ncp_, scan_tmp_);
-  launch_scan(s, gcount_, gstart_, ncg_, scan_tmp_);
+  launch_scan2(s, pcount_, pstart_, ncp_, gcount_, gstart_, ncg_, scan_tmp_);
   const bool clusters = pair_variant_ == 2 && clusters_ok_;
   launch_bin_scatter(s, N_, pcell_, pstart_, pcursor_, pperm_, gcell_, gstart_, gcursor_,
                      gperm_, clusters ? ncol_ : 0, geom_.nc[2], clcount_);
@@ -925,7 +924,7 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
   launch_bin_gather<T>(s, N_, GatherSide<T>{pperm_, prel_, pcell_, psorted_, pcs_, pinv_},
                        kMixed ? prel64_ : nullptr, kMixed ? psorted64_ : nullptr,
                        GatherSide<T>{gperm_, gfrac_, gcell_, gsorted_, gcs_, ginv_});
-  nl += 2 + scan_launches(ncp_) + scan_launches(ncg_) + 3;
+  nl += 2 + scan2_launches(ncp_, ncg_) + 3;
   // Forked form (all but the eagerly timed evaluation): after binning the
   // short-range branch (cluster build and pair sum) runs on its own stream
   // beside the grid branch (anterpolation, grid operator, interpolation);

@@ -260,6 +260,67 @@ k_scan_apply(const int *__restrict__ in, int n, const int *__restrict__ bsum,
   scan_apply_body(hw_ctx(), in, n, bsum, nb, out);
 }
 
+// Both scans of the binning (pair-cell counts, grid-cell counts) in the
+// same launches: the blocks of one launch take the first array's tiles,
+// then the second's (each block computes what its launch for one array
+// would). Integer sums, so the result does not depend on the split.
+struct ScanArray {
+  const int *in;
+  int n;
+  int *out;
+  int *tmp;  // block sums (nb + 1)
+  int nb;    // blocks of the three-pass scan
+};
+__device__ __forceinline__ BlockCtx second(const BlockCtx &ctx, int nb0) {
+  BlockCtx c = ctx;
+  c.b.x -= nb0;
+  return c;
+}
+__device__ __forceinline__ void scan_reduce2_body(const BlockCtx &ctx, ScanArray a, ScanArray b) {
+  if ((int)ctx.b.x < a.nb) scan_reduce_body(ctx, a.in, a.n, a.tmp);
+  else scan_reduce_body(second(ctx, a.nb), b.in, b.n, b.tmp);
+}
+struct KScanReduce2 {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { scan_reduce2_body(c, a...); }
+};
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce2(ScanArray a, ScanArray b) {
+  scan_reduce2_body(hw_ctx(), a, b);
+}
+__device__ __forceinline__ void scan_top2_body(const BlockCtx &ctx, ScanArray a, ScanArray b) {
+  if (ctx.b.x == 0) scan_top_body(ctx, a.tmp, a.nb);
+  else scan_top_body(second(ctx, 1), b.tmp, b.nb);
+}
+struct KScanTop2 {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { scan_top2_body(c, a...); }
+};
+__global__ void __launch_bounds__(kScanThreads) k_scan_top2(ScanArray a, ScanArray b) {
+  scan_top2_body(hw_ctx(), a, b);
+}
+__device__ __forceinline__ void scan_apply2_body(const BlockCtx &ctx, ScanArray a, ScanArray b) {
+  if ((int)ctx.b.x < a.nb) scan_apply_body(ctx, a.in, a.n, a.tmp, a.nb, a.out);
+  else scan_apply_body(second(ctx, a.nb), b.in, b.n, b.tmp, b.nb, b.out);
+}
+struct KScanApply2 {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { scan_apply2_body(c, a...); }
+};
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply2(ScanArray a, ScanArray b) {
+  scan_apply2_body(hw_ctx(), a, b);
+}
+__device__ __forceinline__ void scan_single2_body(const BlockCtx &ctx, ScanArray a, ScanArray b) {
+  if (ctx.b.x == 0) scan_single_body(ctx, a.in, a.n, a.out);
+  else scan_single_body(second(ctx, 1), b.in, b.n, b.out);
+}
+struct KScanSingle2 {
+  template <typename... A>
+  static __device__ __forceinline__ void run(const BlockCtx &c, const A &...a) { scan_single2_body(c, a...); }
+};
+__global__ void __launch_bounds__(kScanThreads) k_scan_single2(ScanArray a, ScanArray b) {
+  scan_single2_body(hw_ctx(), a, b);
+}
+
 // Both cell scatters of the binning in one launch: threads [0, N) place the
 // atoms into pair cells, threads [N, 2N) into grid cells, and threads
 // [2N, 2N + ncol) count each pair-cell column's clusters of 8 atoms (for the
@@ -551,6 +612,23 @@ void launch_scan(cudaStream_t s, const int *in, int *out, int n, int *tmp) {
   launch<KScanReduce, kScanThreads, 4>(s, k_scan_reduce, nb, kScanThreads, 0, in, n, tmp);
   launch<KScanTop, kScanThreads, 4>(s, k_scan_top, 1, kScanThreads, 0, tmp, nb);
   launch<KScanApply, kScanThreads, 4>(s, k_scan_apply, nb, kScanThreads, 0, in, n, tmp, nb, out);
+}
+
+int scan2_launches(int n0, int n1) {
+  return (n0 <= kScanSingleMax && n1 <= kScanSingleMax) ? 1 : 3;
+}
+
+void launch_scan2(cudaStream_t s, const int *in0, int *out0, int n0, const int *in1, int *out1,
+                  int n1, int *tmp) {
+  ScanArray a{in0, n0, out0, tmp, std::max(1, (n0 + kScanTile - 1) / kScanTile)};
+  ScanArray b{in1, n1, out1, tmp + a.nb + 1, std::max(1, (n1 + kScanTile - 1) / kScanTile)};
+  if (scan2_launches(n0, n1) == 1) {
+    launch<KScanSingle2, kScanThreads, 4>(s, k_scan_single2, 2, kScanThreads, 0, a, b);
+    return;
+  }
+  launch<KScanReduce2, kScanThreads, 4>(s, k_scan_reduce2, a.nb + b.nb, kScanThreads, 0, a, b);
+  launch<KScanTop2, kScanThreads, 4>(s, k_scan_top2, 2, kScanThreads, 0, a, b);
+  launch<KScanApply2, kScanThreads, 4>(s, k_scan_apply2, a.nb + b.nb, kScanThreads, 0, a, b);
 }
 
 void launch_bin_scatter(cudaStream_t s, int N, const int *pcell, const int *pstart,

@@ -70,6 +70,11 @@ int prep_blocks(int N);
 size_t scan_temp_ints(int n);
 void launch_scan(cudaStream_t s, const int *in, int *out, int n, int *tmp);
 int scan_launches(int n);  // kernels one launch_scan of n entries issues
+// two independent scans in the same launches (in0 -> out0, in1 -> out1);
+// tmp: scan_temp_ints(n0) + scan_temp_ints(n1) ints
+void launch_scan2(cudaStream_t s, const int *in0, int *out0, int n0, const int *in1, int *out1,
+                  int n1, int *tmp);
+int scan2_launches(int n0, int n1);
 // Binning after the scans, one launch each: both cell scatters (pair cells,
 // grid cells; with ncol > 0 also each pair-cell column's cluster count,
 // ceil(atoms / 8), into clcount); both per-cell sorts (pair cells by key[atom].z, ties by atom
