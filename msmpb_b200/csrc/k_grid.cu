@@ -513,11 +513,24 @@ __device__ __forceinline__ void interpolate_body(const BlockCtx &ctx, int N, int
       const int gy = pwrap(my - (b - NU / 2), M1);
       const T *row = grid + ((long)gx * M1 + gy) * M2;
       T s0 = 0, s1 = 0;
+      if constexpr (sizeof(T) == 4) {
+        // the value and derivative sums as one packed FP32 multiply-add per
+        // grid value (each half rounded as the scalar one)
+        float2 s = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int i = 0; i < NU; ++i) {
-        const T e = row[zi[i]] - ec;
-        s0 += wz[i] * e;
-        s1 += dz[i] * e;
+        for (int i = 0; i < NU; ++i) {
+          const float e = row[zi[i]] - ec;
+          s = __ffma2_rn(make_float2(wz[i], dz[i]), make_float2(e, e), s);
+        }
+        s0 = s.x;
+        s1 = s.y;
+      } else {
+#pragma unroll
+        for (int i = 0; i < NU; ++i) {
+          const T e = row[zi[i]] - ec;
+          s0 += wz[i] * e;
+          s1 += dz[i] * e;
+        }
       }
       t00 += wy[b] * s0;
       t10 += dy[b] * s0;
