@@ -310,6 +310,128 @@ def adjoint_timing(ff, pos_d, q_d, f_d, phi_d, e_d, torch, flush, forward_ms, re
     return out
 
 
+def adjoint_water3000(dev, torch, flush, reps=20, warmup=3):
+    """The force-matching gradient of a 3,000-atom water box (1,000 rigid
+    waters, 31.04 A, nu=6, a0=9 A, automatic grid): loss sum |F - F_tgt|^2
+    with F_tgt the forces under the charges perturbed by N(0, 0.01^2) (seed 4).
+    Times the forward (graph replay) and FF_adjoint_device with
+    fbar = 2 (F - F_tgt), ubar = 0, reusing the forward's state and with the
+    forward recomputed; CUDA events on the stream, L2 flushed before each
+    timed launch, medians."""
+    from msmpb_b200 import systems
+    from msmpb_b200.forcefield import ForceField
+    q, pos, edges, kw = systems.config("water3000")
+    n = len(q)
+    rng = np.random.default_rng(4)
+    q_tgt = q + rng.normal(0.0, 0.01, n)
+    sh = torch.cuda.current_stream().cuda_stream
+    ff = ForceField(q, pos, edges, **kw, precision="mixed", device=dev.index)
+    ff.set_timing(False)
+    pos_d = torch.from_numpy(pos).to(dev)
+    q_d = torch.from_numpy(q).to(dev)
+    qt_d = torch.from_numpy(q_tgt).to(dev)
+    f_d = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    ft_d = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    phi_d = torch.zeros(n, dtype=torch.float64, device=dev)
+    e_d = torch.zeros(1, dtype=torch.float64, device=dev)
+    dq = torch.empty(n, dtype=torch.float64, device=dev)
+    dr = torch.empty((n, 3), dtype=torch.float64, device=dev)
+
+    def fwd(qp, fp):
+        ff.energy_device(pos_d.data_ptr(), qp.data_ptr(), fp.data_ptr(), phi_d.data_ptr(),
+                         e_d.data_ptr(), sh)
+    fwd(qt_d, ft_d)
+    fwd(q_d, f_d)
+    fbar = 2.0 * (f_d - ft_d)
+    loss = float(((f_d - ft_d) ** 2).sum().item())
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        ts = []
+        for _ in range(reps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return float(np.median(ts))
+    out = {"workload": "water3000 (1,000 waters, 31.04 A, nu=6, a0=9 A, grid %s, L=%d)"
+           % ("x".join(str(m) for m in ff.top_grid), ff.levels),
+           "loss": loss}
+    out["forward_ms"] = timed(lambda: fwd(q_d, f_d))
+    for reuse in (True, False):
+        out[("reusing_forward" if reuse else "with_forward") + "_ms"] = timed(
+            lambda: ff.adjoint_device(pos_d.data_ptr(), q_d.data_ptr(), fbar.data_ptr(), 0.0,
+                                      dq.data_ptr(), dr.data_ptr(), reuse=reuse, stream=sh))
+    out["ratio_to_forward"] = round(out["reusing_forward_ms"] / out["forward_ms"], 3)
+    for k in list(out):
+        if k.endswith("_ms"):
+            out[k] = round(out[k], 4)
+    ff.sync()
+    ff.close()
+    return out
+
+
+def _batch_ref_worker(systems_part, lib_path, bar, out_q):
+    """One process of the batch's CPU baseline: builds its systems with the
+    reference library (neighbour lists and tables, untimed), waits for the
+    other workers, then evaluates each system once with FF_energy."""
+    sys.path.insert(0, ROOT)
+    try:
+        from oracle.oracle import RefFF
+        refs = [RefFF(q, pos, edges, cutoff=kw["cutoff"], nu=kw["order"], lib_path=lib_path)
+                for q, pos, edges, kw in systems_part]
+        bar.wait()
+        t0 = time.perf_counter()
+        for r in refs:
+            r.energy()
+        out_q.put(("ok", time.perf_counter() - t0, sum(r.N for r in refs)))
+    except Exception as ex:  # reported in the JSON line, never fatal
+        try:
+            bar.abort()
+        except Exception:
+            pass
+        out_q.put(("error", repr(ex)))
+
+
+def batch_cpu_reference(sysl, procs=8):
+    """The reference's own C code on the batch's systems: `procs` independent
+    host processes (spawned), systems dealt round-robin, each evaluated once
+    with FF_energy after an untimed FF_build; atoms/s = all atoms over the
+    wall time from a common barrier to the last worker's end."""
+    lib_path, kind, build = _ref_library()
+    if lib_path is None:
+        return {"value": None, "unavailable": "reference library not built"}
+    procs = max(1, min(procs, os.cpu_count() or 1, len(sysl)))
+    ctx = mp.get_context("spawn")
+    bar = ctx.Barrier(procs + 1)
+    out_q = ctx.Queue()
+    ps = [ctx.Process(target=_batch_ref_worker,
+                      args=(sysl[w::procs], lib_path, bar, out_q)) for w in range(procs)]
+    for p in ps:
+        p.start()
+    try:
+        bar.wait(timeout=600)
+    except Exception:
+        pass
+    t0 = time.perf_counter()
+    res = [out_q.get(timeout=900) for _ in ps]
+    wall = time.perf_counter() - t0
+    for p in ps:
+        p.join()
+    errs = [r[1] for r in res if r[0] != "ok"]
+    if errs:
+        return {"value": None, "error": errs[0]}
+    atoms = sum(r[2] for r in res)
+    return {"value": atoms / wall, "unit": "atoms/s", "cores": procs, "kind": kind,
+            "seconds": round(wall, 3), "slowest_worker_s": round(max(r[1] for r in res), 3),
+            "sample": "all %d systems (%d atoms), one FF_energy each, on %d independent "
+                      "host processes; FF_build untimed; %s" % (len(sysl), atoms, procs, build)}
+
+
 def box_change_timing(ff, edges, pos, pos_d, q_d, f_d, phi_d, e_d, torch, reps=5):
     """One MD step with a new box: FF_rebuild (tables on the host) or
     FF_rebuild_device (level stencils on the GPU), then one evaluation; wall
@@ -343,13 +465,14 @@ def box_change_timing(ff, edges, pos, pos_d, q_d, f_d, phi_d, e_d, torch, reps=5
 
 
 def batch_timing(dev, torch, flush, reps=10, warmup=3, precisions=("mixed", "fp64"),
-                 branches=0, per_system=True, count=256):
+                 branches=0, per_system=True, count=256, cpu=False):
     """Many independent systems in one graph launch against per-system
     launches: 256 charge-neutral +-1 ion boxes, N uniform in [500, 20000],
     density 0.1 / A^3, 2 A minimum separation, order cycled over 4/6/8,
     cutoff 8 A, grid and levels automatic (seeded; ions at random positions,
     see systems.ions). Device-resident inputs; L2 flushed before every timed
-    step; CUDA events on the launching stream."""
+    step; CUDA events on the launching stream. cpu: also time the reference's
+    C code on the same systems on 8 host processes (batch_cpu_reference)."""
     from msmpb_b200 import systems
     from msmpb_b200.forcefield import Batch, ForceField
     t0 = time.perf_counter()
@@ -433,6 +556,8 @@ def batch_timing(dev, torch, flush, reps=10, warmup=3, precisions=("mixed", "fp6
     for k in list(out):
         if k.endswith("_ms"):
             out[k] = round(out[k], 4)
+    if cpu:
+        out["cpu_reference"] = batch_cpu_reference(sysl)
     return out
 
 
@@ -713,12 +838,14 @@ def run_ours(args):
 
     # ---- adjoint (force and energy cotangents -> charge and position gradients) ----
     adjoint = adjoint_timing(ff, pos_d, q_d, f_d, phi_d, e_d, torch, flush, ms)
+    adjoint["water3000"] = adjoint_water3000(dev, torch, flush)
 
     # ---- box change every step (constant-pressure MD) ----
     rebuild = box_change_timing(ff, edges, pos, pos_d, q_d, f_d, phi_d, e_d, torch)
 
     # ---- many small systems: one graph launch against per-system launches ----
-    batch = None if args.skip_batch else batch_timing(dev, torch, flush)
+    batch = None if args.skip_batch else batch_timing(
+        dev, torch, flush, cpu=rank == 0 and world == 1 and not args.skip_cpu)
 
     # ---- CPU baseline (rank 0, one GPU only): the reference on the same box ----
     cpu = None

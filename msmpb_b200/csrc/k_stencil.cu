@@ -365,14 +365,12 @@ __device__ __forceinline__ void stencil_fold_body(const BlockCtx &ctx, StencilSh
     const T *Ks = smem + 3 * slice + s * tap_elems;
     if (i > 0) {  // F_i = A + B, in place
       for (int t = tid; t < H * W / V; t += nth) {
-        if constexpr (sizeof(T) == 4) {
-          float4 a = reinterpret_cast<float4 *>(As)[t];
+        if constexpr (sizeof(T) == 4) {  // packed adds: the same roundings
+          const float4 a = reinterpret_cast<float4 *>(As)[t];
           const float4 b = reinterpret_cast<const float4 *>(Bsl)[t];
-          a.x += b.x;
-          a.y += b.y;
-          a.z += b.z;
-          a.w += b.w;
-          reinterpret_cast<float4 *>(As)[t] = a;
+          const float2 lo = __fadd2_rn(make_float2(a.x, a.y), make_float2(b.x, b.y));
+          const float2 hi = __fadd2_rn(make_float2(a.z, a.w), make_float2(b.z, b.w));
+          reinterpret_cast<float4 *>(As)[t] = make_float4(lo.x, lo.y, hi.x, hi.y);
         } else {
           double2 a = reinterpret_cast<double2 *>(As)[t];
           const double2 b = reinterpret_cast<const double2 *>(Bsl)[t];
@@ -409,12 +407,16 @@ __device__ __forceinline__ void stencil_fold_body(const BlockCtx &ctx, StencilSh
       if (j < c1) {
 #pragma unroll
         for (int v = 0; v < RLV; v += V) {
-          if constexpr (sizeof(T) == 4) {
+          if constexpr (sizeof(T) == 4) {  // packed adds: the same roundings
             const float4 b = *reinterpret_cast<const float4 *>(r2 + v);
-            row[v] += b.x;
-            row[v + 1] += b.y;
-            row[v + 2] += b.z;
-            row[v + 3] += b.w;
+            const float2 lo =
+                __fadd2_rn(make_float2(row[v], row[v + 1]), make_float2(b.x, b.y));
+            const float2 hi =
+                __fadd2_rn(make_float2(row[v + 2], row[v + 3]), make_float2(b.z, b.w));
+            row[v] = lo.x;
+            row[v + 1] = lo.y;
+            row[v + 2] = hi.x;
+            row[v + 3] = hi.y;
           } else {
             const double2 b = *reinterpret_cast<const double2 *>(r2 + v);
             row[v] += b.x;
