@@ -64,16 +64,21 @@ inline int slice_pitch(int nz, int R, int S, int V) {
   return best * V;
 }
 
+// Padded copy: P[a][b][c] = q[wrap(a - S0/2)][wrap(b - S1/2)][wrap(c - S2/2)]
+// over the padded dimensions. One padded row (a, b) per warp, lanes along it
+// (kThreads / 32 rows per CTA).
 template <typename T>
 __device__ __forceinline__ void pad_body(const BlockCtx &ctx, StencilShape sh, const T *__restrict__ q, T *__restrict__ p) {
-  // one padded row (a, b) per ctx.b.(z, y); threads along it
-  const int a = ctx.b.z, b = ctx.b.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long row = (long)ctx.b.x * (blockDim.x >> 5) + warp;
+  if (row >= (long)sh.P[0] * sh.P[1]) return;
+  const int a = (int)(row / sh.P[1]), b = (int)(row - (long)a * sh.P[1]);
   const int x = pwrap(a - sh.S[0] / 2, sh.M[0]);
   const int y = pwrap(b - sh.S[1] / 2, sh.M[1]);
   const T *src = q + ((long)x * sh.M[1] + y) * sh.M[2];
-  T *dst = p + ((long)a * sh.P[1] + b) * sh.P[2];
+  T *dst = p + row * sh.P[2];
   const int h = sh.S[2] / 2, M2 = sh.M[2];
-  for (int c = ctx.b.x * blockDim.x + threadIdx.x; c < sh.P[2]; c += ctx.g.x * blockDim.x) {
+  for (int c = lane; c < sh.P[2]; c += 32) {
     int z = c - h;
     if (z < 0 || z >= M2) z = pwrap(z, M2);
     dst[c] = src[z];
@@ -728,8 +733,10 @@ bool stencil_fold_taps(const double *kh, const int S[3], bool fp64,
 
 template <typename T>
 void launch_pad(cudaStream_t s, const StencilShape &sh, const T *q, T *p) {
-  const dim3 grid((sh.P[2] + kThreads - 1) / kThreads, sh.P[1], sh.P[0]);
-  launch<KPad<T>, kThreads, 8>(s, k_pad<T>, grid, kThreads, 0, sh, q, p);
+  const long rows = (long)sh.P[0] * sh.P[1];
+  const int per = kThreads / 32;
+  launch<KPad<T>, kThreads, 8>(s, k_pad<T>, dim3((unsigned)((rows + per - 1) / per)), kThreads, 0,
+                               sh, q, p);
 }
 
 template <typename T>
