@@ -66,3 +66,21 @@ def test_reference_arm_under_two_ranks():
     # the same workload as the GPU arm names
     import bench
     assert d["config"] == bench.WORKLOAD_CONFIG
+
+
+def test_batch_cpu_reference_on_small_systems():
+    """The batch section's CPU baseline: the reference's C code on a few small
+    ion boxes of the batch workload, in independent spawned processes,
+    every atom counted once."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from msmpb_b200 import systems
+    from oracle.oracle import RefFF
+    if not RefFF.available():
+        pytest.skip("reference library not built (oracle/build_ref.py)")
+    sysl = systems.ion_batch(6, seed=5, n_min=500, n_max=1500)
+    out = bench.batch_cpu_reference(sysl, procs=3)
+    assert out["value"] > 0 and out["kind"] == "reference"
+    assert out["cores"] == min(3, os.cpu_count() or 1)
+    atoms = sum(len(q) for q, _, _, _ in sysl)
+    assert "all 6 systems (%d atoms)" % atoms in out["sample"]
