@@ -404,17 +404,44 @@ __device__ void sort_cell_by_z(int b, int e, int *__restrict__ perm,
   }
 }
 
-// Both per-cell sorts in one launch: threads [0, ncp) sort pair cells along
-// z, threads [ncp, ncp + ncg) sort grid cells by atom index.
+// Both per-cell sorts in one launch: a warp per pair cell for threads
+// [0, 32 ncp) (along z, ties by atom index), then a thread per grid cell (by
+// atom index). In a pair cell of up to 32 atoms lane l holds atom l's key and
+// its place is the number of atoms before it in (z, index) order, counted
+// from the other lanes' keys by shuffles (the same order as sort_cell_by_z,
+// which lane 0 runs for larger cells). blockDim.x is a multiple of 32, so a
+// warp never straddles two cells or the two parts.
 template <typename T>
 __device__ __forceinline__ void sort_cells_body(const BlockCtx &ctx, int ncp, const int *__restrict__ pstart, int *__restrict__ pperm,
              const V4<T> *__restrict__ key, int ncg, const int *__restrict__ gstart,
              int *__restrict__ gperm) {
-  const int c = ctx.b.x * blockDim.x + threadIdx.x;
-  if (c < ncp)
-    sort_cell_by_z<T>(pstart[c], pstart[c + 1], pperm, key);
-  else if (c < ncp + ncg)
-    sort_cell_by_index(gstart[c - ncp], gstart[c - ncp + 1], gperm);
+  const long t = (long)ctx.b.x * blockDim.x + threadIdx.x;
+  const long np = 32L * ncp;
+  if (t < np) {
+    const int c = (int)(t >> 5), lane = threadIdx.x & 31;
+    const int b = pstart[c], e = pstart[c + 1], n = e - b;
+    if (n <= 32) {
+      int id = 0;
+      T z = T(0);
+      if (lane < n) {
+        id = pperm[b + lane];
+        z = key[id].z;
+      }
+      int r = 0;
+      for (int j = 0; j < n; ++j) {
+        const T zj = __shfl_sync(0xffffffffu, z, j);
+        const int ij = __shfl_sync(0xffffffffu, id, j);
+        r += (zj < z || (zj == z && ij < id)) ? 1 : 0;
+      }
+      __syncwarp();  // every lane has read its slot before any lane writes
+      if (lane < n) pperm[b + r] = id;
+    } else if (lane == 0) {
+      sort_cell_by_z<T>(b, e, pperm, key);
+    }
+    return;
+  }
+  const long g = t - np;
+  if (g < ncg) sort_cell_by_index(gstart[g], gstart[g + 1], gperm);
 }
 template <typename T>
 struct KSortCells {
@@ -641,7 +668,7 @@ void launch_bin_scatter(cudaStream_t s, int N, const int *pcell, const int *psta
 template <typename T>
 void launch_bin_sort(cudaStream_t s, int ncp, const int *pstart, int *pperm, const V4<T> *key,
                      int ncg, const int *gstart, int *gperm) {
-  launch<KSortCells<T>, kThreads, 8>(s, k_sort_cells<T>, blocks_for((long)ncp + ncg, kThreads), kThreads, 0, ncp, pstart, pperm, key, ncg, gstart, gperm);
+  launch<KSortCells<T>, kThreads, 8>(s, k_sort_cells<T>, blocks_for(32L * ncp + ncg, kThreads), kThreads, 0, ncp, pstart, pperm, key, ncg, gstart, gperm);
 }
 
 template <typename T>
