@@ -915,7 +915,6 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
              s);
   launch_prep<T>(s, N_, pos, q, geom_, pcell_, gcell_, pcount_, gcount_, prel_,
                  gfrac_, prel64_, err_d_, qparts_);
-  launch_qstats_final(s, qparts_, nq_, qstats_);
   launch_scan2(s, pcount_, pstart_, ncp_, gcount_, gstart_, ncg_, scan_tmp_);
   const bool clusters = pair_variant_ == 2 && clusters_ok_;
   launch_bin_scatter(s, N_, pcell_, pstart_, pcursor_, pperm_, gcell_, gstart_, gcursor_,
@@ -944,6 +943,9 @@ int Plan<T>::enqueue(const EvalRequest &r, cudaStream_t s, const double *pos,
     }
     sp = aux_[0];
   }
+  // the charge sums (one latency-bound CTA, read by the combine only) on the
+  // short-range branch, off the serial binning path
+  launch_qstats_final(sp, qparts_, nq_, qstats_);
   if (clusters) {  // cluster build (part of the binning phase)
     const V4<double> *src64 =
         kMixed ? psorted64_ : reinterpret_cast<const V4<double> *>(psorted_);
