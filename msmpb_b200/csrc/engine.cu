@@ -1,9 +1,9 @@
 // Device plan and the launch sequence of one MSM evaluation
 // (code/forcefield1.c:101-235 restated for one B200):
 //
-//   bin + sort atoms (pair cells, finest-grid cells),   k_prep, k_qstats_final, scans,
-//   charge sums                                          k_scatter2,
-//                                                        k_sort_cells, k_gather2
+//   bin + sort atoms (pair cells, finest-grid cells),   k_prep, scans, k_scatter2,
+//   charge sums (per block in k_prep)                    k_sort_cells, k_gather2
+//   charge-sum reduction (on the short-range branch)     k_qstats_final
 //   cluster build (column counts in k_scatter2)          scan, k_cluster_fill
 //   short-range pair sum                                 k_pair_clusters_f32/_f64
 //   anterpolation -> q^1                                 k_anterp_tiles, k_anterp_fold
